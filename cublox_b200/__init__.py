@@ -1,0 +1,456 @@
+"""cublox_b200 — B200-native map-integration path of cublox's OccupancyGrid.
+
+Python view of the C ABI in include/cublox_b200.h (libcublox_b200.so, built
+in-tree for sm_100a).  `OccupancyGrid` mirrors the reference's class
+(include/cublox/OccupancyGrid.hpp:29-169): same method names, argument
+meaning and defaults; snake_case aliases are provided as well.
+
+There is no CPU fallback: constructing a grid without the built library or
+without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcublox_b200.so")
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_RANGE, ERR_DEVICE = -1, -2, -3, -4, -5
+LAYOUT_SOA, LAYOUT_AOS = 0, 1
+
+
+class VoxelState(enum.IntEnum):
+    UNKNOWN = 0
+    FREE = 1
+    OCCUPIED = 2
+
+
+class CubloxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+class ScanStats(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_int64), ("op_incs", ctypes.c_int64),
+                ("hit_incs", ctypes.c_int64), ("touched", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Load libcublox_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python cublox_b200/build.py` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        G = ctypes.c_void_p
+        f = ctypes.POINTER(ctypes.c_float)
+        i = ctypes.POINTER(ctypes.c_int)
+        i64 = ctypes.POINTER(ctypes.c_int64)
+        u8 = ctypes.POINTER(ctypes.c_uint8)
+        sig = {
+            "cublox_last_error": ([], ctypes.c_char_p),
+            "cublox_version": ([], ctypes.c_char_p),
+            "cublox_grid_create": ([i, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_double, f,
+                                    ctypes.c_void_p, ctypes.POINTER(G)], ctypes.c_int),
+            "cublox_grid_destroy": ([G], ctypes.c_int),
+            "cublox_grid_reset": ([G], ctypes.c_int),
+            "cublox_grid_reset_voxel": ([G, ctypes.c_int], ctypes.c_int),
+            "cublox_grid_set_max_range": ([G, ctypes.c_float], ctypes.c_int),
+            "cublox_grid_get_max_range": ([G, f], ctypes.c_int),
+            "cublox_grid_set_log_odds": ([G] + [ctypes.c_float] * 6, ctypes.c_int),
+            "cublox_grid_set_fp_mode": ([G, ctypes.c_uint], ctypes.c_int),
+            "cublox_grid_get_fp_mode": ([G, ctypes.POINTER(ctypes.c_uint)], ctypes.c_int),
+            "cublox_grid_update": ([G, f, f, f, ctypes.c_int, f], ctypes.c_int),
+            "cublox_grid_update_xyz": ([G, f, ctypes.c_int, ctypes.c_int, f], ctypes.c_int),
+            "cublox_grid_recenter": ([G, f, i], ctypes.c_int),
+            "cublox_grid_set_recenter_mode": ([G, ctypes.c_int], ctypes.c_int),
+            "cublox_grid_fetch": ([G, f, ctypes.c_float, ctypes.c_int, ctypes.c_int, f, u8, ctypes.c_int64,
+                                   i64], ctypes.c_int),
+            "cublox_grid_fetch_batch": ([G, f, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int, i64,
+                                         f, u8, ctypes.c_int64], ctypes.c_int),
+            "cublox_grid_fetch_counts": ([G, f, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                          i64], ctypes.c_int),
+            "cublox_grid_query_states": ([G, f, ctypes.c_int, u8], ctypes.c_int),
+            "cublox_grid_stored_at": ([G, ctypes.c_int, f], ctypes.c_int),
+            "cublox_grid_origin": ([G, i, f], ctypes.c_int),
+            "cublox_grid_geometry": ([G, i, i, i, f, i], ctypes.c_int),
+            "cublox_grid_first_run": ([G, i], ctypes.c_int),
+            "cublox_grid_set_origin_index": ([G, i], ctypes.c_int),
+            "cublox_grid_export": ([G, f], ctypes.c_int),
+            "cublox_grid_import": ([G, f], ctypes.c_int),
+            "cublox_grid_stream": ([G, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+            "cublox_grid_synchronize": ([G], ctypes.c_int),
+            "cublox_grid_enable_stats": ([G, ctypes.c_int], ctypes.c_int),
+            "cublox_grid_last_stats": ([G, ctypes.POINTER(ScanStats)], ctypes.c_int),
+            "cublox_grid_check": ([G, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+            "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
+            "cublox_grid_enable_timing": ([G, ctypes.c_int], ctypes.c_int),
+            "cublox_grid_last_timing": ([G, f], ctypes.c_int),
+            "cublox_grid_reference_steps": ([G, f, ctypes.c_int, f, i64], ctypes.c_int),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != OK:
+        msg = lib().cublox_last_error().decode(errors="replace")
+        raise CubloxError(rc, f"{what}: {msg}")
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _f3(v):
+    return (ctypes.c_float * 3)(*[float(x) for x in v])
+
+
+def _dev_ptr(obj):
+    """Device pointer of a CUDA array-like (torch tensor or
+    __cuda_array_interface__), else None."""
+    if hasattr(obj, "__cuda_array_interface__"):
+        return obj.__cuda_array_interface__["data"][0]
+    if hasattr(obj, "is_cuda") and getattr(obj, "is_cuda"):
+        return obj.data_ptr()
+    return None
+
+
+class OccupancyGrid:
+    """Drop-in for cublox::OccupancyGrid (OccupancyGrid.hpp:29-169)."""
+
+    VoxelState = VoxelState
+
+    def __init__(self, half_map_size_i, resolution: float, origin_at_center: bool = False,
+                 recenter_threshold: float | None = None, origin=(0.0, 0.0, 0.0), stream=None):
+        L = lib()
+        h = ctypes.c_void_p()
+        rc = L.cublox_grid_create((ctypes.c_int * 3)(*[int(v) for v in half_map_size_i]),
+                                  float(resolution), int(bool(origin_at_center)),
+                                  int(recenter_threshold is not None),
+                                  float(recenter_threshold or 0.0), _f3(origin),
+                                  ctypes.c_void_p(stream or 0), ctypes.byref(h))
+        _check(rc, "OccupancyGrid")
+        self._h = h
+        m = (ctypes.c_int * 3)()
+        hf = (ctypes.c_int * 3)()
+        vn = ctypes.c_int()
+        res = ctypes.c_float()
+        oc = ctypes.c_int()
+        _check(L.cublox_grid_geometry(h, m, hf, ctypes.byref(vn), ctypes.byref(res), ctypes.byref(oc)),
+               "geometry")
+        self.map_size_i = tuple(m)
+        self.half_map_size_i = tuple(hf)
+        self.voxel_num = vn.value
+        self.resolution = res.value
+        self.resolution_inv = np.float32(1.0) / np.float32(self.resolution)
+        self.origin_at_center = bool(oc.value)
+        self.recenter_threshold = recenter_threshold
+        self.l_params = dict(l_hit=0.847, l_miss=-0.405, l_min=-1.992, l_max=3.476,
+                             l_free=-0.0004, l_occupied=1.7346)
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cublox_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- configuration (OccupancyGrid.hpp:68-85) ----
+    def setMaxRaycastRange(self, r: float):
+        _check(lib().cublox_grid_set_max_range(self._h, float(r)), "setMaxRaycastRange")
+
+    def getMaxRaycastRange(self) -> float:
+        v = ctypes.c_float()
+        _check(lib().cublox_grid_get_max_range(self._h, ctypes.byref(v)), "getMaxRaycastRange")
+        return v.value
+
+    def setLogOddsParams(self, l_hit, l_miss, l_min, l_max, l_free, l_occupied):
+        _check(lib().cublox_grid_set_log_odds(self._h, l_hit, l_miss, l_min, l_max, l_free,
+                                              l_occupied), "setLogOddsParams")
+        self.l_params = dict(l_hit=l_hit, l_miss=l_miss, l_min=l_min, l_max=l_max, l_free=l_free,
+                             l_occupied=l_occupied)
+
+    def set_fp_mode(self, mode: int):
+        _check(lib().cublox_grid_set_fp_mode(self._h, int(mode)), "set_fp_mode")
+
+    def fp_mode(self) -> int:
+        v = ctypes.c_uint()
+        _check(lib().cublox_grid_get_fp_mode(self._h, ctypes.byref(v)), "fp_mode")
+        return v.value
+
+    def set_recenter_mode(self, mode: int):
+        _check(lib().cublox_grid_set_recenter_mode(self._h, int(mode)), "set_recenter_mode")
+
+    # ---- path ----
+    def update(self, cloud, sensor_origin):
+        """update(cloud, sensor_origin) — OccupancyGrid.cpp:181-238.
+
+        `cloud`: (N, 3) float32 host array (any order; copied), or a CUDA
+        (N, 3) row-major tensor, or a CUDA (3, N) tensor (SoA)."""
+        so = _f3(sensor_origin)
+        ptr = _dev_ptr(cloud)
+        if ptr is not None:
+            shape = tuple(cloud.shape)
+            if len(shape) != 2 or 3 not in shape:
+                raise ValueError("device cloud must be (N, 3) or (3, N)")
+            if shape[1] == 3 and shape[0] != 3:
+                layout, n = LAYOUT_AOS, shape[0]
+            else:
+                layout, n = LAYOUT_SOA, shape[1]
+            rc = lib().cublox_grid_update_xyz(self._h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)),
+                                              layout, int(n), so)
+            _check(rc, "update")
+            return
+        p = np.asarray(cloud, dtype=np.float32)
+        if p.ndim != 2 or p.shape[1] != 3:
+            raise ValueError("cloud must be (N, 3)")
+        p = np.ascontiguousarray(p)
+        _check(lib().cublox_grid_update_xyz(self._h, _fp(p), LAYOUT_AOS, p.shape[0], so), "update")
+
+    def update_soa(self, x, y, z, sensor_origin):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        z = np.ascontiguousarray(z, dtype=np.float32)
+        _check(lib().cublox_grid_update(self._h, _fp(x), _fp(y), _fp(z), x.shape[0],
+                                        _f3(sensor_origin)), "update")
+
+    def recenter(self, pos) -> int:
+        """recenter(pos) — OccupancyGrid.cpp:141-179.  Returns the action."""
+        a = ctypes.c_int(0)
+        _check(lib().cublox_grid_recenter(self._h, _f3(pos), ctypes.byref(a)), "recenter")
+        return a.value
+
+    def fetchOccupancyAround(self, center, radius: float, state_filter=None, max_results: int = 0):
+        """fetchOccupancyAround — OccupancyGrid.cpp:240-356.
+
+        Returns (positions (n, 3) float32, states (n,) uint8), ordered by
+        ascending (x, y, z) global voxel index."""
+        flt = -1 if state_filter is None else int(state_filter)
+        c = _f3(center)
+        counts = np.zeros(1, dtype=np.int64)
+        _check(lib().cublox_grid_fetch_counts(self._h, c, 1, float(radius), flt, int(max_results),
+                                              counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+               "fetchOccupancyAround")
+        n = int(counts[0])
+        pos = np.empty((max(n, 1), 3), dtype=np.float32)
+        st = np.empty(max(n, 1), dtype=np.uint8)
+        got = ctypes.c_int64(0)
+        _check(lib().cublox_grid_fetch(self._h, c, float(radius), flt, int(max_results), _fp(pos),
+                                       st.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n,
+                                       ctypes.byref(got)), "fetchOccupancyAround")
+        return pos[: got.value], st[: got.value]
+
+    def fetch_batch(self, centers, radius: float, state_filter=None, max_results: int = 0):
+        """All centres in one launch: (offsets (n+1,), positions, states)."""
+        flt = -1 if state_filter is None else int(state_filter)
+        c = np.ascontiguousarray(np.asarray(centers, dtype=np.float32).reshape(-1, 3))
+        nq = c.shape[0]
+        counts = np.zeros(max(nq, 1), dtype=np.int64)
+        _check(lib().cublox_grid_fetch_counts(self._h, _fp(c), nq, float(radius), flt, int(max_results),
+                                              counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+               "fetch_batch")
+        total = int(counts[:nq].sum())
+        off = np.zeros(nq + 1, dtype=np.int64)
+        pos = np.empty((max(total, 1), 3), dtype=np.float32)
+        st = np.empty(max(total, 1), dtype=np.uint8)
+        _check(lib().cublox_grid_fetch_batch(self._h, _fp(c), nq, float(radius), flt, int(max_results),
+                                             off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _fp(pos),
+                                             st.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), total),
+               "fetch_batch")
+        return off, pos[:total], st[:total]
+
+    def fetch_counts(self, centers, radius: float, state_filter=None, max_results: int = 0):
+        flt = -1 if state_filter is None else int(state_filter)
+        c = np.ascontiguousarray(np.asarray(centers, dtype=np.float32).reshape(-1, 3))
+        out = np.zeros(max(c.shape[0], 1), dtype=np.int64)
+        _check(lib().cublox_grid_fetch_counts(self._h, _fp(c), c.shape[0], float(radius), flt,
+                                              int(max_results),
+                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+               "fetch_counts")
+        return out[: c.shape[0]]
+
+    # ---- queries (OccupancyGrid.cpp:358-429) ----
+    def query_states(self, points) -> np.ndarray:
+        p = np.ascontiguousarray(np.asarray(points, dtype=np.float32).reshape(-1, 3))
+        out = np.empty(max(p.shape[0], 1), dtype=np.uint8)
+        _check(lib().cublox_grid_query_states(self._h, _fp(p), p.shape[0],
+                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))),
+               "query_states")
+        return out[: p.shape[0]]
+
+    def isOccupied(self, pos) -> bool:
+        return int(self.query_states([pos])[0]) == VoxelState.OCCUPIED
+
+    def isFree(self, pos) -> bool:
+        return int(self.query_states([pos])[0]) == VoxelState.FREE
+
+    def isUnknown(self, pos) -> bool:
+        return int(self.query_states([pos])[0]) == VoxelState.UNKNOWN
+
+    def storedAt(self, hash_id: int) -> float:
+        v = ctypes.c_float()
+        _check(lib().cublox_grid_stored_at(self._h, int(hash_id), ctypes.byref(v)), "storedAt")
+        return v.value
+
+    # ---- Grid (Grid.hpp:22-57) ----
+    def getOriginIndex(self):
+        o = (ctypes.c_int * 3)()
+        of = (ctypes.c_float * 3)()
+        _check(lib().cublox_grid_origin(self._h, o, of), "getOriginIndex")
+        return tuple(o)
+
+    def getOriginPosition(self):
+        o = (ctypes.c_int * 3)()
+        of = (ctypes.c_float * 3)()
+        _check(lib().cublox_grid_origin(self._h, o, of), "getOriginPosition")
+        return tuple(of)
+
+    def first_run(self) -> bool:
+        v = ctypes.c_int()
+        _check(lib().cublox_grid_first_run(self._h, ctypes.byref(v)), "first_run")
+        return bool(v.value)
+
+    def set_origin_index(self, o):
+        _check(lib().cublox_grid_set_origin_index(self._h, (ctypes.c_int * 3)(*[int(v) for v in o])),
+               "set_origin_index")
+
+    def reset(self):
+        _check(lib().cublox_grid_reset(self._h), "reset")
+
+    def resetVoxel(self, hash_id: int):
+        _check(lib().cublox_grid_reset_voxel(self._h, int(hash_id)), "resetVoxel")
+
+    # ---- state transfer ----
+    def export(self) -> np.ndarray:
+        out = np.empty(self.voxel_num, dtype=np.float32)
+        _check(lib().cublox_grid_export(self._h, _fp(out)), "export")
+        return out
+
+    def import_(self, occ):
+        a = np.ascontiguousarray(occ, dtype=np.float32)
+        if a.size != self.voxel_num:
+            raise ValueError("occ must hold voxel_num floats")
+        _check(lib().cublox_grid_import(self._h, _fp(a)), "import")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().cublox_grid_stream(self._h, ctypes.byref(s)), "stream")
+        return s.value or 0
+
+    def synchronize(self):
+        _check(lib().cublox_grid_synchronize(self._h), "synchronize")
+
+    def enable_stats(self, on: bool = True):
+        _check(lib().cublox_grid_enable_stats(self._h, int(on)), "enable_stats")
+
+    def last_stats(self) -> dict:
+        s = ScanStats()
+        _check(lib().cublox_grid_last_stats(self._h, ctypes.byref(s)), "last_stats")
+        return s.as_dict()
+
+    def count_scan(self, cloud, sensor_origin):
+        """Per-voxel (op, hit) counts of one scan, without folding them."""
+        p = np.ascontiguousarray(np.asarray(cloud, dtype=np.float32).reshape(-1, 3))
+        op = np.empty(self.voxel_num, dtype=np.int32)
+        hit = np.empty(self.voxel_num, dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _check(lib().cublox_grid_count_scan(self._h, _fp(p), p.shape[0], _f3(sensor_origin),
+                                            op.ctypes.data_as(ip), hit.ctypes.data_as(ip)),
+               "count_scan")
+        return op, hit
+
+    def enable_timing(self, on: bool = True):
+        _check(lib().cublox_grid_enable_timing(self._h, int(on)), "enable_timing")
+
+    def last_timing(self):
+        """Device ms of the last (raycast, fold, recenter clear); -1 = none."""
+        ms = (ctypes.c_float * 3)()
+        _check(lib().cublox_grid_last_timing(self._h, ms), "last_timing")
+        return tuple(ms)
+
+    def reference_steps(self, cloud, sensor_origin) -> int:
+        """The reference's work units for one scan (DDA iterations + endpoint)."""
+        p = np.ascontiguousarray(np.asarray(cloud, dtype=np.float32).reshape(-1, 3))
+        v = ctypes.c_int64()
+        _check(lib().cublox_grid_reference_steps(self._h, _fp(p), p.shape[0], _f3(sensor_origin),
+                                                 ctypes.byref(v)), "reference_steps")
+        return v.value
+
+    def update_ptr(self, ptr: int, n: int, sensor_origin, layout: int = LAYOUT_SOA):
+        """update() from a raw pointer (device, pinned or pageable host)."""
+        _check(lib().cublox_grid_update_xyz(self._h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)),
+                                            layout, int(n), _f3(sensor_origin)), "update")
+
+    def check(self) -> int:
+        w = ctypes.c_uint32()
+        _check(lib().cublox_grid_check(self._h, ctypes.byref(w)), "check")
+        return w.value
+
+    # snake_case aliases
+    set_max_raycast_range = setMaxRaycastRange
+    get_max_raycast_range = getMaxRaycastRange
+    set_log_odds_params = setLogOddsParams
+    fetch_occupancy_around = fetchOccupancyAround
+    is_occupied = isOccupied
+    is_free = isFree
+    is_unknown = isUnknown
+    stored_at = storedAt
+    get_origin_index = getOriginIndex
+    get_origin_position = getOriginPosition
+    reset_voxel = resetVoxel
+
+
+_libm = None
+
+
+def logit(p: float) -> float:
+    """utils.hpp:185-188 in float32: clamp to [1e-6, 1 - 1e-6], then the C
+    library's logf of pc / (1 - pc)."""
+    global _libm
+    if _libm is None:
+        _libm = ctypes.CDLL("libm.so.6")
+        _libm.logf.argtypes = [ctypes.c_float]
+        _libm.logf.restype = ctypes.c_float
+    lo, hi = np.float32(1.0e-6), np.float32(1.0) - np.float32(1.0e-6)
+    pc = np.float32(p)
+    pc = lo if pc < lo else (hi if hi < pc else pc)
+    return float(_libm.logf(float(np.float32(pc / (np.float32(1.0) - pc)))))
+
+
+def yaml_log_odds():
+    """Log-odds of the reference's config/cublox_driver.yaml probabilities
+    (hit 0.9, miss 0.49, min 0.12, max 0.98, free 0.499, occupied 0.85)."""
+    return tuple(logit(p) for p in (0.9, 0.49, 0.12, 0.98, 0.499, 0.85))
+
+
+__all__ = ["OccupancyGrid", "VoxelState", "CubloxError", "lib", "logit", "LIB_PATH"]

@@ -1,0 +1,1041 @@
+// C ABI of cublox_b200 (include/cublox_b200.h): host orchestration of one
+// occupancy map on one B200.  Host arithmetic that the reference performs on
+// the CPU (window geometry, fetch bounds, recenter gate) is restated here with
+// plain float ops; this file is compiled with -ffp-contract=off so that the
+// host compiler fuses nothing either.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/cublox_b200.h"
+#include "exact_fp.cuh"
+#include "kernels.cuh"
+
+using namespace cublox_b200;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what, int line) {
+  g_err = std::string("cublox_b200: ") + what + ": " + cudaGetErrorString(e) +
+          " (capi.cu:" + std::to_string(line) + ")";
+  return CUBLOX_ERR_CUDA;
+}
+
+#define CK(call)                                                     \
+  do {                                                               \
+    cudaError_t e_ = (call);                                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call, __LINE__);    \
+  } while (0)
+
+#define CK_LAUNCH()                                                  \
+  do {                                                               \
+    cudaError_t e_ = cudaGetLastError();                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, "launch", __LINE__); \
+  } while (0)
+
+// Host-side posToGlobalIndex as the reference's x86-64 build computes it
+// (utils.hpp:24-31): no FMA, cvttss2si (NaN/out of range -> INT_MIN).
+int f2i_x86(float v) {
+  if (v >= -2147483648.0f && v < 2147483648.0f) return static_cast<int>(v);
+  return std::numeric_limits<int>::min();
+}
+int d2i_x86(double v) {
+  if (v > -2147483649.0 && v < 2147483648.0) return static_cast<int>(v);
+  return std::numeric_limits<int>::min();
+}
+int host_p2g(float p, float inv, bool ctr) {
+  if (ctr) {
+    const float s = p < 0.0f ? -1.0f : 1.0f;
+    const float m = p * inv;
+    return f2i_x86(m + s * 0.5f);
+  }
+  return f2i_x86(std::floor(p * inv));
+}
+float g2p(int g, float res, bool ctr) {
+  return ctr ? static_cast<float>(g) * res
+             : (static_cast<float>(g) + 0.5f) * res;
+}
+
+// 0: pageable host memory, 1: pinned host memory, 2: device-accessible.
+int mem_kind(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return 2;
+  if (a.type == cudaMemoryTypeHost) return 1;
+  return 0;
+}
+
+}  // namespace
+
+struct cublox_grid {
+  // Grid::Config (Grid.hpp:44-53)
+  int half[3] = {0, 0, 0};
+  int map[3] = {0, 0, 0};
+  int voxel_num = 0;
+  float res = 0.0f, res_inv = 0.0f;
+  bool ctr = false;
+  bool has_thr = false;
+  float thr_sq = 0.0f;
+  int origin_i[3] = {0, 0, 0};
+  float origin_f[3] = {0.0f, 0.0f, 0.0f};
+  bool first_run = true;
+  float max_range = 25.0f;
+  // OccupancyGrid.hpp:162-168 defaults
+  float l_hit = 0.847f, l_miss = -0.405f, l_min = -1.992f, l_max = 3.476f;
+  float l_free = -0.0004f, l_occ = 1.7346f, l_unknown = 0.0f;
+  unsigned fp = kFpPinned;
+  int recenter_mode = 0;
+  bool stats_on = false;
+  bool timing_on = false;
+  cudaEvent_t tev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool tev_used[3] = {false, false, false};
+
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  float *d_occ = nullptr;
+  uint32_t *d_cnt = nullptr;
+  uint32_t *d_hit = nullptr;
+  unsigned long long *d_stats = nullptr;  // 4
+  uint32_t *d_err = nullptr;
+  uint32_t *d_masks = nullptr;  // recenter slab masks
+  int mask_words[3] = {0, 0, 0};
+
+  float *d_cloud = nullptr;  // SoA [x|y|z]
+  int cloud_cap = 0;
+  float *h_stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  int stage_cap = 0;
+  int stage_idx = 0;
+
+  // fetch scratch
+  void *d_fq = nullptr;  // centers | qbox | qr2 | counts | offsets | limits
+  size_t fq_bytes = 0;
+  float *d_fpos = nullptr;
+  uint8_t *d_fstate = nullptr;
+  int64_t fcap = 0;
+  uint8_t *d_qout = nullptr;
+  float *d_qin = nullptr;
+  int qcap = 0;
+};
+
+extern "C" {
+
+const char *cublox_last_error(void) { return g_err.c_str(); }
+const char *cublox_version(void) { return "cublox_b200 0.1 (sm_100a)"; }
+
+static void free_all(cublox_grid *g) {
+  cudaFree(g->d_occ);
+  cudaFree(g->d_cnt);
+  cudaFree(g->d_hit);
+  cudaFree(g->d_stats);
+  cudaFree(g->d_err);
+  cudaFree(g->d_masks);
+  cudaFree(g->d_cloud);
+  cudaFree(g->d_fq);
+  cudaFree(g->d_fpos);
+  cudaFree(g->d_fstate);
+  cudaFree(g->d_qout);
+  cudaFree(g->d_qin);
+  for (int i = 0; i < 2; ++i) {
+    if (g->h_stage[i]) cudaFreeHost(g->h_stage[i]);
+    if (g->stage_ev[i]) cudaEventDestroy(g->stage_ev[i]);
+  }
+  for (int i = 0; i < 6; ++i)
+    if (g->tev[i]) cudaEventDestroy(g->tev[i]);
+  if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+}
+
+// Per-stage device timing (raycast, fold, recenter clear), opt-in.
+static void tmark(cublox_grid *g, int stage, int end) {
+  if (!g->timing_on) return;
+  cudaEventRecord(g->tev[2 * stage + end], g->stream);
+  if (end) g->tev_used[stage] = true;
+}
+
+static void set_origin(cublox_grid *g, const int o[3]) {
+  for (int a = 0; a < 3; ++a) {
+    g->origin_i[a] = o[a];
+    g->origin_f[a] = g2p(o[a], g->res, g->ctr);
+  }
+}
+
+int cublox_grid_create(const int half_map_size[3], float resolution,
+                       int origin_at_center, int has_recenter_threshold,
+                       double recenter_threshold, const float origin[3],
+                       void *stream, cublox_grid **out) {
+  if (!half_map_size || !origin || !out)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_create: null argument");
+  *out = nullptr;
+  if (!(resolution > 0.0f) || !std::isfinite(resolution))
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_create: resolution must be > 0");
+  int64_t total = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (half_map_size[a] < 0)
+      return fail(CUBLOX_ERR_INVALID, "cublox_grid_create: negative half size");
+    total *= 2 * static_cast<int64_t>(half_map_size[a]) + 1;
+  }
+  if (total > std::numeric_limits<int>::max())
+    return fail(CUBLOX_ERR_RANGE,
+                "cublox_grid_create: requested voxel_num = " +
+                    std::to_string(total) + " exceeds int32 max (" +
+                    std::to_string(std::numeric_limits<int>::max()) +
+                    "). Pick a smaller half_map_size_i.");
+  cublox_grid *g = new cublox_grid();
+  g->res = resolution;
+  g->res_inv = 1.0f / resolution;
+  for (int a = 0; a < 3; ++a) {
+    g->half[a] = half_map_size[a];
+    g->map[a] = 2 * half_map_size[a] + 1;
+  }
+  g->voxel_num = static_cast<int>(total);
+  g->has_thr = has_recenter_threshold != 0;
+  if (g->has_thr) {
+    const float t = static_cast<float>(recenter_threshold);
+    g->thr_sq = t * t;
+  }
+  g->ctr = origin_at_center != 0;
+  int o[3];
+  for (int a = 0; a < 3; ++a) o[a] = host_p2g(origin[a], g->res_inv, g->ctr);
+  set_origin(g, o);
+  cudaGetDevice(&g->device);
+
+  auto bail = [&](cudaError_t e, const char *what) {
+    int rc = cuda_fail(e, what, __LINE__);
+    if (e == cudaErrorMemoryAllocation) {
+      rc = CUBLOX_ERR_NOMEM;
+      g_err = std::string("cublox_grid_create: failed to allocate voxel buffers: ") +
+              cudaGetErrorString(e);
+    }
+    cudaGetLastError();
+    free_all(g);
+    delete g;
+    return rc;
+  };
+  cudaError_t e;
+  if (stream) {
+    g->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return bail(e, "cudaStreamCreate");
+    g->own_stream = true;
+  }
+  const size_t n = static_cast<size_t>(g->voxel_num);
+  if ((e = cudaMalloc(&g->d_occ, n * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc occ");
+  if ((e = cudaMalloc(&g->d_cnt, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc cnt");
+  if ((e = cudaMalloc(&g->d_hit, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc hit");
+  if ((e = cudaMalloc(&g->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "cudaMalloc stats");
+  if ((e = cudaMalloc(&g->d_err, sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc err");
+  int words = 0;
+  for (int a = 0; a < 3; ++a) {
+    g->mask_words[a] = (g->map[a] + 31) / 32;
+    words += g->mask_words[a];
+  }
+  if ((e = cudaMalloc(&g->d_masks, words * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc masks");
+  if ((e = cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream)) != cudaSuccess) return bail(e, "memset occ");
+  if ((e = cudaMemsetAsync(g->d_cnt, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess) return bail(e, "memset cnt");
+  if ((e = cudaMemsetAsync(g->d_hit, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess) return bail(e, "memset hit");
+  if ((e = cudaMemsetAsync(g->d_stats, 0, 4 * sizeof(unsigned long long), g->stream)) != cudaSuccess) return bail(e, "memset stats");
+  if ((e = cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), g->stream)) != cudaSuccess) return bail(e, "memset err");
+  if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(e, "sync");
+  *out = g;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_destroy(cublox_grid *g) {
+  if (!g) return CUBLOX_OK;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  free_all(g);
+  delete g;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_reset(cublox_grid *g) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  const size_t n = static_cast<size_t>(g->voxel_num);
+  CK(cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream));
+  CK(cudaMemsetAsync(g->d_cnt, 0, n * sizeof(uint32_t), g->stream));
+  CK(cudaMemsetAsync(g->d_hit, 0, n * sizeof(uint32_t), g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  g->first_run = true;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_reset_voxel(cublox_grid *g, int hash_id) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  if (hash_id < 0 || hash_id >= g->voxel_num) return CUBLOX_OK;
+  CK(cudaMemsetAsync(g->d_occ + hash_id, 0, sizeof(float), g->stream));
+  CK(cudaMemsetAsync(g->d_cnt + hash_id, 0, sizeof(uint32_t), g->stream));
+  CK(cudaMemsetAsync(g->d_hit + hash_id, 0, sizeof(uint32_t), g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_set_max_range(cublox_grid *g, float range) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  g->max_range = range;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_get_max_range(const cublox_grid *g, float *range) {
+  if (!g || !range) return fail(CUBLOX_ERR_INVALID, "null argument");
+  *range = g->max_range;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_set_log_odds(cublox_grid *g, float l_hit, float l_miss,
+                             float l_min, float l_max, float l_free,
+                             float l_occupied) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  g->l_hit = l_hit;
+  g->l_miss = l_miss;
+  g->l_min = l_min;
+  g->l_max = l_max;
+  g->l_free = l_free;
+  g->l_occ = l_occupied;
+  g->l_unknown = 0.0f;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_set_fp_mode(cublox_grid *g, unsigned mode) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  g->fp = mode;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode) {
+  if (!g || !mode) return fail(CUBLOX_ERR_INVALID, "null argument");
+  *mode = g->fp;
+  return CUBLOX_OK;
+}
+
+static int ensure_cloud(cublox_grid *g, int n) {
+  if (n <= g->cloud_cap) return CUBLOX_OK;
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(g->d_cloud);
+  g->d_cloud = nullptr;
+  g->cloud_cap = 0;
+  cudaError_t e = cudaMalloc(&g->d_cloud, sizeof(float) * 3 * static_cast<size_t>(n));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update: cloud buffer allocation failed");
+  }
+  g->cloud_cap = n;
+  return CUBLOX_OK;
+}
+
+static int ensure_stage(cublox_grid *g, int n) {
+  if (n <= g->stage_cap) return CUBLOX_OK;
+  for (int i = 0; i < 2; ++i) {
+    if (g->stage_ev[i]) CK(cudaEventSynchronize(g->stage_ev[i]));
+    if (g->h_stage[i]) cudaFreeHost(g->h_stage[i]);
+    g->h_stage[i] = nullptr;
+  }
+  g->stage_cap = 0;
+  for (int i = 0; i < 2; ++i) {
+    cudaError_t e = cudaMallocHost(&g->h_stage[i], sizeof(float) * 3 * static_cast<size_t>(n));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update: pinned staging allocation failed");
+    }
+    if (!g->stage_ev[i]) CK(cudaEventCreateWithFlags(&g->stage_ev[i], cudaEventDisableTiming));
+  }
+  g->stage_cap = n;
+  return CUBLOX_OK;
+}
+
+// Launch raycast (+ fold unless count_only) on a device SoA cloud.
+static int integrate(cublox_grid *g, const float *dx, const float *dy,
+                     const float *dz, int n, int stride,
+                     const float sensor[3], bool count_only = false) {
+  if (g->stats_on)
+    CK(cudaMemsetAsync(g->d_stats, 0, 4 * sizeof(unsigned long long), g->stream));
+  RayParams p{};
+  p.x = dx;
+  p.y = dy;
+  p.z = dz;
+  p.n = n;
+  p.stride = stride;
+  for (int a = 0; a < 3; ++a) {
+    p.o[a] = sensor[a];
+    p.win[a] = g->origin_i[a];
+    p.half[a] = g->half[a];
+    p.map[a] = g->map[a];
+  }
+  p.res = g->res;
+  p.inv = g->res_inv;
+  p.max_range = g->max_range;
+  p.vnum = g->voxel_num;
+  p.ctr = g->ctr ? 1 : 0;
+  p.fp = g->fp;
+  p.cnt = g->d_cnt;
+  p.hit = g->d_hit;
+  p.stats = g->stats_on ? g->d_stats : nullptr;
+  p.err = g->d_err;
+  tmark(g, 0, 0);
+  launch_raycast(p, g->stream);
+  CK_LAUNCH();
+  tmark(g, 0, 1);
+  if (count_only) return CUBLOX_OK;
+  ApplyParams a{};
+  a.occ = g->d_occ;
+  a.cnt = g->d_cnt;
+  a.hit = g->d_hit;
+  a.vnum = g->voxel_num;
+  a.l_hit = g->l_hit;
+  a.l_miss = g->l_miss;
+  a.l_min = g->l_min;
+  a.l_max = g->l_max;
+  a.l_unknown = g->l_unknown;
+  a.fp = g->fp;
+  a.stats = g->stats_on ? g->d_stats : nullptr;
+  tmark(g, 1, 0);
+  launch_apply(a, g->stream);
+  CK_LAUNCH();
+  tmark(g, 1, 1);
+  return CUBLOX_OK;
+}
+
+static void snap_first_run(cublox_grid *g, const float sensor[3]) {
+  if (!g->first_run) return;
+  int o[3];
+  for (int a = 0; a < 3; ++a) o[a] = host_p2g(sensor[a], g->res_inv, g->ctr);
+  set_origin(g, o);
+  g->first_run = false;
+}
+
+static int update_impl(cublox_grid *g, const float *x, const float *y,
+                       const float *z, const float *xyz, int layout, int n,
+                       const float sensor[3]) {
+  if (!g || !sensor) return fail(CUBLOX_ERR_INVALID, "cublox_grid_update: null argument");
+  if (g->voxel_num <= 0 || n <= 0) return CUBLOX_OK;  // OccupancyGrid.cpp:183-190
+  const void *probe = xyz ? static_cast<const void *>(xyz) : static_cast<const void *>(x);
+  if (!probe || (!xyz && (!y || !z)))
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update: null cloud");
+  snap_first_run(g, sensor);
+  const int kind = mem_kind(probe);
+  const bool dev = kind == 2;
+  if (dev && xyz && layout == CUBLOX_LAYOUT_AOS)
+    return integrate(g, xyz, xyz + 1, xyz + 2, n, 3, sensor);
+  if (dev && xyz)
+    return integrate(g, xyz, xyz + n, xyz + 2 * static_cast<size_t>(n), n, 1, sensor);
+  if (dev) return integrate(g, x, y, z, n, 1, sensor);
+  int rc = ensure_cloud(g, n);
+  if (rc) return rc;
+  const size_t nbytes = sizeof(float) * static_cast<size_t>(n);
+  if (kind == 1 && xyz) {
+    // Pinned host cloud: copy straight from it; return once the copy has
+    // landed so the caller may reuse its buffer.
+    CK(cudaMemcpyAsync(g->d_cloud, xyz, 3 * nbytes, cudaMemcpyHostToDevice, g->stream));
+    if (!g->stage_ev[0]) CK(cudaEventCreateWithFlags(&g->stage_ev[0], cudaEventDisableTiming));
+    CK(cudaEventRecord(g->stage_ev[0], g->stream));
+    rc = layout == CUBLOX_LAYOUT_AOS
+             ? integrate(g, g->d_cloud, g->d_cloud + 1, g->d_cloud + 2, n, 3, sensor)
+             : integrate(g, g->d_cloud, g->d_cloud + n, g->d_cloud + 2 * static_cast<size_t>(n),
+                         n, 1, sensor);
+    if (rc) return rc;
+    CK(cudaEventSynchronize(g->stage_ev[0]));
+    return CUBLOX_OK;
+  }
+  // Pageable host cloud: stage into pinned memory, one async copy, then
+  // integrate.
+  rc = ensure_stage(g, n);
+  if (rc) return rc;
+  const int s = g->stage_idx;
+  g->stage_idx ^= 1;
+  CK(cudaEventSynchronize(g->stage_ev[s]));
+  float *h = g->h_stage[s];
+  const size_t nb = sizeof(float) * static_cast<size_t>(n);
+  if (xyz && layout == CUBLOX_LAYOUT_AOS) {
+    for (int i = 0; i < n; ++i) {
+      h[i] = xyz[3 * static_cast<size_t>(i)];
+      h[n + i] = xyz[3 * static_cast<size_t>(i) + 1];
+      h[2 * static_cast<size_t>(n) + i] = xyz[3 * static_cast<size_t>(i) + 2];
+    }
+  } else if (xyz) {
+    std::memcpy(h, xyz, 3 * nb);
+  } else {
+    std::memcpy(h, x, nb);
+    std::memcpy(h + n, y, nb);
+    std::memcpy(h + 2 * static_cast<size_t>(n), z, nb);
+  }
+  CK(cudaMemcpyAsync(g->d_cloud, h, 3 * nb, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaEventRecord(g->stage_ev[s], g->stream));
+  return integrate(g, g->d_cloud, g->d_cloud + n, g->d_cloud + 2 * static_cast<size_t>(n), n,
+                   1, sensor);
+}
+
+int cublox_grid_update(cublox_grid *g, const float *x, const float *y,
+                       const float *z, int n, const float sensor_origin[3]) {
+  return update_impl(g, x, y, z, nullptr, CUBLOX_LAYOUT_SOA, n, sensor_origin);
+}
+
+int cublox_grid_update_xyz(cublox_grid *g, const float *xyz, int layout,
+                           int n, const float sensor_origin[3]) {
+  if (layout != CUBLOX_LAYOUT_SOA && layout != CUBLOX_LAYOUT_AOS)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_xyz: unknown layout");
+  return update_impl(g, nullptr, nullptr, nullptr, xyz, layout, n, sensor_origin);
+}
+
+// ---- recenter ---------------------------------------------------------------
+int cublox_grid_set_recenter_mode(cublox_grid *g, int mode) {
+  if (!g || (mode != 0 && mode != 1)) return fail(CUBLOX_ERR_INVALID, "bad recenter mode");
+  g->recenter_mode = mode;
+  return CUBLOX_OK;
+}
+
+static int normalize_slice(int x, int half) {
+  const int range = 2 * half + 1;
+  int y = (x + half) % range;
+  if (y < 0) y += range;
+  return y - half;
+}
+
+int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
+  if (action) *action = 0;
+  if (!g || !pos) return fail(CUBLOX_ERR_INVALID, "cublox_grid_recenter: null argument");
+  if (!g->has_thr || g->voxel_num <= 0) return CUBLOX_OK;  // OccupancyGrid.cpp:142-145
+  const float dx = pos[0] - g->origin_f[0];
+  const float dy = pos[1] - g->origin_f[1];
+  const float dz = pos[2] - g->origin_f[2];
+  // Host gate (OccupancyGrid.cpp:148): Eigen squaredNorm, no FMA.
+  if (sos(dx, dy, dz, kSosPlain) < g->thr_sq) return CUBLOX_OK;
+  // planRecenterKernel's own re-check (kernels.cu:326-331), device rounding.
+  if (sos(dx, dy, dz, (g->fp >> kFpRecSosShift) & 7u) < g->thr_sq) return CUBLOX_OK;
+  int no[3], shift[3];
+  int max_shift = 0, max_map = 0;
+  for (int a = 0; a < 3; ++a) {
+    no[a] = pos_to_global_dev(pos[a], g->res_inv, g->ctr, g->fp);
+    shift[a] = no[a] - g->origin_i[a];
+    max_shift = std::max(max_shift, std::abs(shift[a]));
+    max_map = std::max(max_map, g->map[a]);
+  }
+  if (max_shift >= max_map) {  // kernels.cu:338-347, :652-662
+    CK(cudaMemsetAsync(g->d_occ, 0, sizeof(float) * static_cast<size_t>(g->voxel_num),
+                       g->stream));
+    set_origin(g, no);
+    if (action) *action = 2;
+    return CUBLOX_OK;
+  }
+  // Slab plan (kernels.cu:355-397) as a union of marked local slots.
+  std::vector<uint32_t> masks(g->mask_words[0] + g->mask_words[1] + g->mask_words[2], 0u);
+  uint32_t *m[3] = {masks.data(), masks.data() + g->mask_words[0],
+                    masks.data() + g->mask_words[0] + g->mask_words[1]};
+  auto mark = [&](int a, int l) {
+    const int s = l + g->half[a];
+    m[a][s >> 5] |= 1u << (s & 31);
+  };
+  const bool compat = g->recenter_mode == 0;
+  bool any_z = false;
+  for (int a = 0; a < 3; ++a) {
+    const int sh = shift[a];
+    if (sh == 0) continue;
+    const int half = g->half[a];
+    const int min_l = (-half + g->origin_i[a]) % g->map[a];
+    const int n = std::min(std::abs(sh), g->map[a]);
+    if (sh > 0) {
+      for (int k = 0; k < n; ++k) mark(a, normalize_slice(min_l + k, half));
+      if (compat)
+        for (int k = 0; k < n; ++k) mark(a, normalize_slice(half - k, half));
+    } else {
+      for (int k = 1; k <= n; ++k) mark(a, normalize_slice(min_l - k, half));
+      if (compat)
+        for (int k = 0; k < n; ++k) mark(a, normalize_slice(-half + k, half));
+    }
+    if (a == 2) any_z = true;
+  }
+  const size_t mb = masks.size() * sizeof(uint32_t);
+  CK(cudaMemcpyAsync(g->d_masks, masks.data(), mb, cudaMemcpyHostToDevice, g->stream));
+  ClearParams cp{};
+  cp.occ = g->d_occ;
+  cp.xmask = g->d_masks;
+  cp.ymask = g->d_masks + g->mask_words[0];
+  cp.zmask = g->d_masks + g->mask_words[0] + g->mask_words[1];
+  for (int a = 0; a < 3; ++a) cp.map[a] = g->map[a];
+  cp.any_z = any_z ? 1 : 0;
+  tmark(g, 2, 0);
+  launch_clear(cp, g->stream);
+  CK_LAUNCH();
+  tmark(g, 2, 1);
+  // masks is a host vector: wait for the async copy before it goes away.
+  CK(cudaStreamSynchronize(g->stream));
+  set_origin(g, no);
+  if (action) *action = 1;
+  return CUBLOX_OK;
+}
+
+// ---- fetch -------------------------------------------------------------------
+namespace {
+struct QueryBox {
+  int box[8];
+  float r2;
+};
+
+// fetchOccupancyAround's host part (OccupancyGrid.cpp:244-293) for one centre:
+// the window-clipped candidate box, or an empty box.
+QueryBox plan_query(const cublox_grid *g, const float c[3], float radius) {
+  QueryBox q{};
+  q.box[0] = 0;
+  q.box[1] = -1;  // empty
+  q.box[2] = 0;
+  q.box[3] = -1;
+  q.box[4] = 0;
+  q.box[5] = -1;
+  q.r2 = 0.0f;
+  if (g->voxel_num <= 0 || radius <= 0.0f) return q;
+  int cg[3];
+  for (int a = 0; a < 3; ++a) cg[a] = host_p2g(c[a], g->res_inv, g->ctr);
+  float margin = 0.0f;
+  {
+    const int mx = g->half[0] - std::abs(cg[0] - g->origin_i[0]);
+    const int my = g->half[1] - std::abs(cg[1] - g->origin_i[1]);
+    if (mx >= 0 && my >= 0) margin = static_cast<float>(std::min(mx, my)) * g->res;
+  }
+  const float r_eff = std::min(radius, margin);
+  if (r_eff <= 0.0f) return q;
+  int gmin[3], gmax[3], wmin[3], wmax[3];
+  for (int a = 0; a < 3; ++a) {
+    wmin[a] = g->origin_i[a] - g->half[a];
+    wmax[a] = g->origin_i[a] + g->half[a];
+    gmin[a] = std::max(host_p2g(c[a] - r_eff, g->res_inv, g->ctr), wmin[a]);
+    gmax[a] = std::min(host_p2g(c[a] + r_eff, g->res_inv, g->ctr), wmax[a]);
+    if (gmax[a] < gmin[a]) return q;
+  }
+  const int disk_r = d2i_x86(std::ceil(static_cast<double>(r_eff * g->res_inv)));
+  const int nz = gmax[2] - gmin[2] + 1;
+  const int diam = 2 * disk_r + 1;
+  const int64_t est = static_cast<int64_t>(diam) * diam * nz;
+  if (est <= 0 || est > std::numeric_limits<int>::max() || disk_r < 0) return q;
+  // The reference's threads cover x, y in cg +- disk_r (plus a tail that
+  // never passes the sphere test) and z in [gmin.z, gmax.z]; its per-voxel
+  // window test is applied here as a clip.
+  q.box[0] = std::max(cg[0] - disk_r, wmin[0]);
+  q.box[1] = std::min(cg[0] + disk_r, wmax[0]);
+  q.box[2] = std::max(cg[1] - disk_r, wmin[1]);
+  q.box[3] = std::min(cg[1] + disk_r, wmax[1]);
+  q.box[4] = gmin[2];
+  q.box[5] = gmax[2];
+  q.r2 = r_eff * r_eff;
+  return q;
+}
+}  // namespace
+
+static int ensure_fq(cublox_grid *g, size_t bytes) {
+  if (bytes <= g->fq_bytes) return CUBLOX_OK;
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(g->d_fq);
+  g->d_fq = nullptr;
+  g->fq_bytes = 0;
+  if (cudaMalloc(&g->d_fq, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUBLOX_ERR_NOMEM, "fetch: query buffer allocation failed");
+  }
+  g->fq_bytes = bytes;
+  return CUBLOX_OK;
+}
+
+static int ensure_fout(cublox_grid *g, int64_t n) {
+  if (n <= g->fcap) return CUBLOX_OK;
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(g->d_fpos);
+  cudaFree(g->d_fstate);
+  g->d_fpos = nullptr;
+  g->d_fstate = nullptr;
+  g->fcap = 0;
+  if (cudaMalloc(&g->d_fpos, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess ||
+      cudaMalloc(&g->d_fstate, static_cast<size_t>(n)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUBLOX_ERR_NOMEM, "fetch: output buffer allocation failed");
+  }
+  g->fcap = n;
+  return CUBLOX_OK;
+}
+
+// Plans, counts and (if out_pos) writes.  counts_out gets the kept count per
+// query (min(count, cap) as fetchOccupancyAround returns it).
+static int fetch_impl(cublox_grid *g, const float *centers, int nq, float radius,
+                      int filter, int max_results, int64_t *kept, int64_t *offsets,
+                      float *out_pos, uint8_t *out_state, int64_t capacity,
+                      bool write) {
+  if (!g || (nq > 0 && !centers)) return fail(CUBLOX_ERR_INVALID, "fetch: null argument");
+  if (filter < -1 || filter > 2) return fail(CUBLOX_ERR_INVALID, "fetch: bad filter");
+  if (nq <= 0) {
+    if (offsets) offsets[0] = 0;
+    return CUBLOX_OK;
+  }
+  std::vector<int> boxes(8 * static_cast<size_t>(nq));
+  std::vector<float> r2(nq);
+  for (int q = 0; q < nq; ++q) {
+    const QueryBox b = plan_query(g, centers + 3 * static_cast<size_t>(q), radius);
+    std::memcpy(&boxes[8 * static_cast<size_t>(q)], b.box, sizeof(b.box));
+    r2[q] = b.r2;
+  }
+  const size_t b_cent = sizeof(float) * 3 * nq, b_box = sizeof(int) * 8 * nq,
+               b_r2 = sizeof(float) * nq, b_ll = sizeof(long long) * nq;
+  auto al = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  const size_t o_box = al(b_cent), o_r2 = o_box + al(b_box), o_cnt = o_r2 + al(b_r2),
+               o_off = o_cnt + al(b_ll), o_lim = o_off + al(b_ll), total = o_lim + al(b_ll);
+  int rc = ensure_fq(g, total);
+  if (rc) return rc;
+  char *base = static_cast<char *>(g->d_fq);
+  CK(cudaMemcpyAsync(base, centers, b_cent, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaMemcpyAsync(base + o_box, boxes.data(), b_box, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaMemcpyAsync(base + o_r2, r2.data(), b_r2, cudaMemcpyHostToDevice, g->stream));
+  FetchParams p{};
+  p.occ = g->d_occ;
+  p.centers = reinterpret_cast<const float *>(base);
+  p.qbox = reinterpret_cast<const int *>(base + o_box);
+  p.qr2 = reinterpret_cast<const float *>(base + o_r2);
+  p.nq = nq;
+  for (int a = 0; a < 3; ++a) {
+    p.win[a] = g->origin_i[a];
+    p.half[a] = g->half[a];
+    p.map[a] = g->map[a];
+  }
+  p.res = g->res;
+  p.ctr = g->ctr ? 1 : 0;
+  p.fp = g->fp;
+  p.l_free = g->l_free;
+  p.l_occ = g->l_occ;
+  p.l_unknown = g->l_unknown;
+  p.filter = filter;
+  p.counts = reinterpret_cast<long long *>(base + o_cnt);
+  p.offsets = reinterpret_cast<const long long *>(base + o_off);
+  p.limits = reinterpret_cast<const long long *>(base + o_lim);
+  p.err = g->d_err;
+  launch_fetch(p, 1, g->stream);
+  CK_LAUNCH();
+  std::vector<long long> cnt(nq), off(nq + 1), lim(nq);
+  CK(cudaMemcpyAsync(cnt.data(), p.counts, b_ll, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  const long long cap_q = max_results > 0 ? max_results : 500000;  // OccupancyGrid.cpp:292
+  off[0] = 0;
+  for (int q = 0; q < nq; ++q) {
+    lim[q] = std::min<long long>(cnt[q], cap_q);
+    off[q + 1] = off[q] + lim[q];
+    if (kept) kept[q] = lim[q];
+  }
+  if (offsets)
+    for (int q = 0; q <= nq; ++q) offsets[q] = off[q];
+  if (!write) return CUBLOX_OK;
+  const long long total_s = off[nq];
+  if (total_s > capacity)
+    return fail(CUBLOX_ERR_INVALID, "fetch: output capacity " + std::to_string(capacity) +
+                                        " < " + std::to_string(total_s) + " samples");
+  if (total_s == 0) return CUBLOX_OK;
+  rc = ensure_fout(g, total_s);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(base + o_off, off.data(), b_ll, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaMemcpyAsync(base + o_lim, lim.data(), b_ll, cudaMemcpyHostToDevice, g->stream));
+  p.out_pos = g->d_fpos;
+  p.out_state = g->d_fstate;
+  launch_fetch(p, 2, g->stream);
+  CK_LAUNCH();
+  if (out_pos)
+    CK(cudaMemcpyAsync(out_pos, g->d_fpos, sizeof(float) * 3 * static_cast<size_t>(total_s),
+                       cudaMemcpyDeviceToHost, g->stream));
+  if (out_state)
+    CK(cudaMemcpyAsync(out_state, g->d_fstate, static_cast<size_t>(total_s),
+                       cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_fetch(cublox_grid *g, const float center[3], float radius,
+                      int filter, int max_results, float *out_pos,
+                      uint8_t *out_state, int64_t capacity, int64_t *n_out) {
+  if (n_out) *n_out = 0;
+  if (!g || !center) return fail(CUBLOX_ERR_INVALID, "cublox_grid_fetch: null argument");
+  int64_t kept = 0;
+  int rc = fetch_impl(g, center, 1, radius, filter, max_results, &kept, nullptr, nullptr,
+                      nullptr, 0, false);
+  if (rc) return rc;
+  if (kept > capacity)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_fetch: capacity " + std::to_string(capacity) +
+                                        " < " + std::to_string(kept) + " samples");
+  int64_t off[2];
+  rc = fetch_impl(g, center, 1, radius, filter, max_results, nullptr, off, out_pos, out_state,
+                  capacity, true);
+  if (rc) return rc;
+  if (n_out) *n_out = off[1];
+  return CUBLOX_OK;
+}
+
+int cublox_grid_fetch_batch(cublox_grid *g, const float *centers,
+                            int n_centers, float radius, int filter,
+                            int max_results, int64_t *out_offsets,
+                            float *out_pos, uint8_t *out_state,
+                            int64_t capacity) {
+  if (!out_offsets) return fail(CUBLOX_ERR_INVALID, "fetch_batch: null offsets");
+  return fetch_impl(g, centers, n_centers, radius, filter, max_results, nullptr, out_offsets,
+                    out_pos, out_state, capacity, true);
+}
+
+int cublox_grid_fetch_counts(cublox_grid *g, const float *centers,
+                             int n_centers, float radius, int filter,
+                             int max_results, int64_t *out_counts) {
+  if (!out_counts) return fail(CUBLOX_ERR_INVALID, "fetch_counts: null output");
+  return fetch_impl(g, centers, n_centers, radius, filter, max_results, out_counts, nullptr,
+                    nullptr, nullptr, 0, false);
+}
+
+// ---- queries / state access ---------------------------------------------------
+int cublox_grid_query_states(cublox_grid *g, const float *xyz, int n,
+                             uint8_t *out_state) {
+  if (!g || (n > 0 && (!xyz || !out_state)))
+    return fail(CUBLOX_ERR_INVALID, "query_states: null argument");
+  if (n <= 0) return CUBLOX_OK;
+  if (n > g->qcap) {
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(g->d_qin);
+    cudaFree(g->d_qout);
+    g->d_qin = nullptr;
+    g->d_qout = nullptr;
+    g->qcap = 0;
+    if (cudaMalloc(&g->d_qin, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess ||
+        cudaMalloc(&g->d_qout, static_cast<size_t>(n)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "query_states: allocation failed");
+    }
+    g->qcap = n;
+  }
+  CK(cudaMemcpyAsync(g->d_qin, xyz, sizeof(float) * 3 * static_cast<size_t>(n),
+                     cudaMemcpyHostToDevice, g->stream));
+  QueryParams p{};
+  p.occ = g->d_occ;
+  p.xyz = g->d_qin;
+  p.n = n;
+  for (int a = 0; a < 3; ++a) {
+    p.win[a] = g->origin_i[a];
+    p.half[a] = g->half[a];
+    p.map[a] = g->map[a];
+  }
+  p.inv = g->res_inv;
+  p.ctr = g->ctr ? 1 : 0;
+  p.l_free = g->l_free;
+  p.l_occ = g->l_occ;
+  p.l_unknown = g->l_unknown;
+  p.out = g->d_qout;
+  launch_query(p, g->stream);
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(out_state, g->d_qout, static_cast<size_t>(n), cudaMemcpyDeviceToHost,
+                     g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_stored_at(cublox_grid *g, int hash_id, float *out) {
+  if (!g || !out) return fail(CUBLOX_ERR_INVALID, "stored_at: null argument");
+  *out = 0.0f;
+  if (hash_id < 0 || hash_id >= g->voxel_num) return CUBLOX_OK;
+  CK(cudaMemcpyAsync(out, g->d_occ + hash_id, sizeof(float), cudaMemcpyDeviceToHost,
+                     g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_origin(const cublox_grid *g, int origin_i[3], float origin_f[3]) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  for (int a = 0; a < 3; ++a) {
+    if (origin_i) origin_i[a] = g->origin_i[a];
+    if (origin_f) origin_f[a] = g->origin_f[a];
+  }
+  return CUBLOX_OK;
+}
+
+int cublox_grid_geometry(const cublox_grid *g, int map_size[3], int half[3],
+                         int *voxel_num, float *resolution,
+                         int *origin_at_center) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  for (int a = 0; a < 3; ++a) {
+    if (map_size) map_size[a] = g->map[a];
+    if (half) half[a] = g->half[a];
+  }
+  if (voxel_num) *voxel_num = g->voxel_num;
+  if (resolution) *resolution = g->res;
+  if (origin_at_center) *origin_at_center = g->ctr ? 1 : 0;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_first_run(const cublox_grid *g, int *first_run) {
+  if (!g || !first_run) return fail(CUBLOX_ERR_INVALID, "null argument");
+  *first_run = g->first_run ? 1 : 0;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_set_origin_index(cublox_grid *g, const int origin_i[3]) {
+  if (!g || !origin_i) return fail(CUBLOX_ERR_INVALID, "null argument");
+  set_origin(g, origin_i);
+  g->first_run = false;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_export(cublox_grid *g, float *occ_host) {
+  if (!g || !occ_host) return fail(CUBLOX_ERR_INVALID, "export: null argument");
+  CK(cudaMemcpyAsync(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->voxel_num),
+                     cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_import(cublox_grid *g, const float *occ_host) {
+  if (!g || !occ_host) return fail(CUBLOX_ERR_INVALID, "import: null argument");
+  CK(cudaMemcpyAsync(g->d_occ, occ_host, sizeof(float) * static_cast<size_t>(g->voxel_num),
+                     cudaMemcpyHostToDevice, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_stream(const cublox_grid *g, void **stream) {
+  if (!g || !stream) return fail(CUBLOX_ERR_INVALID, "null argument");
+  *stream = g->stream;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_synchronize(cublox_grid *g) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+int cublox_grid_enable_stats(cublox_grid *g, int enable) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  g->stats_on = enable != 0;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_last_stats(cublox_grid *g, cublox_scan_stats *out) {
+  if (!g || !out) return fail(CUBLOX_ERR_INVALID, "null argument");
+  unsigned long long v[4];
+  CK(cudaMemcpyAsync(v, g->d_stats, sizeof(v), cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  out->rays = static_cast<int64_t>(v[0]);
+  out->op_incs = static_cast<int64_t>(v[1]);
+  out->hit_incs = static_cast<int64_t>(v[2]);
+  out->touched = static_cast<int64_t>(v[3]);
+  return CUBLOX_OK;
+}
+
+int cublox_grid_count_scan(cublox_grid *g, const float *xyz, int n,
+                           const float sensor_origin[3], int32_t *op_out,
+                           int32_t *hit_out) {
+  if (!g || !sensor_origin || !op_out || !hit_out || (n > 0 && !xyz))
+    return fail(CUBLOX_ERR_INVALID, "count_scan: null argument");
+  const size_t vb = sizeof(uint32_t) * static_cast<size_t>(g->voxel_num);
+  if (n > 0) {
+    int rc = ensure_cloud(g, n);
+    if (rc) return rc;
+    std::vector<float> soa(3 * static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a)
+        soa[a * static_cast<size_t>(n) + i] = xyz[3 * static_cast<size_t>(i) + a];
+    CK(cudaMemcpyAsync(g->d_cloud, soa.data(), soa.size() * sizeof(float),
+                       cudaMemcpyHostToDevice, g->stream));
+    rc = integrate(g, g->d_cloud, g->d_cloud + n, g->d_cloud + 2 * static_cast<size_t>(n), n,
+                   1, sensor_origin, true);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(g->stream));
+  }
+  std::vector<uint32_t> c(g->voxel_num);
+  CK(cudaMemcpyAsync(c.data(), g->d_cnt, vb, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaMemcpyAsync(hit_out, g->d_hit, vb, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaMemsetAsync(g->d_cnt, 0, vb, g->stream));
+  CK(cudaMemsetAsync(g->d_hit, 0, vb, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  for (int h = 0; h < g->voxel_num; ++h) {
+    op_out[h] = static_cast<int32_t>(c[h] & kOpMask);
+    if (!(c[h] & kHitFlag)) hit_out[h] = 0;
+  }
+  return CUBLOX_OK;
+}
+
+int cublox_grid_enable_timing(cublox_grid *g, int enable) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  if (enable)
+    for (int i = 0; i < 6; ++i)
+      if (!g->tev[i]) CK(cudaEventCreate(&g->tev[i]));
+  g->timing_on = enable != 0;
+  for (int i = 0; i < 3; ++i) g->tev_used[i] = false;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_last_timing(cublox_grid *g, float ms[3]) {
+  if (!g || !ms) return fail(CUBLOX_ERR_INVALID, "null argument");
+  CK(cudaStreamSynchronize(g->stream));
+  for (int i = 0; i < 3; ++i) {
+    ms[i] = -1.0f;
+    if (g->timing_on && g->tev_used[i])
+      CK(cudaEventElapsedTime(&ms[i], g->tev[2 * i], g->tev[2 * i + 1]));
+    g->tev_used[i] = false;
+  }
+  return CUBLOX_OK;
+}
+
+int cublox_grid_reference_steps(cublox_grid *g, const float *xyz, int n,
+                                const float sensor_origin[3], int64_t *voxel_steps) {
+  if (!g || !sensor_origin || !voxel_steps || (n > 0 && !xyz))
+    return fail(CUBLOX_ERR_INVALID, "reference_steps: null argument");
+  *voxel_steps = 0;
+  if (n <= 0) return CUBLOX_OK;
+  int rc = ensure_cloud(g, n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(g->d_cloud, xyz, sizeof(float) * 3 * static_cast<size_t>(n),
+                     cudaMemcpyHostToDevice, g->stream));
+  CK(cudaMemsetAsync(g->d_stats, 0, 4 * sizeof(unsigned long long), g->stream));
+  RayParams p{};
+  p.x = g->d_cloud;
+  p.y = g->d_cloud + 1;
+  p.z = g->d_cloud + 2;
+  p.n = n;
+  p.stride = 3;
+  for (int a = 0; a < 3; ++a) {
+    p.o[a] = sensor_origin[a];
+    p.win[a] = g->origin_i[a];
+    p.half[a] = g->half[a];
+    p.map[a] = g->map[a];
+  }
+  p.res = g->res;
+  p.inv = g->res_inv;
+  p.max_range = g->max_range;
+  p.vnum = g->voxel_num;
+  p.ctr = g->ctr ? 1 : 0;
+  p.fp = g->fp;
+  p.stats = g->d_stats;
+  p.err = g->d_err;
+  launch_step_count(p, g->stream);
+  CK_LAUNCH();
+  unsigned long long v[4];
+  CK(cudaMemcpyAsync(v, g->d_stats, sizeof(v), cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  *voxel_steps = static_cast<int64_t>(v[0]);
+  return CUBLOX_OK;
+}
+
+int cublox_grid_check(cublox_grid *g, uint32_t *error_word) {
+  if (!g || !error_word) return fail(CUBLOX_ERR_INVALID, "null argument");
+  CK(cudaMemcpyAsync(error_word, g->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                     g->stream));
+  CK(cudaMemsetAsync(g->d_err, 0, sizeof(uint32_t), g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  return CUBLOX_OK;
+}
+
+}  // extern "C"

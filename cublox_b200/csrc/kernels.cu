@@ -1,0 +1,498 @@
+// Device kernels of the map-integration path (sm_100a).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace cublox_b200 {
+
+namespace {
+
+__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
+
+__device__ __forceinline__ int wrap_slot(int s, int map) {
+  return s >= map ? s - map : (s < 0 ? s + map : s);
+}
+
+__device__ __forceinline__ bool inside(int r, int h) { return abs(r) <= h; }
+
+// One ray, op for op as rayCastUpdateKernel (kernels.cu:44-151), with the
+// window test and hash kept incrementally and the walk cut short once the
+// ray has left the window for good (indices are monotone per axis, so no
+// later voxel of the loop can be inside).  Returns false if dropped.
+// kAccount: count the reference loop's iterations instead (no early exit,
+// no counters touched); u_incs gets iterations + 1.
+template <bool kAccount = false>
+__device__ __forceinline__ bool cast_one(const RayParams &p, float ex,
+                                         float ey, float ez, uint32_t &u_incs,
+                                         uint32_t &h_incs) {
+  const float ox = p.o[0], oy = p.o[1], oz = p.o[2];
+  float dx = fsub(ex, ox), dy = fsub(ey, oy), dz = fsub(ez, oz);
+  float L = fsqrt(sos(dx, dy, dz, (p.fp >> kFpRaySosShift) & 7u));
+  if (L < 1e-6f || !isfinite(L) || !isfinite(ex) || !isfinite(ey) ||
+      !isfinite(ez))
+    return false;
+  const bool clipped = L > p.max_range;
+  if (clipped) {
+    const float s = fdiv(p.max_range, L);
+    if (p.fp & kFpClipFma) {
+      ex = ffma(dx, s, ox);
+      ey = ffma(dy, s, oy);
+      ez = ffma(dz, s, oz);
+    } else {
+      ex = fadd(ox, fmul(dx, s));
+      ey = fadd(oy, fmul(dy, s));
+      ez = fadd(oz, fmul(dz, s));
+    }
+    dx = fmul(dx, s);
+    dy = fmul(dy, s);
+    dz = fmul(dz, s);
+    L = p.max_range;
+  }
+  const float invL = fdiv(1.0f, L);
+  const float u[3] = {fmul(dx, invL), fmul(dy, invL), fmul(dz, invL)};
+  const float oo[3] = {ox, oy, oz};
+  const float ee[3] = {ex, ey, ez};
+  const bool ctr = p.ctr != 0;
+  int id[3], en[3], st[3], rel[3], slot[3];
+  float tD[3], tM[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    id[a] = pos_to_global_dev(oo[a], p.inv, ctr, p.fp);
+    en[a] = pos_to_global_dev(ee[a], p.inv, ctr, p.fp);
+    st[a] = (u[a] > 0.0f) - (u[a] < 0.0f);
+    tD[a] = st[a] == 0 ? inf_f() : fabsf(fdiv(p.res, u[a]));
+    float t;
+    if (ctr) {
+      t = fadd(static_cast<float>(id[a]), fmul(0.5f, static_cast<float>(st[a])));
+    } else {
+      t = fadd(static_cast<float>(id[a]), static_cast<float>(st[a] > 0));
+    }
+    const float num = (p.fp & kFpBoundFma) ? ffma(t, p.res, -oo[a])
+                                           : fsub(fmul(t, p.res), oo[a]);
+    tM[a] = st[a] == 0 ? inf_f() : fdiv(num, u[a]);
+    rel[a] = id[a] - p.win[a];
+    slot[a] = global_to_local(id[a], p.map[a], p.half[a]) + p.half[a];
+  }
+  const int max_steps = abs(en[0] - id[0]) + abs(en[1] - id[1]) +
+                        abs(en[2] - id[2]) + 4;
+  const int ny = p.map[1], nz = p.map[2];
+  uint32_t incs = 0;
+  for (int step = 0; step < max_steps; ++step) {
+    if (id[0] == en[0] && id[1] == en[1] && id[2] == en[2]) break;
+    if (kAccount) {
+      ++incs;
+    } else {
+    const bool in0 = inside(rel[0], p.half[0]);
+    const bool in1 = inside(rel[1], p.half[1]);
+    const bool in2 = inside(rel[2], p.half[2]);
+    if (in0 && in1 && in2) {
+      const int h = (slot[0] * ny + slot[1]) * nz + slot[2];
+      if (static_cast<unsigned>(h) < static_cast<unsigned>(p.vnum)) {
+        atomicAdd(p.cnt + h, 1u);
+        ++incs;
+      } else {
+        atomicOr(p.err, kErrHashRange);
+      }
+    } else {
+      // Outside on some axis and not moving back: nothing left to count.
+      if ((!in0 && rel[0] * st[0] >= 0) || (!in1 && rel[1] * st[1] >= 0) ||
+          (!in2 && rel[2] * st[2] >= 0))
+        break;
+    }
+    }
+    int a;
+    if (tM[0] < tM[1]) {
+      a = tM[0] < tM[2] ? 0 : 2;
+    } else {
+      a = tM[1] < tM[2] ? 1 : 2;
+    }
+    // Select-by-index keeps the three axes in registers.
+    if (a == 0) {
+      id[0] += st[0];
+      rel[0] += st[0];
+      slot[0] = wrap_slot(slot[0] + st[0], p.map[0]);
+      tM[0] = fadd(tM[0], tD[0]);
+    } else if (a == 1) {
+      id[1] += st[1];
+      rel[1] += st[1];
+      slot[1] = wrap_slot(slot[1] + st[1], p.map[1]);
+      tM[1] = fadd(tM[1], tD[1]);
+    } else {
+      id[2] += st[2];
+      rel[2] += st[2];
+      slot[2] = wrap_slot(slot[2] + st[2], p.map[2]);
+      tM[2] = fadd(tM[2], tD[2]);
+    }
+  }
+  if (kAccount) {
+    u_incs += incs + 1;
+    return true;
+  }
+  // Endpoint: op, and hit unless clipped (kernels.cu:139-151).
+  if (inside(en[0] - p.win[0], p.half[0]) &&
+      inside(en[1] - p.win[1], p.half[1]) &&
+      inside(en[2] - p.win[2], p.half[2])) {
+    const int h = ((global_to_local(en[0], p.map[0], p.half[0]) + p.half[0]) *
+                       ny +
+                   (global_to_local(en[1], p.map[1], p.half[1]) + p.half[1])) *
+                      nz +
+                  (global_to_local(en[2], p.map[2], p.half[2]) + p.half[2]);
+    if (static_cast<unsigned>(h) < static_cast<unsigned>(p.vnum)) {
+      if (clipped) {
+        atomicAdd(p.cnt + h, 1u);
+      } else {
+        atomicAdd(p.cnt + h, 1u);
+        atomicOr(p.cnt + h, kHitFlag);
+        atomicAdd(p.hit + h, 1u);
+        ++h_incs;
+      }
+      ++incs;
+    } else {
+      atomicOr(p.err, kErrHashRange);
+    }
+  }
+  u_incs += incs;
+  return true;
+}
+
+template <bool kStats>
+__global__ void __launch_bounds__(256) raycast_kernel(const RayParams p) {
+  uint32_t rays = 0, u = 0, hh = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
+       i += gridDim.x * blockDim.x) {
+    const size_t k = static_cast<size_t>(i) * p.stride;
+    if (cast_one(p, p.x[k], p.y[k], p.z[k], u, hh)) ++rays;
+  }
+  if (kStats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      rays += __shfl_down_sync(0xffffffffu, rays, off);
+      u += __shfl_down_sync(0xffffffffu, u, off);
+      hh += __shfl_down_sync(0xffffffffu, hh, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(p.stats + 0, static_cast<unsigned long long>(rays));
+      atomicAdd(p.stats + 1, static_cast<unsigned long long>(u));
+      atomicAdd(p.stats + 2, static_cast<unsigned long long>(hh));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) step_count_kernel(const RayParams p) {
+  uint32_t it = 0, hh = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
+       i += gridDim.x * blockDim.x) {
+    const size_t k = static_cast<size_t>(i) * p.stride;
+    cast_one<true>(p, p.x[k], p.y[k], p.z[k], it, hh);
+  }
+  unsigned long long v = it;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(p.stats, v);
+}
+
+// Fold one voxel's counters (applyUpdateKernel, kernels.cu:179-200).
+__device__ __forceinline__ void fold(const ApplyParams &p, int h, uint32_t c) {
+  const int op = static_cast<int>(c & kOpMask);
+  int hit = 0;
+  if (c & kHitFlag) {
+    hit = static_cast<int>(p.hit[h]);
+    p.hit[h] = 0u;
+  }
+  const int miss = op > hit ? op - hit : 0;
+  const float s0 = p.occ[h];
+  float l = fadd(s0, p.l_unknown);
+  l = (p.fp & kFpMissFma) ? ffma(p.l_miss, static_cast<float>(miss), l)
+                          : fadd(l, fmul(p.l_miss, static_cast<float>(miss)));
+  l = (p.fp & kFpHitFma) ? ffma(p.l_hit, static_cast<float>(hit), l)
+                         : fadd(l, fmul(p.l_hit, static_cast<float>(hit)));
+  if (l < p.l_min) l = p.l_min;
+  if (l > p.l_max) l = p.l_max;
+  p.occ[h] = fsub(l, p.l_unknown);
+}
+
+template <bool kStats>
+__global__ void __launch_bounds__(256) apply_sweep_kernel(const ApplyParams p) {
+  const int n4 = p.vnum >> 2;
+  uint32_t touched = 0;
+  uint4 *c4 = reinterpret_cast<uint4 *>(p.cnt);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+       i += gridDim.x * blockDim.x) {
+    const uint4 c = c4[i];
+    if ((c.x | c.y | c.z | c.w) == 0u) continue;
+    const int h = i << 2;
+    if (c.x) { fold(p, h + 0, c.x); ++touched; }
+    if (c.y) { fold(p, h + 1, c.y); ++touched; }
+    if (c.z) { fold(p, h + 2, c.z); ++touched; }
+    if (c.w) { fold(p, h + 3, c.w); ++touched; }
+    c4[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  // tail (vnum not a multiple of 4)
+  if (blockIdx.x == 0 && threadIdx.x < (p.vnum & 3)) {
+    const int h = (n4 << 2) + threadIdx.x;
+    const uint32_t c = p.cnt[h];
+    if (c) {
+      fold(p, h, c);
+      p.cnt[h] = 0u;
+      ++touched;
+    }
+  }
+  if (kStats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      touched += __shfl_down_sync(0xffffffffu, touched, off);
+    if ((threadIdx.x & 31) == 0 && touched)
+      atomicAdd(p.stats + 3, static_cast<unsigned long long>(touched));
+  }
+}
+
+// Union-of-slabs clear.  One block per x slot: a marked x slab is one
+// contiguous run of ny*nz floats; otherwise every (x, y) column clears its
+// whole run if y is marked, else the marked z slots.
+__global__ void __launch_bounds__(256) clear_kernel(const ClearParams p) {
+  extern __shared__ uint32_t sm[];
+  const int nx = p.map[0], ny = p.map[1], nz = p.map[2];
+  const int wy = (ny + 31) >> 5, wz = (nz + 31) >> 5;
+  uint32_t *my = sm;
+  int *zl = reinterpret_cast<int *>(sm + wy);
+  __shared__ int nzl;
+  for (int i = threadIdx.x; i < wy; i += blockDim.x) my[i] = p.ymask[i];
+  if (threadIdx.x == 0) {
+    int c = 0;
+    if (p.any_z)
+      for (int w = 0; w < wz; ++w) {
+        uint32_t b = p.zmask[w];
+        while (b) {
+          const int k = __ffs(b) - 1;
+          b &= b - 1;
+          zl[c++] = w * 32 + k;
+        }
+      }
+    nzl = c;
+  }
+  __syncthreads();
+  for (int lx = blockIdx.x; lx < nx; lx += gridDim.x) {
+    float *base = p.occ + static_cast<size_t>(lx) * ny * nz;
+    if ((p.xmask[lx >> 5] >> (lx & 31)) & 1u) {
+      const int n = ny * nz;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) base[i] = 0.0f;
+      continue;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    for (int ly = warp; ly < ny; ly += nw) {
+      float *col = base + static_cast<size_t>(ly) * nz;
+      if ((my[ly >> 5] >> (ly & 31)) & 1u) {
+        for (int z = lane; z < nz; z += 32) col[z] = 0.0f;
+      } else {
+        for (int k = lane; k < nzl; k += 32) col[zl[k]] = 0.0f;
+      }
+    }
+  }
+}
+
+// Sphere fetch over host-clipped candidate boxes, one block per query
+// (grid-stride), candidates in (x, y, z) order with z fastest so that
+// consecutive threads read consecutive voxels of one column.  Pass 1 counts,
+// pass 2 writes the first `limits[q]` samples at `offsets[q]` in that order.
+template <int kPass>
+__global__ void __launch_bounds__(256) fetch_kernel(const FetchParams p) {
+  __shared__ int warp_tot[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = blockIdx.x; q < p.nq; q += gridDim.x) {
+    const int *b = p.qbox + 8 * q;
+    const int gx0 = b[0], gy0 = b[2], gz0 = b[4];
+    const int nx = b[1] - b[0] + 1, nyy = b[3] - b[2] + 1, nzz = b[5] - b[4] + 1;
+    const float c[3] = {p.centers[3 * q], p.centers[3 * q + 1],
+                        p.centers[3 * q + 2]};
+    const float r2 = p.qr2[q];
+    long long running = 0;
+    const long long limit = kPass == 2 ? p.limits[q] : 0;
+    const long long base_off = kPass == 2 ? p.offsets[q] : 0;
+    const long long total = (nx > 0 && nyy > 0 && nzz > 0)
+                                ? static_cast<long long>(nx) * nyy * nzz
+                                : 0;
+    for (long long t0 = 0; t0 < total; t0 += blockDim.x) {
+      if (kPass == 2 && running >= limit) break;
+      const long long t = t0 + threadIdx.x;
+      bool keep = false;
+      float pos[3];
+      uint8_t state = 0;
+      if (t < total) {
+        const int iz = static_cast<int>(t % nzz);
+        const long long r = t / nzz;
+        const int iy = static_cast<int>(r % nyy);
+        const int ix = static_cast<int>(r / nyy);
+        const int g[3] = {gx0 + ix, gy0 + iy, gz0 + iz};
+        float d[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float tt = p.ctr ? static_cast<float>(g[a])
+                                 : fadd(static_cast<float>(g[a]), 0.5f);
+          pos[a] = fmul(tt, p.res);
+          d[a] = (p.fp & kFpFetchDFma) ? ffma(tt, p.res, -c[a])
+                                       : fsub(pos[a], c[a]);
+        }
+        const float s = sos(d[0], d[1], d[2], (p.fp >> kFpFetchSosShift) & 7u);
+        if (!(s > r2)) {
+          const int h =
+              ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) *
+                   p.map[1] +
+               (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
+                  p.map[2] +
+              (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+          const float l = fadd(p.occ[h], p.l_unknown);
+          state = l >= p.l_occ ? 2 : (l < p.l_free ? 1 : 0);
+          keep = p.filter < 0 || static_cast<int>(state) == p.filter;
+        }
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) warp_tot[warp] = __popc(bal);
+      __syncthreads();
+      int before = 0, blk = 0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) {
+        const int v = warp_tot[w];
+        before += w < warp ? v : 0;
+        blk += v;
+      }
+      if (kPass == 2 && keep) {
+        const long long rank =
+            running + before + __popc(bal & ((1u << lane) - 1u));
+        if (rank < limit) {
+          const long long o = base_off + rank;
+          p.out_pos[3 * o + 0] = pos[0];
+          p.out_pos[3 * o + 1] = pos[1];
+          p.out_pos[3 * o + 2] = pos[2];
+          p.out_state[o] = state;
+        }
+      }
+      running += blk;
+      __syncthreads();
+    }
+    if (kPass == 1 && threadIdx.x == 0) p.counts[q] = running;
+  }
+}
+
+// Host-side float->int of the reference's point queries (x86 cvttss2si:
+// NaN or out of range gives INT_MIN).
+__device__ __forceinline__ int f2i_hostlike(float v) {
+  return (v >= -2147483648.0f && v < 2147483648.0f) ? static_cast<int>(v)
+                                                    : (-2147483647 - 1);
+}
+
+__global__ void __launch_bounds__(256) query_kernel(const QueryParams p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
+       i += gridDim.x * blockDim.x) {
+    int g[3];
+    bool in = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = p.xyz[3 * static_cast<size_t>(i) + a];
+      const float m = fmul(v, p.inv);
+      g[a] = p.ctr ? f2i_hostlike(fadd(m, v < 0.0f ? -0.5f : 0.5f))
+                   : f2i_hostlike(ffloor(m));
+      in = in && abs(g[a] - p.win[a]) <= p.half[a];
+    }
+    uint8_t st = 0;
+    if (in) {
+      const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) *
+                         p.map[1] +
+                     (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
+                        p.map[2] +
+                    (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+      const float l = fadd(p.occ[h], p.l_unknown);
+      st = l >= p.l_occ ? 2 : (l < p.l_free ? 1 : 0);
+    }
+    p.out[i] = st;
+  }
+}
+
+__global__ void gather_soa_kernel(const float *xyz, int layout, int n,
+                                  float *dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    if (layout == 1) {
+      dst[i] = xyz[3 * static_cast<size_t>(i)];
+      dst[n + i] = xyz[3 * static_cast<size_t>(i) + 1];
+      dst[2 * static_cast<size_t>(n) + i] = xyz[3 * static_cast<size_t>(i) + 2];
+    }
+  }
+}
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+}  // namespace
+
+void launch_raycast(const RayParams &p, cudaStream_t s) {
+  if (p.n <= 0) return;
+  const int block = 256;
+  int grid = (p.n + block - 1) / block;
+  if (p.stats)
+    raycast_kernel<true><<<grid, block, 0, s>>>(p);
+  else
+    raycast_kernel<false><<<grid, block, 0, s>>>(p);
+}
+
+void launch_step_count(const RayParams &p, cudaStream_t s) {
+  if (p.n <= 0) return;
+  step_count_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(p);
+}
+
+void launch_apply(const ApplyParams &p, cudaStream_t s) {
+  if (p.vnum <= 0) return;
+  const int block = 256;
+  const int n4 = (p.vnum >> 2) + 1;
+  int grid = (n4 + block - 1) / block;
+  const int cap = sm_count() * 16;
+  if (grid > cap) grid = cap;
+  if (p.stats)
+    apply_sweep_kernel<true><<<grid, block, 0, s>>>(p);
+  else
+    apply_sweep_kernel<false><<<grid, block, 0, s>>>(p);
+}
+
+void launch_clear(const ClearParams &p, cudaStream_t s) {
+  const int wy = (p.map[1] + 31) >> 5;
+  const size_t smem = sizeof(uint32_t) * wy + sizeof(int) * (p.map[2] + 1);
+  int grid = p.map[0];
+  clear_kernel<<<grid, 256, smem, s>>>(p);
+}
+
+void launch_fetch(const FetchParams &p, int pass, cudaStream_t s) {
+  if (p.nq <= 0) return;
+  int grid = p.nq;
+  const int cap = sm_count() * 8;
+  if (grid > cap) grid = cap;
+  if (pass == 1)
+    fetch_kernel<1><<<grid, 256, 0, s>>>(p);
+  else
+    fetch_kernel<2><<<grid, 256, 0, s>>>(p);
+}
+
+void launch_query(const QueryParams &p, cudaStream_t s) {
+  if (p.n <= 0) return;
+  int grid = (p.n + 255) / 256;
+  query_kernel<<<grid, 256, 0, s>>>(p);
+}
+
+void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
+                       cudaStream_t s) {
+  if (n <= 0) return;
+  int grid = (n + 255) / 256;
+  gather_soa_kernel<<<grid, 256, 0, s>>>(xyz, layout, n, dst);
+}
+
+}  // namespace cublox_b200

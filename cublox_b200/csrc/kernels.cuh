@@ -1,0 +1,99 @@
+// Device kernels of the map-integration path.
+//
+// Grid storage (one map):
+//   occ  float[V]     stored log-odds, the reference's ring-buffer hash order
+//                     h = ((lx+hx)*ny + (ly+hy))*nz + (lz+hz)  (utils.cuh:131)
+//   cnt  uint32[V]    per-scan traversal count (bits 0..30) and a "has hit"
+//                     flag (bit 31); zero between scans
+//   hit  uint32[V]    per-scan endpoint-hit count, read only where flagged
+#pragma once
+
+#include <cstdint>
+
+#include "exact_fp.cuh"
+
+namespace cublox_b200 {
+
+constexpr uint32_t kHitFlag = 0x80000000u;
+constexpr uint32_t kOpMask = 0x7fffffffu;
+
+// Error-word bits (never expected; set instead of trapping).
+constexpr uint32_t kErrHashRange = 1u << 0;
+constexpr uint32_t kErrFetchOverflow = 1u << 1;
+
+struct RayParams {
+  const float *x, *y, *z;  // point i is (x[i*stride], y[i*stride], z[i*stride])
+  int n;
+  int stride;
+  float o[3];       // sensor origin (world)
+  int win[3];       // sliding-window origin (global voxel index)
+  int half[3], map[3];
+  float res, inv, max_range;
+  int vnum;
+  int ctr;
+  unsigned fp;
+  uint32_t *cnt;
+  uint32_t *hit;
+  unsigned long long *stats;  // [rays, op_incs, hit_incs] or null
+  uint32_t *err;
+};
+
+struct ApplyParams {
+  float *occ;
+  uint32_t *cnt;
+  uint32_t *hit;
+  int vnum;
+  float l_hit, l_miss, l_min, l_max, l_unknown;
+  unsigned fp;
+  unsigned long long *stats;  // [3] += touched
+};
+
+struct ClearParams {
+  float *occ;
+  const uint32_t *xmask, *ymask, *zmask;  // bit per local slab slot
+  int map[3];
+  int any_z;
+};
+
+struct FetchParams {
+  const float *occ;
+  const float *centers;  // 3 per query
+  const int *qbox;       // 8 ints per query: gx0 gx1 gy0 gy1 gz0 gz1 pad pad
+  const float *qr2;      // radius_sq per query
+  int nq;
+  int win[3], half[3], map[3];
+  float res;
+  int ctr;
+  unsigned fp;
+  float l_free, l_occ, l_unknown;
+  int filter;
+  long long *counts;         // pass 1 output: samples per query
+  const long long *offsets;  // pass 2 input: exclusive scan of kept counts
+  const long long *limits;   // pass 2: samples to keep per query
+  float *out_pos;
+  uint8_t *out_state;
+  uint32_t *err;
+};
+
+struct QueryParams {
+  const float *occ;
+  const float *xyz;
+  int n;
+  int win[3], half[3], map[3];
+  float inv;
+  int ctr;
+  float l_free, l_occ, l_unknown;
+  uint8_t *out;
+};
+
+void launch_raycast(const RayParams &p, cudaStream_t s);
+// Accounting: stats[0] += the reference loop's iterations + 1 per ray.
+void launch_step_count(const RayParams &p, cudaStream_t s);
+void launch_apply(const ApplyParams &p, cudaStream_t s);
+void launch_clear(const ClearParams &p, cudaStream_t s);
+void launch_fetch(const FetchParams &p, int pass, cudaStream_t s);
+void launch_query(const QueryParams &p, cudaStream_t s);
+void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
+                       cudaStream_t s);
+
+}  // namespace cublox_b200

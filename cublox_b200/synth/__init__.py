@@ -1,0 +1,247 @@
+"""Seeded synthetic LiDAR scenes, scans and trajectories.
+
+Inputs for the parity tests and the benchmark.  The reference's own input (a
+recorded LiDAR bag) is not available, so scans are ray-cast from a seeded
+scene: the ground plane z = 0 plus axis-aligned boxes standing on it.
+
+Per-scan recipe (shared by every configuration):
+  * beams at evenly spaced elevations, azimuths evenly spaced over 360 deg,
+    rotated by the sensor yaw; points ordered azimuth-major (all beams of one
+    azimuth, then the next), as a spinning LiDAR reports them;
+  * the true hit range gets Gaussian noise N(0, sigma);
+  * a return whose noisy range exceeds max_range, or a beam that hits
+    nothing, becomes a "no-return" endpoint at 1.5 x max_range along the
+    beam, which the reference's clip path integrates as free space only
+    (src/kernels.cu:57-67);
+  * points are world-frame float32, sensor at the given pose.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libcublox_synth.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the C ray caster next to this file (gcc, no GPU needed)."""
+    src = os.path.join(_HERE, "scan_synth.c")
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < os.path.getmtime(src)
+    ):
+        import subprocess
+
+        subprocess.check_call(
+            ["gcc", "-O2", "-fPIC", "-shared", "-o", _LIB_PATH, src, "-lm", "-lpthread"]
+        )
+    return _LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        lib = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.synth_cast.argtypes = [dp, dp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+        lib.synth_cast.restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclass
+class Scene:
+    boxes: np.ndarray  # (B, 6) float64: xmin, ymin, zmin, xmax, ymax, zmax
+    ground: bool = True
+
+
+def make_scene(seed: int, n_boxes: int, extent: float, side=(0.3, 3.0), height=None,
+               keepout=None) -> Scene:
+    """Boxes with centres uniform in +-extent (x, y), base on the ground.
+
+    `side` bounds the x/y/z side lengths (uniform); `height`, if given,
+    bounds the z side separately.  `keepout(cx, cy, hx, hy) -> bool` rejects
+    boxes (resampled) that would sit on the sensor's path.
+    """
+    rng = np.random.default_rng(seed)
+    boxes = []
+    tries = 0
+    while len(boxes) < n_boxes and tries < 100 * max(n_boxes, 1):
+        tries += 1
+        cx, cy = rng.uniform(-extent, extent, size=2)
+        sx, sy = rng.uniform(side[0], side[1], size=2)
+        sz = rng.uniform(height[0], height[1]) if height else rng.uniform(side[0], side[1])
+        if keepout is not None and keepout(cx, cy, sx / 2, sy / 2):
+            continue
+        boxes.append([cx - sx / 2, cy - sy / 2, 0.0, cx + sx / 2, cy + sy / 2, sz])
+    return Scene(np.asarray(boxes, dtype=np.float64).reshape(-1, 6))
+
+
+@dataclass
+class Sensor:
+    beams: int
+    azimuths: int
+    elev_min_deg: float
+    elev_max_deg: float
+    max_range: float
+    sigma: float
+
+    @property
+    def n_points(self) -> int:
+        return self.beams * self.azimuths
+
+    def directions(self, yaw: float = 0.0) -> np.ndarray:
+        el = np.deg2rad(np.linspace(self.elev_min_deg, self.elev_max_deg, self.beams))
+        az = yaw + 2.0 * np.pi * np.arange(self.azimuths) / self.azimuths
+        ce, se = np.cos(el), np.sin(el)
+        ca, sa = np.cos(az), np.sin(az)
+        d = np.empty((self.azimuths, self.beams, 3), dtype=np.float64)
+        d[..., 0] = ca[:, None] * ce[None, :]
+        d[..., 1] = sa[:, None] * ce[None, :]
+        d[..., 2] = se[None, :]
+        return d.reshape(-1, 3)
+
+
+def cast(scene: Scene, origin, dirs: np.ndarray, threads: int | None = None) -> np.ndarray:
+    lib = _load()
+    o = np.ascontiguousarray(np.asarray(origin, dtype=np.float64))
+    d = np.ascontiguousarray(dirs, dtype=np.float64)
+    b = np.ascontiguousarray(scene.boxes, dtype=np.float64)
+    out = np.empty(d.shape[0], dtype=np.float64)
+    th = threads or min(8, os.cpu_count() or 1)
+    rc = lib.synth_cast(_dp(o), _dp(d), d.shape[0], _dp(b), b.shape[0], int(scene.ground), _dp(out), th)
+    if rc != 0:
+        raise RuntimeError("synth_cast failed")
+    return out
+
+
+def scan(scene: Scene, sensor: Sensor, origin, yaw: float, seed: int) -> np.ndarray:
+    """One scan: (N, 3) float32 world-frame points."""
+    dirs = sensor.directions(yaw)
+    t = cast(scene, origin, dirs)
+    rng = np.random.default_rng(seed)
+    r = t + rng.normal(0.0, sensor.sigma, size=t.shape)
+    no_ret = ~np.isfinite(t) | (r > sensor.max_range)
+    r = np.where(no_ret, 1.5 * sensor.max_range, np.maximum(r, 1e-3))
+    pts = np.asarray(origin, dtype=np.float64)[None, :] + r[:, None] * dirs
+    return pts.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Trajectories
+# ---------------------------------------------------------------------------
+def circle_trajectory(n: int, radius: float, speed: float, rate_hz: float, height: float):
+    """Poses (x, y, z, yaw) on a circle about the origin, starting at (R, 0)."""
+    dth = speed / rate_hz / radius
+    th = dth * np.arange(n)
+    x = radius * np.cos(th)
+    y = radius * np.sin(th)
+    yaw = th + np.pi / 2
+    return np.stack([x, y, np.full(n, height), yaw], axis=1)
+
+
+def line_trajectory(n: int, speed: float, rate_hz: float, height: float, start=(0.0, 0.0),
+                    heading: float = 0.0):
+    step = speed / rate_hz
+    s = step * np.arange(n)
+    x = start[0] + s * np.cos(heading)
+    y = start[1] + s * np.sin(heading)
+    return np.stack([x, y, np.full(n, height), np.full(n, heading)], axis=1)
+
+
+# ---------------------------------------------------------------------------
+# The five workloads (log-odds from the reference's yaml defaults).
+# ---------------------------------------------------------------------------
+YAML_PROBS = dict(hit=0.9, miss=0.49, min=0.12, max=0.98, free=0.499, occupied=0.85)
+
+
+@dataclass
+class Workload:
+    name: str
+    half: tuple
+    resolution: float
+    sensor: Sensor
+    scene: Scene
+    poses: np.ndarray
+    threshold: float | None
+    seed: int
+    fetch_centres: int = 0
+    fetch_radius: float = 0.0
+    extra: dict = field(default_factory=dict)
+
+    def scan(self, k: int) -> np.ndarray:
+        x, y, z, yaw = self.poses[k]
+        return scan(self.scene, self.sensor, (x, y, z), yaw, seed=self.seed * 100003 + k)
+
+    def sensor_origin(self, k: int) -> np.ndarray:
+        return np.asarray(self.poses[k][:3], dtype=np.float32)
+
+
+def _keepout_point(px, py, margin):
+    def f(cx, cy, hx, hy):
+        return abs(cx - px) < hx + margin and abs(cy - py) < hy + margin
+    return f
+
+
+def _keepout_circle(radius, margin):
+    def f(cx, cy, hx, hy):
+        r = np.hypot(cx, cy)
+        return abs(r - radius) < np.hypot(hx, hy) + margin
+    return f
+
+
+def _keepout_line(y0, margin):
+    def f(cx, cy, hx, hy):
+        return abs(cy - y0) < hy + margin
+    return f
+
+
+def plain_small(threshold: float | None = 4.0) -> Workload:
+    """200x200x40 voxels at 0.1 m, one 16x1024 scan from (0, 0, 1.8)."""
+    sensor = Sensor(16, 1024, -15.0, 15.0, 20.0, 0.02)
+    scene = make_scene(0, 40, 9.0, keepout=_keepout_point(0.0, 0.0, 1.0))
+    poses = np.array([[0.0, 0.0, 1.8, 0.0]])
+    return Workload("plain_small_201x201x41", (100, 100, 20), 0.1, sensor, scene, poses,
+                    threshold, seed=0, fetch_centres=1000, fetch_radius=1.0,
+                    extra=dict(recenter_shift=(37, -12, 3)))
+
+
+def readme_scale(n_scans: int = 200) -> Workload:
+    """701x701x151 voxels (74.2M) at 0.1 m, 64x1024 scans, 50 m, circle R=25 m."""
+    sensor = Sensor(64, 1024, -22.5, 22.5, 50.0, 0.02)
+    scene = make_scene(1, 400, 60.0, keepout=_keepout_circle(25.0, 1.5))
+    poses = circle_trajectory(n_scans, 25.0, 1.5, 10.0, 1.8)
+    return Workload("readme_701x701x151_64x1024", (350, 350, 75), 0.1, sensor, scene, poses,
+                    4.0, seed=1)
+
+
+def stress(n_scans: int = 300) -> Workload:
+    """1025x1025x257 voxels at 0.05 m, 128x2048 scans, 100 m, 8 m/s line."""
+    sensor = Sensor(128, 2048, -22.5, 22.5, 100.0, 0.03)
+    scene = make_scene(4, 3000, 150.0, side=(1.0, 12.0), height=(2.0, 20.0),
+                       keepout=_keepout_line(0.0, 2.0))
+    poses = line_trajectory(n_scans, 8.0, 10.0, 1.8, start=(-120.0, 0.0))
+    return Workload("stress_1025x1025x257_128x2048", (512, 512, 128), 0.05, sensor, scene,
+                    poses, 0.5, seed=4, fetch_centres=10000, fetch_radius=2.0)
+
+
+def perf_test_cloud(n: int = 500000, r_min: float = 1.5, r_max: float = 8.0, seed: int = 42):
+    """Spherical-shell cloud with the shape of the reference's perf test
+    (test/test_occupancy_grid_perf.cpp:31-50): radius uniform in
+    [r_min, r_max], direction uniform on the sphere, about the origin."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(r_min, r_max, n)
+    ct = rng.uniform(-1.0, 1.0, n)
+    st = np.sqrt(np.maximum(0.0, 1.0 - ct * ct))
+    ph = rng.uniform(0.0, 2.0 * np.pi, n)
+    return np.stack([r * st * np.cos(ph), r * st * np.sin(ph), r * ct], axis=1).astype(np.float32)

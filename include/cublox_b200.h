@@ -1,0 +1,187 @@
+/*
+ * cublox_b200 — C ABI of the B200 (sm_100a) map-integration path.
+ *
+ * Plain C types only.  Every call returns CUBLOX_OK (0) or a negative status;
+ * cublox_last_error() gives the message of the calling thread's last failure.
+ * Citations name the reference interface (mrsp/cublox) each entry replaces.
+ *
+ * Streams: every grid owns (or borrows) one CUDA stream; all of its device
+ * work is ordered on it.  Calls that return host data wait for that stream;
+ * cublox_grid_update* only enqueue (the host cloud is staged into pinned
+ * memory before the call returns, so the caller may reuse its buffer).
+ */
+#ifndef CUBLOX_B200_H
+#define CUBLOX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUBLOX_OK 0
+#define CUBLOX_ERR_INVALID -1 /* bad argument                              */
+#define CUBLOX_ERR_CUDA -2    /* CUDA runtime error (message has details) */
+#define CUBLOX_ERR_NOMEM -3   /* device or pinned allocation failed       */
+#define CUBLOX_ERR_RANGE -4   /* voxel count above int32 (Grid.cpp:44-50) */
+#define CUBLOX_ERR_DEVICE -5  /* device-side check failed (error word)    */
+
+#define CUBLOX_STATE_UNKNOWN 0 /* OccupancyGrid.hpp:31-35 */
+#define CUBLOX_STATE_FREE 1
+#define CUBLOX_STATE_OCCUPIED 2
+#define CUBLOX_FILTER_ALL (-1)
+
+/* Point-cloud layouts accepted by cublox_grid_update_xyz.                   */
+#define CUBLOX_LAYOUT_SOA 0 /* x[0..n), y[0..n), z[0..n) back to back       */
+#define CUBLOX_LAYOUT_AOS 1 /* x0 y0 z0 x1 y1 z1 ...                        */
+
+typedef struct cublox_grid cublox_grid;
+
+/* Per-scan algorithmic counters (filled when stats are enabled).            */
+typedef struct {
+  int64_t rays;        /* points not dropped (finite, length >= 1e-6)      */
+  int64_t op_incs;     /* in-window op increments incl. endpoints (U)      */
+  int64_t hit_incs;    /* endpoint hits (H)                                 */
+  int64_t touched;     /* voxels whose counters were folded (T)            */
+} cublox_scan_stats;
+
+const char *cublox_last_error(void);
+const char *cublox_version(void);
+
+/* OccupancyGrid(half_map_size_i, resolution, origin_at_center,
+ * recenter_threshold, origin)  — OccupancyGrid.hpp:42-45,
+ * OccupancyGrid.cpp:54-65, Grid.cpp:27-54.  `stream` is a cudaStream_t or
+ * NULL (the grid then creates its own non-blocking stream).                 */
+int cublox_grid_create(const int half_map_size[3], float resolution,
+                       int origin_at_center, int has_recenter_threshold,
+                       double recenter_threshold, const float origin[3],
+                       void *stream, cublox_grid **out);
+/* ~OccupancyGrid — OccupancyGrid.cpp:67-114.                               */
+int cublox_grid_destroy(cublox_grid *g);
+
+/* reset() / resetVoxel(hash) — OccupancyGrid.cpp:116-139.                  */
+int cublox_grid_reset(cublox_grid *g);
+int cublox_grid_reset_voxel(cublox_grid *g, int hash_id);
+
+/* setMaxRaycastRange / getMaxRaycastRange — OccupancyGrid.hpp:68-71.       */
+int cublox_grid_set_max_range(cublox_grid *g, float range);
+int cublox_grid_get_max_range(const cublox_grid *g, float *range);
+/* setLogOddsParams — OccupancyGrid.hpp:74-85 (l_unknown stays 0).         */
+int cublox_grid_set_log_odds(cublox_grid *g, float l_hit, float l_miss,
+                             float l_min, float l_max, float l_free,
+                             float l_occupied);
+
+/* FP32 multiply-add contraction pattern to reproduce.  Bits 0-2: shape of
+ * the ray-length sum of squares (0 plain, 1 fma(z,z,fma(y,y,x*x)),
+ * 2 fma(z,z,fma(x,x,y*y)), 3 fma(z,z,x*x+y*y), 4 fma(y,y,x*x)+z*z,
+ * 5 fma(x,x,y*y)+z*z); bit 3 clip point; bit 4 voxel-boundary distance;
+ * bit 5 centre binning; bits 6/7 miss/hit log-odds terms; bits 8-10 and
+ * 11-13 the recenter-gate and fetch sums of squares; bit 14 fetch offset.
+ * The default is the pattern of the reference's own sm_100a release build,
+ * pinned black-box by tests/test_contraction_pins.py.                      */
+int cublox_grid_set_fp_mode(cublox_grid *g, unsigned mode);
+int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
+
+/* update(cloud, sensor_origin) — OccupancyGrid.hpp:53-54,
+ * OccupancyGrid.cpp:181-238.  x/y/z are the three columns of the reference's
+ * column-major PointCloud (host or device pointers; n points each).         */
+int cublox_grid_update(cublox_grid *g, const float *x, const float *y,
+                       const float *z, int n, const float sensor_origin[3]);
+/* Same, with the cloud in one buffer of the given layout.                   */
+int cublox_grid_update_xyz(cublox_grid *g, const float *xyz, int layout,
+                           int n, const float sensor_origin[3]);
+
+/* recenter(pos) — OccupancyGrid.hpp:57, OccupancyGrid.cpp:141-179.
+ * *action (may be NULL): 0 nothing, 1 slabs cleared, 2 full reset.
+ * mode 0 reproduces the reference's slab set exactly (its extra band of
+ * "entering" slabs included); mode 1 clears only the slabs that left.      */
+int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action);
+int cublox_grid_set_recenter_mode(cublox_grid *g, int mode);
+
+/* fetchOccupancyAround(center, radius, filter, max_results) —
+ * OccupancyGrid.hpp:62-65, OccupancyGrid.cpp:240-356.  filter is -1 (all)
+ * or a CUBLOX_STATE_*.  Samples come in ascending (x, y, z) global-index
+ * order; out_pos holds 3 floats per sample.  Writes at most `capacity`;
+ * *n_out = samples returned (as the reference returns them).               */
+int cublox_grid_fetch(cublox_grid *g, const float center[3], float radius,
+                      int filter, int max_results, float *out_pos,
+                      uint8_t *out_state, int64_t capacity, int64_t *n_out);
+/* Many fetches in one launch (no reference counterpart beyond calling
+ * fetchOccupancyAround once per centre).  out_offsets gets n_centers+1
+ * entries; query q's samples are [out_offsets[q], out_offsets[q+1]).
+ * Output buffers are host pointers.  If capacity is too small the call
+ * fills out_offsets and returns CUBLOX_ERR_INVALID without samples.       */
+int cublox_grid_fetch_batch(cublox_grid *g, const float *centers,
+                            int n_centers, float radius, int filter,
+                            int max_results, int64_t *out_offsets,
+                            float *out_pos, uint8_t *out_state,
+                            int64_t capacity);
+/* Counts only: per-centre sample counts, no samples materialised.         */
+int cublox_grid_fetch_counts(cublox_grid *g, const float *centers,
+                             int n_centers, float radius, int filter,
+                             int max_results, int64_t *out_counts);
+
+/* isOccupied/isFree/isUnknown(pos) — OccupancyGrid.cpp:368-393, for n
+ * points in one launch: out_state[i] = CUBLOX_STATE_* of point i (outside
+ * the window: UNKNOWN).                                                     */
+int cublox_grid_query_states(cublox_grid *g, const float *xyz, int n,
+                             uint8_t *out_state);
+/* storedAt(hash) — OccupancyGrid.cpp:358-366 (0 for an out-of-range hash). */
+int cublox_grid_stored_at(cublox_grid *g, int hash_id, float *out);
+
+/* getOriginIndex / getOriginPosition — Grid.hpp:37-38.                    */
+int cublox_grid_origin(const cublox_grid *g, int origin_i[3],
+                       float origin_f[3]);
+/* Grid::Config — Grid.hpp:44-53.                                           */
+int cublox_grid_geometry(const cublox_grid *g, int map_size[3], int half[3],
+                         int *voxel_num, float *resolution,
+                         int *origin_at_center);
+/* first_run_ flag of the reference (OccupancyGrid.cpp:192-198): 1 until the
+ * first update snaps the window origin to the sensor.                      */
+int cublox_grid_first_run(const cublox_grid *g, int *first_run);
+/* Force the window origin (global voxel index); clears first_run.          */
+int cublox_grid_set_origin_index(cublox_grid *g, const int origin_i[3]);
+
+/* The stored log-odds of every voxel, in the reference's ring-buffer hash
+ * order (utils.cuh:131-136), into a host buffer of voxel_num floats.       */
+int cublox_grid_export(cublox_grid *g, float *occ_host);
+int cublox_grid_import(cublox_grid *g, const float *occ_host);
+
+/* Stream handling.                                                          */
+int cublox_grid_stream(const cublox_grid *g, void **stream);
+int cublox_grid_synchronize(cublox_grid *g);
+
+/* Algorithmic counters of the last update (enable first; costs one extra
+ * device->host copy per update when read).                                 */
+int cublox_grid_enable_stats(cublox_grid *g, int enable);
+int cublox_grid_last_stats(cublox_grid *g, cublox_scan_stats *out);
+
+/* Raycast one scan (AoS host points) without folding it, return the per-
+ * voxel traversal and hit counts the reference keeps in op_cnt / hit_cnt
+ * (kernels.cu:33-152; ring-buffer hash order), then zero them.  The map is
+ * left unchanged.  For verification.                                       */
+int cublox_grid_count_scan(cublox_grid *g, const float *xyz, int n,
+                           const float sensor_origin[3], int32_t *op_out,
+                           int32_t *hit_out);
+
+/* Device time of the last raycast, fold and recenter-clear launches in ms
+ * (-1 where none ran since the last read); timing is opt-in.               */
+int cublox_grid_enable_timing(cublox_grid *g, int enable);
+int cublox_grid_last_timing(cublox_grid *g, float ms[3]);
+
+/* Work units of one scan as the reference counts them: per ray, the DDA
+ * iterations of rayCastUpdateKernel's loop that did not break, plus one for
+ * the endpoint (kernels.cu:105-151), over the current window.  Accounting
+ * only; no map state changes.                                              */
+int cublox_grid_reference_steps(cublox_grid *g, const float *xyz, int n,
+                                const float sensor_origin[3],
+                                int64_t *voxel_steps);
+
+/* Device error word: nonzero if a kernel's own bounds checks rejected an
+ * index (a bug, never expected).  Reading it clears it.                    */
+int cublox_grid_check(cublox_grid *g, uint32_t *error_word);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUBLOX_B200_H */

@@ -1,0 +1,308 @@
+"""cublox_b200 on the GPU against the oracle and the reference's own kernels.
+
+Bit-exact bars (integer/index work and the FP32 path, whose operation order
+and contraction are reproduced): per-voxel traversal and hit counts, stored
+log-odds, recenter action/origin/cleared slabs, fetch samples.
+"""
+import numpy as np
+import pytest
+
+import cublox_b200 as C
+import oracle as O
+from cublox_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+LO = C.yaml_log_odds()
+
+
+def pair(half, res, ctr=False, thr=None, origin=(0.0, 0.0, 0.0), max_range=None):
+    g = C.OccupancyGrid(half, res, ctr, thr, origin)
+    o = O.OracleGrid(half, res, ctr, thr, origin)
+    g.setLogOddsParams(*LO)
+    o.set_log_odds(*LO)
+    if max_range is not None:
+        g.setMaxRaycastRange(max_range)
+        o.set_max_range(max_range)
+    return g, o
+
+
+def same_bits(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32),
+                          np.asarray(b, np.float32).view(np.uint32))
+
+
+def ref_grid(half, res, ctr=False, thr=None, origin=(0.0, 0.0, 0.0), max_range=None):
+    if not O.ref_available():
+        return None
+    r = O.RefGrid(half, res, ctr, thr, origin)
+    r.set_log_odds(*LO)
+    if max_range is not None:
+        r.set_max_range(max_range)
+    return r
+
+
+@pytest.fixture(scope="module")
+def small():
+    w = synth.plain_small()
+    return w, w.scan(0), w.sensor_origin(0)
+
+
+def test_counts_match_oracle_plain_small(small):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.set_origin_index((0, 0, 18))
+    o.set_origin_index((0, 0, 18))
+    op, hit = g.count_scan(pts, s)
+    st = o.raycast(pts, s)
+    assert np.array_equal(op, o.op())
+    assert np.array_equal(hit, o.hit())
+    assert int(op.sum()) == st["op_incs"] and int(hit.sum()) == st["hit_incs"]
+    assert g.check() == 0
+
+
+def test_update_matches_oracle_and_reference(small):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, thr=4.0, max_range=w.sensor.max_range)
+    assert g.first_run()
+    g.update(pts, s)
+    st = o.update(pts, s)
+    assert not g.first_run()
+    assert g.getOriginIndex() == o.origin()[0]
+    assert same_bits(g.export(), o.occ())
+    assert st["touched"] > 0
+    r = ref_grid(w.half, w.resolution, thr=4.0, max_range=w.sensor.max_range)
+    if r is not None:
+        r.update(pts, s)
+        occ, op, hit = r.download()
+        assert same_bits(occ, o.occ())
+        assert not op.any() and not hit.any()
+        assert r.origin()[0] == o.origin()[0]
+
+
+def test_update_stats(small):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.enable_stats(True)
+    g.update(pts, s)
+    st = o.update(pts, s)
+    gs = g.last_stats()
+    assert gs["rays"] == st["rays"]
+    assert gs["op_incs"] == st["op_incs"]
+    assert gs["hit_incs"] == st["hit_incs"]
+    assert gs["touched"] == st["touched"]
+
+
+def test_repeated_scans_and_clamp(small):
+    """Many scans drive voxels into both clamps; every stored value exact."""
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    for k in range(6):
+        sk = s + np.float32([0.013 * k, -0.021 * k, 0.0])
+        g.update(pts, sk)
+        o.update(pts, sk)
+    occ = g.export()
+    assert same_bits(occ, o.occ())
+    assert (occ == np.float32(LO[3])).any() and (occ == np.float32(LO[2])).any()
+
+
+@pytest.mark.parametrize("thr,expect_action", [(4.0, 0), (1.0, 1)])
+def test_recenter_plain_small(small, thr, expect_action):
+    """The (37,-12,3)-voxel shift is 3.901 m: below the 4 m yaml threshold
+    (a no-op in the reference), above 1 m (slabs on all three axes)."""
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, thr=thr, max_range=w.sensor.max_range)
+    g.update(pts, s)
+    o.update(pts, s)
+    oi, of = o.origin()
+    shift = np.array(w.extra["recenter_shift"], dtype=np.float32)
+    pos = (np.float32(of) + shift * np.float32(w.resolution)).astype(np.float32)
+    a = g.recenter(pos)
+    ro = o.recenter(pos)
+    assert a == ro["action"] == expect_action
+    assert g.getOriginIndex() == o.origin()[0]
+    assert same_bits(g.export(), o.occ())
+    r = ref_grid(w.half, w.resolution, thr=thr, max_range=w.sensor.max_range)
+    if r is not None:
+        r.update(pts, s)
+        rr = r.recenter(pos)
+        assert rr["action"] == expect_action
+        assert r.origin()[0] == o.origin()[0]
+        assert same_bits(r.download()[0], o.occ())
+    # integrate again after the move
+    g.update(pts, pos)
+    o.update(pts, pos)
+    assert same_bits(g.export(), o.occ())
+
+
+def test_recenter_full_reset_and_mode1(small):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, thr=0.5, max_range=w.sensor.max_range)
+    g.update(pts, s)
+    o.update(pts, s)
+    far = np.float32([500.0, 0.0, 1.8])  # shift >= largest map side
+    assert g.recenter(far) == 2 == o.recenter(far)["action"]
+    assert not g.export().any()
+    assert g.getOriginIndex() == o.origin()[0]
+    # exiting-slabs-only mode clears a subset of compat mode's slabs
+    g2, o2 = pair(w.half, w.resolution, thr=0.5, max_range=w.sensor.max_range)
+    g2.set_recenter_mode(1)
+    g2.update(pts, s)
+    o2.update(pts, s)
+    pos = np.float32(s + np.float32([1.2, -0.7, 0.3]))
+    assert g2.recenter(pos) == 1
+    r = o2.recenter(pos, compat=False)
+    assert same_bits(g2.export(), o2.occ())
+    assert r["action"] == 1
+
+
+def test_fetch_plain_small(small):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.update(pts, s)
+    o.update(pts, s)
+    rng = np.random.default_rng(5)
+    oi, of = o.origin()
+    ext = np.float32(w.half) * np.float32(w.resolution)
+    centres = (np.float32(of) + rng.uniform(-1, 1, (1000, 3)) * ext).astype(np.float32)
+    off, pos, st = g.fetch_batch(centres, w.fetch_radius)
+    r = ref_grid(w.half, w.resolution, max_range=w.sensor.max_range)
+    if r is not None:
+        r.update(pts, s)
+    for q in range(len(centres)):
+        opos, ost, _ = o.fetch(centres[q], w.fetch_radius)
+        gp, gs = pos[off[q]:off[q + 1]], st[off[q]:off[q + 1]]
+        assert same_bits(gp, opos) and np.array_equal(gs, ost), q
+        if r is not None and q < 200:
+            rp, rs = r.fetch(centres[q], w.fetch_radius)
+            key = lambda p, t: sorted(map(tuple, np.concatenate(
+                [p.view(np.uint32), t[:, None].astype(np.uint32)], axis=1).tolist()))
+            assert key(rp, rs) == key(gp, gs), q
+
+
+@pytest.mark.parametrize("flt,maxr", [(2, 0), (1, 0), (0, 0), (-1, 50), (2, 7)])
+def test_fetch_filters_and_caps(small, flt, maxr):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.update(pts, s)
+    o.update(pts, s)
+    rng = np.random.default_rng(6)
+    centres = (s + rng.uniform(-6, 6, (64, 3)) * np.float32([1, 1, 0.2])).astype(np.float32)
+    for c in centres:
+        gp, gs = g.fetchOccupancyAround(c, 1.5, None if flt < 0 else flt, maxr)
+        opos, ost, npass = o.fetch(c, 1.5, flt, maxr)
+        assert same_bits(gp, opos) and np.array_equal(gs, ost)
+        if maxr:
+            assert len(gp) == min(npass, maxr)
+
+
+def test_point_queries(small):
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.update(pts, s)
+    o.update(pts, s)
+    rng = np.random.default_rng(7)
+    q = np.concatenate([pts[::7], rng.uniform(-12, 12, (4000, 3)).astype(np.float32)])
+    st = g.query_states(q)
+    for i in range(0, len(q), 3):
+        want = [k for k in (0, 1, 2) if o.is_state(q[i], k)]
+        assert want == [int(st[i])], i
+    assert g.isUnknown([1000.0, 0.0, 0.0])
+    h = int(np.flatnonzero(o.occ())[0])
+    assert g.storedAt(h) == o.occ()[h]
+    assert g.storedAt(-1) == 0.0 and g.storedAt(g.voxel_num) == 0.0
+
+
+def test_edge_case_rays():
+    """Non-finite points, zero-length rays, clipped rays, axis-aligned and
+    face-aligned rays, negative coordinates, sensor outside the window."""
+    half, res = (20, 16, 12), 0.1
+    sensors = [np.float32([0.0, 0.0, 0.0]), np.float32([-0.35, 0.2, -0.1]),
+               np.float32([3.0, 0.05, 0.0])]  # the last is outside in x
+    rng = np.random.default_rng(8)
+    special = [
+        [np.nan, 0, 0], [np.inf, 1, 1], [0, -np.inf, 0],
+        [0.0, 0.0, 0.0], [1e-8, 0, 0],
+        [1.0, 0.0, 0.0], [0.0, -1.3, 0.0], [0.0, 0.0, 0.9], [-1.7, 0, 0],
+        [0.5, 0.5, 0.5], [-0.5, -0.5, -0.5], [0.3, -0.3, 0.0], [0.1, 0.2, 0.3],
+        [100.0, 0.0, 0.0], [-30.0, 40.0, 1.0], [0.7, 0.7, 0.0],
+    ]
+    for s in sensors:
+        pts = np.concatenate([np.float32(special) + 0 * s,
+                              (s + rng.uniform(-4, 4, (3000, 3))).astype(np.float32),
+                              (s + np.round(rng.uniform(-20, 20, (500, 3))) * np.float32(res)).astype(np.float32)])
+        g, o = pair(half, res, max_range=2.5)
+        g.set_origin_index((0, 0, 0))
+        o.set_origin_index((0, 0, 0))
+        op, hit = g.count_scan(pts, s)
+        o.raycast(pts, s)
+        assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit())
+
+
+@pytest.mark.parametrize("fx", [((200, 200, 100), (17, -42, 8), 0.05, True),
+                                ((350, 350, 75), (-120, 55, 0), 0.1, False),
+                                ((3, 5, 7), (2, -1, 4), 0.25, True)])
+def test_reference_fixture_grids(fx):
+    """The three geometries of the reference's index tests
+    (test/test_utils_index_roundtrip.cpp:44-53): a scan integrated into each,
+    window origin as in the fixture, against the oracle."""
+    half, origin, res, ctr = fx
+    g, o = pair(half, res, ctr=ctr, max_range=8.0)
+    g.set_origin_index(origin)
+    o.set_origin_index(origin)
+    c = np.float32(origin) * np.float32(res)
+    pts = (c + synth.perf_test_cloud(20000, 0.3, 9.0, seed=42)).astype(np.float32)
+    g.update(pts, c)
+    o.update(pts, c)
+    assert same_bits(g.export(), o.occ())
+
+
+def test_trajectory_with_recenters():
+    """A 40-scan drive on a 241x241x81 grid at 0.1 m, recentering at 1.5 m."""
+    sensor = synth.Sensor(32, 512, -20.0, 20.0, 15.0, 0.02)
+    scene = synth.make_scene(21, 150, 30.0, keepout=synth._keepout_line(0.0, 1.5))
+    poses = synth.line_trajectory(40, 4.0, 10.0, 1.8, start=(-8.0, 0.0))
+    half = (120, 120, 40)
+    g, o = pair(half, 0.1, thr=1.5, max_range=sensor.max_range)
+    actions = []
+    for k, (x, y, z, yaw) in enumerate(poses):
+        pts = synth.scan(scene, sensor, (x, y, z), yaw, seed=900 + k)
+        so = np.float32([x, y, z])
+        g.update(pts, so)
+        o.update(pts, so)
+        a = g.recenter(so)
+        assert a == o.recenter(so)["action"]
+        actions.append(a)
+        assert g.getOriginIndex() == o.origin()[0]
+        if k % 8 == 7:
+            assert same_bits(g.export(), o.occ()), k
+    assert same_bits(g.export(), o.occ())
+    assert actions.count(1) >= 3
+
+
+def test_empty_and_invalid_inputs():
+    g = C.OccupancyGrid((4, 4, 4), 0.1, False, None)
+    g.update(np.zeros((0, 3), np.float32), [0, 0, 0])
+    assert g.first_run()  # an empty cloud returns before the first-run snap
+    with pytest.raises(C.CubloxError):
+        C.OccupancyGrid((40000, 40000, 40000), 0.1, False, None)
+    with pytest.raises(C.CubloxError):
+        C.OccupancyGrid((4, 4, 4), 0.0, False, None)
+    with pytest.raises(ValueError):
+        g.update(np.zeros((5, 2), np.float32), [0, 0, 0])
+    pos, st = g.fetchOccupancyAround([0, 0, 0], -1.0)
+    assert len(pos) == 0
+    g.reset()
+    assert g.first_run()
+
+
+def test_readme_scale_scan_exact():
+    """One full-size 64x1024 scan on the 701x701x151 (74.2M voxel) grid."""
+    w = synth.readme_scale(2)
+    g, o = pair(w.half, w.resolution, thr=4.0, max_range=w.sensor.max_range)
+    for k in range(2):
+        pts, so = w.scan(k), w.sensor_origin(k)
+        g.update(pts, so)
+        o.update(pts, so, threads=8)
+    occ = g.export()
+    assert same_bits(occ, o.occ())
