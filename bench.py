@@ -151,7 +151,9 @@ def run_cublox(args, rank, world, dist):
     w, scans, origins = build_workload(n_scans)
     steps = count_steps(w, scans, origins)
     N = scans[0].shape[0]
-    stream = torch.cuda.current_stream()
+    # A dedicated stream shared by torch (events, L2 flush) and the grid.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     lo = C.yaml_log_odds()
 

@@ -29,11 +29,13 @@ constexpr unsigned kFpRecSosShift = 8;      // kernels.cu:326-331
 constexpr unsigned kFpFetchSosShift = 11;   // kernels.cu:532-535
 constexpr unsigned kFpFetchDFma = 1u << 14; // kernels.cu:529-534
 
-// The contraction pattern of the reference's own sm_100a release build.
+// The contraction pattern of the reference's own sm_100a release build,
+// pinned black-box: sums of squares fma(z,z, fma(x,x, y*y)); apply terms
+// fused; clip point, boundary distance and fetch offset not fused.  Centre
+// binning reads the same fused or not except at exact ties of p*inv.
 constexpr unsigned kFpPinned =
-    (kSosFxFz << kFpRaySosShift) | kFpClipFma | kFpBoundFma | kFpCenterFma |
-    kFpMissFma | kFpHitFma | (kSosFxFz << kFpRecSosShift) |
-    (kSosFxFz << kFpFetchSosShift) | kFpFetchDFma;
+    (kSosFxFz << kFpRaySosShift) | kFpCenterFma | kFpMissFma | kFpHitFma |
+    (kSosFxFz << kFpRecSosShift) | (kSosFxFz << kFpFetchSosShift);
 
 #if defined(__CUDACC__)
 #define CBX_HD __host__ __device__ __forceinline__

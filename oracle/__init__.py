@@ -34,13 +34,12 @@ FP_HIT_FMA = 1 << 7
 FP_REC_SOS_SHIFT = 8
 FP_FETCH_SOS_SHIFT = 11
 FP_FETCH_DFMA = 1 << 14
-FP_PINNED = ((SOS_FX_FZ << FP_RAY_SOS_SHIFT) | FP_CLIP_FMA | FP_BOUND_FMA | FP_CENTER_FMA
-             | FP_MISS_FMA | FP_HIT_FMA | (SOS_FX_FZ << FP_REC_SOS_SHIFT)
-             | (SOS_FX_FZ << FP_FETCH_SOS_SHIFT) | FP_FETCH_DFMA)
+FP_PINNED = ((SOS_FX_FZ << FP_RAY_SOS_SHIFT) | FP_CENTER_FMA | FP_MISS_FMA | FP_HIT_FMA
+             | (SOS_FX_FZ << FP_REC_SOS_SHIFT) | (SOS_FX_FZ << FP_FETCH_SOS_SHIFT))
 
 
-def fp_mode(ray_sos=SOS_FX_FZ, clip=True, bound=True, center=True, miss=True, hit=True,
-            rec_sos=SOS_FX_FZ, fetch_sos=SOS_FX_FZ, fetch_d=True) -> int:
+def fp_mode(ray_sos=SOS_FX_FZ, clip=False, bound=False, center=True, miss=True, hit=True,
+            rec_sos=SOS_FX_FZ, fetch_sos=SOS_FX_FZ, fetch_d=False) -> int:
     m = (ray_sos << FP_RAY_SOS_SHIFT) | (rec_sos << FP_REC_SOS_SHIFT) | (fetch_sos << FP_FETCH_SOS_SHIFT)
     m |= FP_CLIP_FMA if clip else 0
     m |= FP_BOUND_FMA if bound else 0

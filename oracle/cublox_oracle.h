@@ -49,11 +49,15 @@ extern "C" {
 #define ORC_FP_FETCH_SOS(m) (((m) >> ORC_FP_FETCH_SOS_SHIFT) & 7u)
 
 /* Pinned device contraction pattern of the reference's sm_100a build.      */
+/* Pinned on the reference built for sm_100a with its release flags:      */
+/* sums of squares fma(z,z, fma(x,x, y*y)); apply terms fused; clip point, */
+/* boundary distance and fetch offset not fused.  Centre binning: fused    */
+/* and unfused agree except at exact ties of p*inv (no input separates     */
+/* them), so the fused reading is kept.                                    */
 #define ORC_FP_PINNED                                                        \
-  ((ORC_SOS_FX_FZ << ORC_FP_RAY_SOS_SHIFT) | ORC_FP_CLIP_FMA |              \
-   ORC_FP_BOUND_FMA | ORC_FP_CENTER_FMA | ORC_FP_MISS_FMA | ORC_FP_HIT_FMA | \
-   (ORC_SOS_FX_FZ << ORC_FP_REC_SOS_SHIFT) |                                 \
-   (ORC_SOS_FX_FZ << ORC_FP_FETCH_SOS_SHIFT) | ORC_FP_FETCH_DFMA)
+  ((ORC_SOS_FX_FZ << ORC_FP_RAY_SOS_SHIFT) | ORC_FP_CENTER_FMA |            \
+   ORC_FP_MISS_FMA | ORC_FP_HIT_FMA | (ORC_SOS_FX_FZ << ORC_FP_REC_SOS_SHIFT) | \
+   (ORC_SOS_FX_FZ << ORC_FP_FETCH_SOS_SHIFT))
 
 /* ---- grid state (mirrors Grid + OccupancyGrid members) ------------------ */
 typedef struct {

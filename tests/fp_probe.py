@@ -89,7 +89,7 @@ def build_ray_scenarios(seed: int = 11, per_pair: int = 24):
         g = O.OracleGrid(half, float(res), ctr, None)
         g.set_origin_index((0, 0, 0))
         g.set_max_range(float(M))
-        base = _ray_mode(O.SOS_FX_FZ, True, True, True)
+        base = _ray_mode(O.SOS_FX_FZ, False, False, True)
         # Pool 1: endpoints at |d| ~ M, a few ulps either side (clip decision).
         u = _unit(rng, 200000)
         e = (sensor[None, :].astype(np.float64) + float(M) * u).astype(np.float32)
@@ -118,11 +118,10 @@ def build_ray_scenarios(seed: int = 11, per_pair: int = 24):
             pools.append(_jitter(rng, e.astype(np.float32), 12))
         variants = []
         for s in SHAPES:
-            variants.append(_ray_mode(s, True, True, True))
-        variants.append(_ray_mode(O.SOS_FX_FZ, False, True, True))
+            variants.append(_ray_mode(s, False, False, True))
         variants.append(_ray_mode(O.SOS_FX_FZ, True, False, True))
-        if ctr:
-            variants.append(_ray_mode(O.SOS_FX_FZ, True, True, False))
+        variants.append(_ray_mode(O.SOS_FX_FZ, False, True, True))
+        variants.append(_ray_mode(O.SOS_FX_FZ, True, True, True))
         # Also discriminate against the all-plain reading.
         variants.append(_ray_mode(O.SOS_PLAIN, False, False, False))
         sel = []
