@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libcublox_b200.so")
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_RANGE, ERR_DEVICE = -1, -2, -3, -4, -5
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
+OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT = 1, 2, 3, 4
 
 
 class VoxelState(enum.IntEnum):
@@ -99,6 +100,8 @@ def lib():
             "cublox_grid_check": ([G, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
             "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
             "cublox_grid_enable_timing": ([G, ctypes.c_int], ctypes.c_int),
+            "cublox_grid_set_option": ([G, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+            "cublox_grid_get_option": ([G, ctypes.c_int, i], ctypes.c_int),
             "cublox_grid_last_timing": ([G, f], ctypes.c_int),
             "cublox_grid_reference_steps": ([G, f, ctypes.c_int, f, i64], ctypes.c_int),
         }
@@ -388,6 +391,14 @@ class OccupancyGrid:
                                             op.ctypes.data_as(ip), hit.ctypes.data_as(ip)),
                "count_scan")
         return op, hit
+
+    def set_option(self, key: int, value: int):
+        _check(lib().cublox_grid_set_option(self._h, int(key), int(value)), "set_option")
+
+    def get_option(self, key: int) -> int:
+        v = ctypes.c_int()
+        _check(lib().cublox_grid_get_option(self._h, int(key), ctypes.byref(v)), "get_option")
+        return v.value
 
     def enable_timing(self, on: bool = True):
         _check(lib().cublox_grid_enable_timing(self._h, int(on)), "enable_timing")

@@ -103,6 +103,15 @@ struct cublox_grid {
   unsigned fp = kFpPinned;
   int recenter_mode = 0;
   bool stats_on = false;
+  // kernel options (cublox_grid_set_option)
+  int opt_raycast = 1;  // 0 one thread per ray, 1 direction-binned walk
+  int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
+  int opt_match = 1;    // merge duplicate voxels within a warp
+  int opt_sort = 1;     // walk rays in direction-bin order
+  int *d_bins = nullptr;
+  int *d_hist = nullptr;
+  float *d_sorted = nullptr;
+  int bin_cap = 0;
   bool timing_on = false;
   cudaEvent_t tev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool tev_used[3] = {false, false, false};
@@ -150,6 +159,9 @@ static void free_all(cublox_grid *g) {
   cudaFree(g->d_err);
   cudaFree(g->d_masks);
   cudaFree(g->d_cloud);
+  cudaFree(g->d_bins);
+  cudaFree(g->d_hist);
+  cudaFree(g->d_sorted);
   cudaFree(g->d_fq);
   cudaFree(g->d_fpos);
   cudaFree(g->d_fstate);
@@ -315,6 +327,41 @@ int cublox_grid_set_log_odds(cublox_grid *g, float l_hit, float l_miss,
   return CUBLOX_OK;
 }
 
+int cublox_grid_set_option(cublox_grid *g, int key, int value) {
+  if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
+  switch (key) {
+    case CUBLOX_OPT_RAYCAST:
+      if (value != 0 && value != 1) break;
+      g->opt_raycast = value;
+      return CUBLOX_OK;
+    case CUBLOX_OPT_CUBE:
+      if (value != 0 && value != 16 && value != 32) break;
+      g->opt_cube = value;
+      return CUBLOX_OK;
+    case CUBLOX_OPT_MATCH:
+      g->opt_match = value != 0;
+      return CUBLOX_OK;
+    case CUBLOX_OPT_SORT:
+      g->opt_sort = value != 0;
+      return CUBLOX_OK;
+    default:
+      break;
+  }
+  return fail(CUBLOX_ERR_INVALID, "set_option: unknown key or value");
+}
+
+int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
+  if (!g || !value) return fail(CUBLOX_ERR_INVALID, "null argument");
+  switch (key) {
+    case CUBLOX_OPT_RAYCAST: *value = g->opt_raycast; return CUBLOX_OK;
+    case CUBLOX_OPT_CUBE: *value = g->opt_cube; return CUBLOX_OK;
+    case CUBLOX_OPT_MATCH: *value = g->opt_match; return CUBLOX_OK;
+    case CUBLOX_OPT_SORT: *value = g->opt_sort; return CUBLOX_OK;
+    default: break;
+  }
+  return fail(CUBLOX_ERR_INVALID, "get_option: unknown key");
+}
+
 int cublox_grid_set_fp_mode(cublox_grid *g, unsigned mode) {
   if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
   g->fp = mode;
@@ -390,8 +437,31 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   p.hit = g->d_hit;
   p.stats = g->stats_on ? g->d_stats : nullptr;
   p.err = g->d_err;
+  if (g->opt_raycast == 1 && n > g->bin_cap) {
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(g->d_bins);
+    cudaFree(g->d_sorted);
+    g->d_bins = nullptr;
+    g->d_sorted = nullptr;
+    g->bin_cap = 0;
+    if (!g->d_hist && cudaMalloc(&g->d_hist, sizeof(int) * 2 * binned_bins()) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "update: bin buffer allocation failed");
+    }
+    if (cudaMalloc(&g->d_bins, sizeof(int) * static_cast<size_t>(n)) != cudaSuccess ||
+        cudaMalloc(&g->d_sorted, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "update: sort buffer allocation failed");
+    }
+    g->bin_cap = n;
+  }
   tmark(g, 0, 0);
-  launch_raycast(p, g->stream);
+  if (g->opt_raycast == 1) {
+    BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};
+    launch_raycast_binned(p, b, g->opt_cube, g->opt_match != 0, g->opt_sort != 0, g->stream);
+  } else {
+    launch_raycast(p, g->stream);
+  }
   CK_LAUNCH();
   tmark(g, 0, 1);
   if (count_only) return CUBLOX_OK;

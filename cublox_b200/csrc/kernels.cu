@@ -5,18 +5,11 @@
 #include <cstdint>
 
 #include "kernels.cuh"
+#include "ray_walk.cuh"
 
 namespace cublox_b200 {
 
 namespace {
-
-__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
-
-__device__ __forceinline__ int wrap_slot(int s, int map) {
-  return s >= map ? s - map : (s < 0 ? s + map : s);
-}
-
-__device__ __forceinline__ bool inside(int r, int h) { return abs(r) <= h; }
 
 // One ray, op for op as rayCastUpdateKernel (kernels.cu:44-151), with the
 // window test and hash kept incrementally and the walk cut short once the
@@ -28,131 +21,35 @@ template <bool kAccount = false>
 __device__ __forceinline__ bool cast_one(const RayParams &p, float ex,
                                          float ey, float ez, uint32_t &u_incs,
                                          uint32_t &h_incs) {
-  const float ox = p.o[0], oy = p.o[1], oz = p.o[2];
-  float dx = fsub(ex, ox), dy = fsub(ey, oy), dz = fsub(ez, oz);
-  float L = fsqrt(sos(dx, dy, dz, (p.fp >> kFpRaySosShift) & 7u));
-  if (L < 1e-6f || !isfinite(L) || !isfinite(ex) || !isfinite(ey) ||
-      !isfinite(ez))
-    return false;
-  const bool clipped = L > p.max_range;
-  if (clipped) {
-    const float s = fdiv(p.max_range, L);
-    if (p.fp & kFpClipFma) {
-      ex = ffma(dx, s, ox);
-      ey = ffma(dy, s, oy);
-      ez = ffma(dz, s, oz);
-    } else {
-      ex = fadd(ox, fmul(dx, s));
-      ey = fadd(oy, fmul(dy, s));
-      ez = fadd(oz, fmul(dz, s));
-    }
-    dx = fmul(dx, s);
-    dy = fmul(dy, s);
-    dz = fmul(dz, s);
-    L = p.max_range;
-  }
-  const float invL = fdiv(1.0f, L);
-  const float u[3] = {fmul(dx, invL), fmul(dy, invL), fmul(dz, invL)};
-  const float oo[3] = {ox, oy, oz};
-  const float ee[3] = {ex, ey, ez};
-  const bool ctr = p.ctr != 0;
-  int id[3], en[3], st[3], rel[3], slot[3];
-  float tD[3], tM[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    id[a] = pos_to_global_dev(oo[a], p.inv, ctr, p.fp);
-    en[a] = pos_to_global_dev(ee[a], p.inv, ctr, p.fp);
-    st[a] = (u[a] > 0.0f) - (u[a] < 0.0f);
-    tD[a] = st[a] == 0 ? inf_f() : fabsf(fdiv(p.res, u[a]));
-    float t;
-    if (ctr) {
-      t = fadd(static_cast<float>(id[a]), fmul(0.5f, static_cast<float>(st[a])));
-    } else {
-      t = fadd(static_cast<float>(id[a]), static_cast<float>(st[a] > 0));
-    }
-    const float num = (p.fp & kFpBoundFma) ? ffma(t, p.res, -oo[a])
-                                           : fsub(fmul(t, p.res), oo[a]);
-    tM[a] = st[a] == 0 ? inf_f() : fdiv(num, u[a]);
-    rel[a] = id[a] - p.win[a];
-    slot[a] = global_to_local(id[a], p.map[a], p.half[a]) + p.half[a];
-  }
-  const int max_steps = abs(en[0] - id[0]) + abs(en[1] - id[1]) +
-                        abs(en[2] - id[2]) + 4;
-  const int ny = p.map[1], nz = p.map[2];
+  RayWalk w;
+  if (!ray_begin(p, ex, ey, ez, w)) return false;
   uint32_t incs = 0;
-  for (int step = 0; step < max_steps; ++step) {
-    if (id[0] == en[0] && id[1] == en[1] && id[2] == en[2]) break;
+  for (int step = 0; step < w.max_steps; ++step) {
+    if (at_end(w)) break;
     if (kAccount) {
       ++incs;
-    } else {
-    const bool in0 = inside(rel[0], p.half[0]);
-    const bool in1 = inside(rel[1], p.half[1]);
-    const bool in2 = inside(rel[2], p.half[2]);
-    if (in0 && in1 && in2) {
-      const int h = (slot[0] * ny + slot[1]) * nz + slot[2];
-      if (static_cast<unsigned>(h) < static_cast<unsigned>(p.vnum)) {
-        atomicAdd(p.cnt + h, 1u);
-        ++incs;
-      } else {
-        atomicOr(p.err, kErrHashRange);
-      }
-    } else {
-      // Outside on some axis and not moving back: nothing left to count.
-      if ((!in0 && rel[0] * st[0] >= 0) || (!in1 && rel[1] * st[1] >= 0) ||
-          (!in2 && rel[2] * st[2] >= 0))
-        break;
+    } else if (in_window(w, p)) {
+      atomicAdd(p.cnt + walk_hash(w, p), 1u);
+      ++incs;
+    } else if (left_for_good(w, p)) {
+      break;
     }
-    }
-    int a;
-    if (tM[0] < tM[1]) {
-      a = tM[0] < tM[2] ? 0 : 2;
-    } else {
-      a = tM[1] < tM[2] ? 1 : 2;
-    }
-    // Select-by-index keeps the three axes in registers.
-    if (a == 0) {
-      id[0] += st[0];
-      rel[0] += st[0];
-      slot[0] = wrap_slot(slot[0] + st[0], p.map[0]);
-      tM[0] = fadd(tM[0], tD[0]);
-    } else if (a == 1) {
-      id[1] += st[1];
-      rel[1] += st[1];
-      slot[1] = wrap_slot(slot[1] + st[1], p.map[1]);
-      tM[1] = fadd(tM[1], tD[1]);
-    } else {
-      id[2] += st[2];
-      rel[2] += st[2];
-      slot[2] = wrap_slot(slot[2] + st[2], p.map[2]);
-      tM[2] = fadd(tM[2], tD[2]);
-    }
+    ray_step(w, p);
   }
   if (kAccount) {
     u_incs += incs + 1;
     return true;
   }
   // Endpoint: op, and hit unless clipped (kernels.cu:139-151).
-  if (inside(en[0] - p.win[0], p.half[0]) &&
-      inside(en[1] - p.win[1], p.half[1]) &&
-      inside(en[2] - p.win[2], p.half[2])) {
-    const int h = ((global_to_local(en[0], p.map[0], p.half[0]) + p.half[0]) *
-                       ny +
-                   (global_to_local(en[1], p.map[1], p.half[1]) + p.half[1])) *
-                      nz +
-                  (global_to_local(en[2], p.map[2], p.half[2]) + p.half[2]);
-    if (static_cast<unsigned>(h) < static_cast<unsigned>(p.vnum)) {
-      if (clipped) {
-        atomicAdd(p.cnt + h, 1u);
-      } else {
-        atomicAdd(p.cnt + h, 1u);
-        atomicOr(p.cnt + h, kHitFlag);
-        atomicAdd(p.hit + h, 1u);
-        ++h_incs;
-      }
-      ++incs;
-    } else {
-      atomicOr(p.err, kErrHashRange);
+  const int h = end_hash(w, p);
+  if (h >= 0) {
+    atomicAdd(p.cnt + h, 1u);
+    if (!w.clipped) {
+      atomicOr(p.cnt + h, kHitFlag);
+      atomicAdd(p.hit + h, 1u);
+      ++h_incs;
     }
+    ++incs;
   }
   u_incs += incs;
   return true;

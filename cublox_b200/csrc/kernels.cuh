@@ -87,6 +87,19 @@ struct QueryParams {
 };
 
 void launch_raycast(const RayParams &p, cudaStream_t s);
+
+// Scratch of the direction-binned raycast (raycast_binned.cu).
+struct BinnedScratch {
+  int *bins;      // per ray
+  int *hist;      // binned_bins()
+  int *cursor;    // binned_bins()
+  float *sorted;  // 3 * n (SoA)
+};
+int binned_bins();
+// cube: side of the shared-memory counter cube (16 or 32); match: merge
+// duplicate voxel keys within a warp; sort: walk rays in direction order.
+void launch_raycast_binned(const RayParams &p, const BinnedScratch &b, int cube,
+                           bool match, bool sort, cudaStream_t s);
 // Accounting: stats[0] += the reference loop's iterations + 1 per ray.
 void launch_step_count(const RayParams &p, cudaStream_t s);
 void launch_apply(const ApplyParams &p, cudaStream_t s);

@@ -306,3 +306,56 @@ def test_readme_scale_scan_exact():
         o.update(pts, so, threads=8)
     occ = g.export()
     assert same_bits(occ, o.occ())
+
+
+VARIANTS = [dict(raycast=0), dict(raycast=1, cube=32, match=1, sort=1),
+            dict(raycast=1, cube=16, match=0, sort=1), dict(raycast=1, cube=0, match=1, sort=0),
+            dict(raycast=1, cube=32, match=1, sort=0)]
+
+
+def set_variant(g, v):
+    g.set_option(C.OPT_RAYCAST, v["raycast"])
+    if v["raycast"]:
+        g.set_option(C.OPT_CUBE, v["cube"])
+        g.set_option(C.OPT_MATCH, v["match"])
+        g.set_option(C.OPT_SORT, v["sort"])
+
+
+@pytest.mark.parametrize("v", VARIANTS, ids=lambda v: "-".join(f"{k}{x}" for k, x in v.items()))
+def test_raycast_variants_exact(small, v):
+    """Every kernel variant gives the oracle's counts, stats and map."""
+    w, pts, s = small
+    rng = np.random.default_rng(11)
+    extra = (s + rng.uniform(-25, 25, (5000, 3))).astype(np.float32)
+    extra[:100] = s  # zero-length rays
+    extra[100:200] = s + np.float32([0.01, 0.0, 0.0])
+    cloud = np.concatenate([pts, extra, np.float32([[np.nan, 0, 0], [np.inf, 0, 1]])])
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    set_variant(g, v)
+    g.set_origin_index((3, -2, 18))
+    o.set_origin_index((3, -2, 18))
+    op, hit = g.count_scan(cloud, s)
+    o.raycast(cloud, s)
+    assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit())
+    o.apply()
+    g.enable_stats(True)
+    g.update(cloud, s)
+    st = o.update(cloud, s)
+    assert same_bits(g.export(), o.occ())
+    gs = g.last_stats()
+    assert gs["rays"] == st["rays"] and gs["op_incs"] == st["op_incs"]
+    assert gs["hit_incs"] == st["hit_incs"] and gs["touched"] == st["touched"]
+    assert g.check() == 0
+
+
+@pytest.mark.parametrize("v", VARIANTS[1:3], ids=["cube32", "cube16"])
+def test_raycast_variants_readme_scale(v):
+    w = synth.readme_scale(1)
+    pts, so = w.scan(0), w.sensor_origin(0)
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    set_variant(g, v)
+    g.set_origin_index((250, 0, 18))
+    o.set_origin_index((250, 0, 18))
+    op, hit = g.count_scan(pts, so)
+    o.raycast(pts, so, threads=8)
+    assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit())
