@@ -104,10 +104,12 @@ struct cublox_grid {
   int recenter_mode = 0;
   bool stats_on = false;
   // kernel options (cublox_grid_set_option)
-  int opt_raycast = 1;  // 0 one thread per ray, 1 direction-binned walk
+  int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
+  int opt_seg = 48;     // split walk: target in-window steps per lane
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
-  int opt_match = 1;    // merge duplicate voxels within a warp
+  int opt_match = 0;    // merge duplicate voxels within a warp
   int opt_sort = 1;     // walk rays in direction-bin order
+  int *d_work = nullptr;  // split-walk work counter
   int *d_bins = nullptr;
   int *d_hist = nullptr;
   float *d_sorted = nullptr;
@@ -160,6 +162,7 @@ static void free_all(cublox_grid *g) {
   cudaFree(g->d_masks);
   cudaFree(g->d_cloud);
   cudaFree(g->d_bins);
+  cudaFree(g->d_work);
   cudaFree(g->d_hist);
   cudaFree(g->d_sorted);
   cudaFree(g->d_fq);
@@ -331,8 +334,12 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
   if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
   switch (key) {
     case CUBLOX_OPT_RAYCAST:
-      if (value != 0 && value != 1) break;
+      if (value < 0 || value > 2) break;
       g->opt_raycast = value;
+      return CUBLOX_OK;
+    case CUBLOX_OPT_SEGMENT:
+      if (value < 4 || value > 100000) break;
+      g->opt_seg = value;
       return CUBLOX_OK;
     case CUBLOX_OPT_CUBE:
       if (value != 0 && value != 16 && value != 32) break;
@@ -357,6 +364,7 @@ int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
     case CUBLOX_OPT_CUBE: *value = g->opt_cube; return CUBLOX_OK;
     case CUBLOX_OPT_MATCH: *value = g->opt_match; return CUBLOX_OK;
     case CUBLOX_OPT_SORT: *value = g->opt_sort; return CUBLOX_OK;
+    case CUBLOX_OPT_SEGMENT: *value = g->opt_seg; return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "get_option: unknown key");
@@ -456,7 +464,28 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
     g->bin_cap = n;
   }
   tmark(g, 0, 0);
-  if (g->opt_raycast == 1) {
+  if (g->opt_raycast == 2 && p.stride != 1) {
+    // the split walk reads SoA: gather an AoS cloud first
+    int rc = ensure_cloud(g, n);
+    if (rc) return rc;
+    if (dx != g->d_cloud) {
+      launch_gather_soa(dx, CUBLOX_LAYOUT_AOS, n, g->d_cloud, g->stream);
+      CK_LAUNCH();
+      p.x = g->d_cloud;
+      p.y = g->d_cloud + n;
+      p.z = g->d_cloud + 2 * static_cast<size_t>(n);
+      p.stride = 1;
+    }
+  }
+  if (g->opt_raycast == 2 && !g->d_work) {
+    if (cudaMalloc(&g->d_work, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "update: work counter allocation failed");
+    }
+  }
+  if (g->opt_raycast == 2) {
+    launch_raycast_split(p, g->opt_cube, g->opt_seg, g->d_work, g->stream);
+  } else if (g->opt_raycast == 1) {
     BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};
     launch_raycast_binned(p, b, g->opt_cube, g->opt_match != 0, g->opt_sort != 0, g->stream);
   } else {

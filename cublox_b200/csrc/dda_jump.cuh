@@ -1,0 +1,136 @@
+// Exact jump-ahead through a rounded running sum s_{j+1} = fl(s_j + d).
+//
+// The Amanatides–Woo walk keeps, per axis, tM <- fl(tM + tD) (kernels.cu:
+// 123-135).  Splitting one ray between several lanes needs the walk state
+// at an arbitrary point, i.e. s_j for large j, bit for bit.  Summing j times
+// is what the split avoids; instead:
+//
+// Within one binade [2^e, 2^(e+1)) every float is a multiple of the ulp u,
+// so for s_j in the binade with s_j + d < 2^(e+1):
+//   fl(s_j + d) = s_j + (d rounded to a multiple of u),
+// with ties to even.  The increment is therefore the same for every step
+// after the first one in a binade (a tie can flip it once, after which the
+// sum's parity is fixed), and the whole stretch is an arithmetic progression
+// whose terms are exact in FP32.  Only the step that leaves the binade (or
+// one starting at or below zero) needs a real rounded add.  A query costs
+// O(number of binades crossed) adds and a few exact FP64 divisions.
+//
+// Everything here is __host__ __device__ and plain IEEE arithmetic, so the
+// CPU test (tests/cpp/test_dda_jump.cpp) checks the same code the kernels run.
+#pragma once
+
+#include <cstdint>
+
+#include "exact_fp.cuh"
+
+namespace cublox_b200 {
+
+struct JumpResult {
+  int64_t j;  // index reached
+  float s;    // s_j
+  bool ok;    // false: the sum stalls (d below half an ulp) before the target
+};
+
+CBX_HD int f32_exponent(float v) {  // unbiased exponent of a positive normal
+#if defined(__CUDA_ARCH__)
+  return ((__float_as_uint(v) >> 23) & 0xff) - 127;
+#else
+  uint32_t b;
+  __builtin_memcpy(&b, &v, 4);
+  return static_cast<int>((b >> 23) & 0xff) - 127;
+#endif
+}
+
+CBX_HD bool f32_is_normal_pos(float v) {
+  return v >= 1.17549435e-38f && v < 3.4028234e38f;
+}
+
+// Exact 2^k as float for k in [-126, 127].
+CBX_HD float f32_pow2(int k) {
+  const uint32_t b = static_cast<uint32_t>(k + 127) << 23;
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(b);
+#else
+  float v;
+  __builtin_memcpy(&v, &b, 4);
+  return v;
+#endif
+}
+
+// Exact steps from v stay on the grid of v's binade: with |v| in
+// [2^e, 2^(e+1)) and ulp u, in units of u (V = v/u, Dd = d/u exactly):
+//   v > 0: V + Dd < 2^24      (the sum stays below 2^(e+1))
+//   v < 0: V + Dd <= -2^23    (the sum keeps magnitude >= 2^e)
+CBX_HD bool on_grid_step(double V, double Dd, bool neg) {
+  return neg ? (V + Dd <= -8388608.0) : (V + Dd < 16777216.0);
+}
+
+// Smallest j >= 0 with s_j >= tau (the sequence starts at s_0 = s0), and s_j.
+// Also stops at j == jmax (returning s_jmax) so callers can bound work.
+// d must be > 0 and finite; s0 may be any non-NaN value.
+CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax) {
+  JumpResult r{0, s0, true};
+  for (int guard = 0; guard < 4096; ++guard) {
+    if (r.s >= tau || r.j >= jmax) return r;
+    const float s1 = fadd(r.s, d);
+    if (s1 == r.s) {  // stalled: never reaches tau
+      r.ok = false;
+      return r;
+    }
+    r.j += 1;
+    r.s = s1;
+    if (r.s >= tau || r.j >= jmax) return r;
+    const float mag = r.s < 0.0f ? -r.s : r.s;
+    if (!f32_is_normal_pos(mag)) continue;  // zero, subnormal or infinite
+    const bool neg = r.s < 0.0f;
+    const int e = f32_exponent(mag);
+    if (e > 126 || e < -100) continue;
+    const double u = static_cast<double>(f32_pow2(e - 23));
+    const double Dd = static_cast<double>(d) / u;
+    // A second on-grid step: if d sits exactly halfway between two ulp
+    // multiples, it rounds the sum to an even multiple, after which every
+    // on-grid step rounds the same way.
+    if (!on_grid_step(static_cast<double>(r.s) / u, Dd, neg)) continue;
+    const float s2 = fadd(r.s, d);
+    r.j += 1;
+    r.s = s2;
+    if (r.s >= tau || r.j >= jmax) return r;
+    if (!on_grid_step(static_cast<double>(r.s) / u, Dd, neg)) continue;
+    const float s3 = fadd(r.s, d);
+    const float delta = fsub(s3, r.s);  // exact: both on the ulp grid
+    if (!(delta > 0.0f)) continue;
+    const double S = static_cast<double>(r.s) / u;
+    const double D = static_cast<double>(delta) / u;
+    // m = number of on-grid steps from here = #{k >= 0 : S + k D on grid}
+    const double lim = neg ? (-8388608.0 - Dd) : (16777216.0 - Dd);
+    double mk = (lim - S) / D;
+    int64_t m = mk > 0.0 ? static_cast<int64_t>(mk) : 0;
+    while (m > 0 && !on_grid_step(S + static_cast<double>(m - 1) * D, Dd, neg)) --m;
+    while (on_grid_step(S + static_cast<double>(m) * D, Dd, neg)) ++m;
+    if (m <= 0) continue;
+    // Within the stretch s_{j+k} = r.s + k*delta.  First k with value >= tau.
+    int64_t kt;
+    if (tau > 3.4028234e38f) {
+      kt = m + 1;
+    } else {
+      const double T = static_cast<double>(tau) / u;
+      const double kk = (T - S) / D;
+      kt = kk > 0.0 ? (kk < static_cast<double>(m + 1) ? static_cast<int64_t>(kk) : m + 1) : 0;
+      while (kt > 0 && S + static_cast<double>(kt - 1) * D >= T) --kt;
+      while (kt <= m && S + static_cast<double>(kt) * D < T) ++kt;
+    }
+    int64_t k = kt < m ? kt : m;
+    if (jmax - r.j < k) k = jmax - r.j;
+    r.s = fadd(r.s, fmul(static_cast<float>(k), delta));  // exact
+    r.j += k;
+  }
+  r.ok = false;
+  return r;
+}
+
+// s_j for a given j (jump by index).
+CBX_HD JumpResult value_at(float s0, float d, int64_t j) {
+  return first_at_or_above(s0, d, 3.4028235e38f * 2.0f, j);
+}
+
+}  // namespace cublox_b200

@@ -20,6 +20,7 @@ constexpr uint32_t kOpMask = 0x7fffffffu;
 // Error-word bits (never expected; set instead of trapping).
 constexpr uint32_t kErrHashRange = 1u << 0;
 constexpr uint32_t kErrFetchOverflow = 1u << 1;
+constexpr uint32_t kErrJumpStall = 1u << 2;
 
 struct RayParams {
   const float *x, *y, *z;  // point i is (x[i*stride], y[i*stride], z[i*stride])
@@ -96,6 +97,11 @@ struct BinnedScratch {
   float *sorted;  // 3 * n (SoA)
 };
 int binned_bins();
+// Warp-cooperative exact walk (raycast_split.cu): rays longer than seg_len
+// in-window steps are cut into time segments walked by separate lanes.
+// counter: one device int of scratch (work queue).
+void launch_raycast_split(const RayParams &p, int cube, int seg_len, int *counter,
+                          cudaStream_t s);
 // cube: side of the shared-memory counter cube (16 or 32); match: merge
 // duplicate voxel keys within a warp; sort: walk rays in direction order.
 void launch_raycast_binned(const RayParams &p, const BinnedScratch &b, int cube,

@@ -39,6 +39,12 @@ namespace cublox {
 
 using PointCloud = Eigen::Matrix<float, Eigen::Dynamic, 3>;
 
+// Probability -> log-odds, clamped to [1e-6, 1 - 1e-6] (utils.hpp:185-188).
+inline float logit(const float p) {
+  const float pc = std::clamp(p, 1.0e-6f, 1.0f - 1.0e-6f);
+  return std::log(pc / (1.0f - pc));
+}
+
 namespace detail {
 inline void ok(int rc, const char *what) {
   if (rc != CUBLOX_OK)

@@ -85,11 +85,13 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 /* Kernel choices (no reference counterpart; results are identical for
  * every choice, only speed differs).                                       */
 #define CUBLOX_OPT_RAYCAST 1 /* 0: one thread per ray; 1: direction-binned
-                                warp walk (default)                        */
+                                warp walk; 2: rays split between lanes at
+                                exact time cuts (default)                  */
 #define CUBLOX_OPT_CUBE 2    /* shared-memory counter cube side around the
                                 sensor: 0, 16 or 32 (default 32)            */
-#define CUBLOX_OPT_MATCH 3   /* merge duplicate voxels per warp (default 1) */
+#define CUBLOX_OPT_MATCH 3   /* merge duplicate voxels per warp (default 0) */
 #define CUBLOX_OPT_SORT 4    /* walk rays in direction order (default 1)    */
+#define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (48)   */
 int cublox_grid_set_option(cublox_grid *g, int key, int value);
 int cublox_grid_get_option(const cublox_grid *g, int key, int *value);
 

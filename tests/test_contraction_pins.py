@@ -34,7 +34,7 @@ def test_ref_ray_sites_pinned(ray_scenarios):
         names = [P.describe(m) for m in got]
         assert got, f"{sc.name}: no candidate pattern reproduces the reference"
         pinned = _ray_bits(O.FP_PINNED)
-        assert {m & ~CENTER_AGNOSTIC for m in got} == {pinned & ~CENTER_AGNOSTIC}, names
+        assert {_ray_bits(m) & ~CENTER_AGNOSTIC for m in got} == {pinned & ~CENTER_AGNOSTIC}, names
 
 
 def test_ref_apply_sites_pinned():

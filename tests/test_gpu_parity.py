@@ -310,15 +310,19 @@ def test_readme_scale_scan_exact():
 
 VARIANTS = [dict(raycast=0), dict(raycast=1, cube=32, match=1, sort=1),
             dict(raycast=1, cube=16, match=0, sort=1), dict(raycast=1, cube=0, match=1, sort=0),
-            dict(raycast=1, cube=32, match=1, sort=0)]
+            dict(raycast=2, cube=32, seg=48), dict(raycast=2, cube=0, seg=4),
+            dict(raycast=2, cube=16, seg=7)]
 
 
 def set_variant(g, v):
     g.set_option(C.OPT_RAYCAST, v["raycast"])
     if v["raycast"]:
         g.set_option(C.OPT_CUBE, v["cube"])
+    if v["raycast"] == 1:
         g.set_option(C.OPT_MATCH, v["match"])
         g.set_option(C.OPT_SORT, v["sort"])
+    if v["raycast"] == 2:
+        g.set_option(C.OPT_SEGMENT, v["seg"])
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=lambda v: "-".join(f"{k}{x}" for k, x in v.items()))
@@ -337,7 +341,8 @@ def test_raycast_variants_exact(small, v):
     op, hit = g.count_scan(cloud, s)
     o.raycast(cloud, s)
     assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit())
-    o.apply()
+    o.op()[:] = 0  # count_scan leaves the map untouched: drop the counts
+    o.hit()[:] = 0
     g.enable_stats(True)
     g.update(cloud, s)
     st = o.update(cloud, s)
@@ -348,7 +353,8 @@ def test_raycast_variants_exact(small, v):
     assert g.check() == 0
 
 
-@pytest.mark.parametrize("v", VARIANTS[1:3], ids=["cube32", "cube16"])
+@pytest.mark.parametrize("v", [VARIANTS[1], VARIANTS[4], VARIANTS[5]],
+                         ids=["binned32", "split48", "split4"])
 def test_raycast_variants_readme_scale(v):
     w = synth.readme_scale(1)
     pts, so = w.scan(0), w.sensor_origin(0)
@@ -359,3 +365,25 @@ def test_raycast_variants_readme_scale(v):
     op, hit = g.count_scan(pts, so)
     o.raycast(pts, so, threads=8)
     assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit())
+
+
+def test_split_walk_many_geometries():
+    """The split walk on tiny segments over varied grids, resolutions and
+    binnings: every ray is cut at many exact time points."""
+    rng = np.random.default_rng(12)
+    for half, res, ctr in [((40, 40, 40), 0.1, False), ((30, 50, 20), 0.07, True),
+                           ((64, 64, 16), 0.05, False), ((25, 25, 25), 0.3, True)]:
+        g, o = pair(half, res, ctr=ctr, max_range=float(np.float32(res) * 60))
+        g.set_option(C.OPT_RAYCAST, 2)
+        g.set_option(C.OPT_SEGMENT, 4)
+        s = rng.uniform(-1, 1, 3).astype(np.float32) * np.float32(res) * 3
+        g.set_origin_index((1, -2, 0))
+        o.set_origin_index((1, -2, 0))
+        d = rng.normal(size=(20000, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        r = rng.uniform(0.01, 1.0, (20000, 1)) * float(np.float32(res) * 90)
+        pts = (s + d * r).astype(np.float32)
+        op, hit = g.count_scan(pts, s)
+        o.raycast(pts, s)
+        assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit()), (half, res, ctr)
+        assert g.check() == 0
