@@ -106,10 +106,14 @@ struct cublox_grid {
   // kernel options (cublox_grid_set_option)
   int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
   int opt_seg = 48;     // split walk: target in-window steps per lane
+  int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
   int opt_match = 0;    // merge duplicate voxels within a warp
   int opt_sort = 1;     // walk rays in direction-bin order
-  int *d_work = nullptr;  // split-walk work counter
+  void *d_segs = nullptr;  // split walk: segment records
+  void *d_rays = nullptr;  // split walk: ray records
+  int *d_work = nullptr;   // split walk: 2 counters
+  int split_cap = 0;       // rays the split scratch holds
   int *d_bins = nullptr;
   int *d_hist = nullptr;
   float *d_sorted = nullptr;
@@ -163,6 +167,8 @@ static void free_all(cublox_grid *g) {
   cudaFree(g->d_cloud);
   cudaFree(g->d_bins);
   cudaFree(g->d_work);
+  cudaFree(g->d_segs);
+  cudaFree(g->d_rays);
   cudaFree(g->d_hist);
   cudaFree(g->d_sorted);
   cudaFree(g->d_fq);
@@ -341,6 +347,10 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
       if (value < 4 || value > 100000) break;
       g->opt_seg = value;
       return CUBLOX_OK;
+    case CUBLOX_OPT_FOLD:
+      if (value != 0 && value != 1) break;
+      g->opt_fold = value;
+      return CUBLOX_OK;
     case CUBLOX_OPT_CUBE:
       if (value != 0 && value != 16 && value != 32) break;
       g->opt_cube = value;
@@ -365,6 +375,7 @@ int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
     case CUBLOX_OPT_MATCH: *value = g->opt_match; return CUBLOX_OK;
     case CUBLOX_OPT_SORT: *value = g->opt_sort; return CUBLOX_OK;
     case CUBLOX_OPT_SEGMENT: *value = g->opt_seg; return CUBLOX_OK;
+    case CUBLOX_OPT_FOLD: *value = g->opt_fold; return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "get_option: unknown key");
@@ -477,14 +488,26 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
       p.stride = 1;
     }
   }
-  if (g->opt_raycast == 2 && !g->d_work) {
-    if (cudaMalloc(&g->d_work, sizeof(int)) != cudaSuccess) {
+  constexpr int kMaxSegsPerRay = 16;
+  if (g->opt_raycast == 2 && (n > g->split_cap || !g->d_work)) {
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(g->d_segs);
+    cudaFree(g->d_rays);
+    g->d_segs = nullptr;
+    g->d_rays = nullptr;
+    g->split_cap = 0;
+    if ((!g->d_work && cudaMalloc(&g->d_work, 2 * sizeof(int)) != cudaSuccess) ||
+        cudaMalloc(&g->d_segs, split_seg_bytes() * kMaxSegsPerRay * static_cast<size_t>(n)) !=
+            cudaSuccess ||
+        cudaMalloc(&g->d_rays, split_ray_bytes() * static_cast<size_t>(n)) != cudaSuccess) {
       cudaGetLastError();
-      return fail(CUBLOX_ERR_NOMEM, "update: work counter allocation failed");
+      return fail(CUBLOX_ERR_NOMEM, "update: split-walk scratch allocation failed");
     }
+    g->split_cap = n;
   }
   if (g->opt_raycast == 2) {
-    launch_raycast_split(p, g->opt_cube, g->opt_seg, g->d_work, g->stream);
+    SplitScratch sc{g->d_segs, g->d_rays, g->d_work, kMaxSegsPerRay * n, kMaxSegsPerRay};
+    launch_raycast_split(p, g->opt_cube, g->opt_seg, sc, g->stream);
   } else if (g->opt_raycast == 1) {
     BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};
     launch_raycast_binned(p, b, g->opt_cube, g->opt_match != 0, g->opt_sort != 0, g->stream);
@@ -506,6 +529,7 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   a.l_unknown = g->l_unknown;
   a.fp = g->fp;
   a.stats = g->stats_on ? g->d_stats : nullptr;
+  a.variant = g->opt_fold;
   tmark(g, 1, 0);
   launch_apply(a, g->stream);
   CK_LAUNCH();

@@ -47,6 +47,7 @@ struct ApplyParams {
   float l_hit, l_miss, l_min, l_max, l_unknown;
   unsigned fp;
   unsigned long long *stats;  // [3] += touched
+  int variant;                // 0 scalar sweep, 1 vector sweep
 };
 
 struct ClearParams {
@@ -99,8 +100,16 @@ struct BinnedScratch {
 int binned_bins();
 // Warp-cooperative exact walk (raycast_split.cu): rays longer than seg_len
 // in-window steps are cut into time segments walked by separate lanes.
-// counter: one device int of scratch (work queue).
-void launch_raycast_split(const RayParams &p, int cube, int seg_len, int *counter,
+struct SplitScratch {
+  void *segs;     // seg_cap segment records (split_seg_bytes() each)
+  void *rays;     // n ray records (split_ray_bytes() each)
+  int *counters;  // 2 ints: segments planned, work queue
+  int seg_cap;
+  int max_segs;   // per ray
+};
+size_t split_seg_bytes();
+size_t split_ray_bytes();
+void launch_raycast_split(const RayParams &p, int cube, int seg_len, const SplitScratch &sc,
                           cudaStream_t s);
 // cube: side of the shared-memory counter cube (16 or 32); match: merge
 // duplicate voxel keys within a warp; sort: walk rays in direction order.

@@ -158,187 +158,251 @@ struct Emitter {
   }
 };
 
-// Walk segment k of K of one ray.  Returns false if the ray is dropped.
-template <int S>
-__device__ bool walk_segment(const RayParams &p, float ex, float ey, float ez, int k,
-                             const Cuts &cuts, Emitter<S> &em, uint32_t &hits) {
+// ---- planned split ------------------------------------------------------
+// Per ray (plan kernel, one thread per ray): the exact setup, the cuts, and
+// every segment's start state, computed by continuing each axis's jump from
+// the previous cut (so each axis's binades are walked once per ray).  Per
+// segment (walk kernel, one lane per segment from a global queue): load the
+// start state and walk until the next cut.
+
+struct SegRec {     // 48 bytes
+  int ray;
+  int i;            // index of the start state
+  int id[3];        // start voxel
+  float tM[3];      // per-axis next event times
+  float tau_next;   // the segment owns events with T < tau_next
+  int k;            // segment number within the ray
+  int pad[2];
+};
+
+struct RayRec {     // 48 bytes
+  int en[3];
+  int st[3];
+  float tD[3];
+  int max_steps;
+  int L1;
+  int flags;        // bit0 clipped, bit1 state L1 is the end voxel
+};
+
+__global__ void __launch_bounds__(256) seg_plan_kernel(const RayParams p, int seg_len,
+                                                       int max_segs, SegRec *segs,
+                                                       RayRec *rays, int *seg_count,
+                                                       int seg_cap) {
+  __shared__ int warp_tot[8];
+  __shared__ int block_base;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   RayWalk w;
-  if (!ray_begin(p, ex, ey, ez, w)) return false;
-  const int L1 = abs(w.en[0] - w.id[0]) + abs(w.en[1] - w.id[1]) + abs(w.en[2] - w.id[2]);
-  int64_t i = 0;  // index of the current state
-  int ended = -1; // unknown
-  RayWalk w0;
-  if (k > 0) {
-    w0 = w;
-    const float tau = cut_time(cuts, k);
+  bool valid = false;
+  Cuts cuts{0.0f, 0.0f, 0};
+  float ex = 0.0f, ey = 0.0f, ez = 0.0f;
+  if (i < p.n) {
+    const size_t k = static_cast<size_t>(i) * p.stride;
+    ex = p.x[k];
+    ey = p.y[k];
+    ez = p.z[k];
+    valid = ray_begin(p, ex, ey, ez, w);
+    if (valid) {
+      cuts = plan_cuts(p, w, ex, ey, ez, seg_len);
+      if (cuts.K > max_segs) cuts.K = max_segs;
+    }
+  }
+  int K = valid ? cuts.K : 0;
+  // block-wide exclusive scan of K, one global reservation per block
+  int incl = K;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int q = 0; q < static_cast<int>(blockDim.x >> 5); ++q) {
+      const int t = warp_tot[q];
+      warp_tot[q] = run;
+      run += t;
+    }
+    block_base = atomicAdd(seg_count, run);
+  }
+  __syncthreads();
+  int base = block_base + warp_tot[warp] + incl - K;
+  if (!valid) return;
+  if (base + K > seg_cap) {  // never expected: capacity is n * max_segs
+    atomicOr(p.err, kErrFetchOverflow);
+    return;
+  }
+  RayRec rr;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    rr.en[a] = w.en[a];
+    rr.st[a] = w.st[a];
+    rr.tD[a] = w.tD[a];
+  }
+  rr.max_steps = w.max_steps;
+  rr.L1 = abs(w.en[0] - w.id[0]) + abs(w.en[1] - w.id[1]) + abs(w.en[2] - w.id[2]);
+  rr.flags = (w.clipped ? 1 : 0) | ((K > 1 && reaches_end(w)) ? 2 : 0);
+  rays[i] = rr;
+  // segment start states, cut by cut
+  int64_t jc[3] = {0, 0, 0};
+  float sc[3] = {w.tM[0], w.tM[1], w.tM[2]};
+  for (int k = 0; k < K; ++k) {
+    SegRec sr;
+    sr.ray = i;
+    sr.k = k;
+    sr.tau_next = cut_time(cuts, k + 1);
+    int64_t idx = 0;
+    if (k > 0) {
+      const float tau = cut_time(cuts, k);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (w.st[a] == 0) continue;
+        const JumpResult r =
+            first_at_or_above(sc[a], w.tD[a], tau, static_cast<int64_t>(w.max_steps) - jc[a]);
+        if (!r.ok) atomicOr(p.err, kErrJumpStall);  // excluded by plan_cuts
+        jc[a] += r.j;
+        sc[a] = r.s;
+      }
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      if (w.st[a] == 0) continue;
-      const JumpResult r = first_at_or_above(w0.tM[a], w0.tD[a], tau, w.max_steps);
-      if (!r.ok) atomicOr(p.err, kErrJumpStall);  // excluded by plan_cuts
-      const int c = static_cast<int>(r.j);
-      i += c;
-      w.tM[a] = r.s;
-      w.id[a] = w0.id[a] + w0.st[a] * c;
-      w.rel[a] = w.id[a] - p.win[a];
-      w.slot[a] = global_to_local(w.id[a], p.map[a], p.half[a]) + p.half[a];
+      idx += jc[a];
+      sr.id[a] = w.id[a] + w.st[a] * static_cast<int>(jc[a]);
+      sr.tM[a] = sc[a];
     }
+    sr.i = idx > w.max_steps ? w.max_steps : static_cast<int>(idx);
+    sr.pad[0] = sr.pad[1] = 0;
+    segs[base + k] = sr;
   }
-  const float tau_next = cut_time(cuts, k + 1);
-  // process the current state (lane 0 owns the initial one)
-  bool go = true;
-  if (k == 0) {
-    if (i >= w.max_steps || at_end(w)) {
-      go = false;
-    } else if (in_window(w, p)) {
-      em.voxel(w);
-    } else if (left_for_good(w, p)) {
-      go = false;
-    }
-  }
-  while (go) {
-    const int a = pick_axis(w);
-    if (axis_time(w, a) >= tau_next) break;
-    if (a == 0) {
-      w.id[0] += w.st[0];
-      w.rel[0] += w.st[0];
-      w.slot[0] = wrap_slot(w.slot[0] + w.st[0], p.map[0]);
-      w.tM[0] = fadd(w.tM[0], w.tD[0]);
-    } else if (a == 1) {
-      w.id[1] += w.st[1];
-      w.rel[1] += w.st[1];
-      w.slot[1] = wrap_slot(w.slot[1] + w.st[1], p.map[1]);
-      w.tM[1] = fadd(w.tM[1], w.tD[1]);
-    } else {
-      w.id[2] += w.st[2];
-      w.rel[2] += w.st[2];
-      w.slot[2] = wrap_slot(w.slot[2] + w.st[2], p.map[2]);
-      w.tM[2] = fadd(w.tM[2], w.tD[2]);
-    }
-    ++i;
-    if (i >= w.max_steps) break;
-    if (i >= L1) {
-      // Only state L1 can be the end voxel; past it, the walk went on only
-      // if state L1 was not the end.
-      if (i == L1) {
-        if (at_end(w)) break;
-      } else {
-        if (ended < 0) ended = (k == 0) ? 0 : (reaches_end(w0) ? 1 : 0);
-        if (ended) break;
-      }
-    }
-    if (in_window(w, p)) {
-      em.voxel(w);
-    } else if (left_for_good(w, p)) {
-      break;
-    }
-  }
-  if (k == 0) {
-    // Endpoint (kernels.cu:139-151).
-    const int h = end_hash(w, p);
-    if (h >= 0) {
-      const int c0 = w.en[0] - em.clo0, c1 = w.en[1] - em.clo1, c2 = w.en[2] - em.clo2;
-      if (S > 0 && static_cast<unsigned>(c0) < static_cast<unsigned>(S) &&
-          static_cast<unsigned>(c1) < static_cast<unsigned>(S) &&
-          static_cast<unsigned>(c2) < static_cast<unsigned>(S))
-        atomicAdd(&em.cube[(c0 * S + c1) * S + c2], 1u);
-      else
-        atomicAdd(p.cnt + h, 1u);
-      ++em.incs;
-      if (!w.clipped) {
-        atomicOr(p.cnt + h, kHitFlag);
-        atomicAdd(p.hit + h, 1u);
-        ++hits;
-      }
-    }
-  }
-  return true;
 }
 
 template <int S>
-__global__ void __launch_bounds__(512, 1) split_walk_kernel(const RayParams p, const int cl0,
-                                                            const int cl1, const int cl2,
-                                                            const int seg_len,
-                                                            int *work_counter) {
+__global__ void __launch_bounds__(512) seg_walk_kernel(const RayParams p, const int cl0,
+                                                       const int cl1, const int cl2,
+                                                       const SegRec *segs, const RayRec *rays,
+                                                       const int *seg_count, int *work) {
   extern __shared__ uint32_t cube[];
   constexpr int kCube = S * S * S;
-  for (int i = threadIdx.x; i < kCube / 4; i += blockDim.x)
-    reinterpret_cast<uint4 *>(cube)[i] = make_uint4(0u, 0u, 0u, 0u);
+  for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
+    reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  const int total = *seg_count;
   Emitter<S> em{p, cube, cl0, cl1, cl2, 0u};
-  uint32_t rays = 0, hits = 0;
+  uint32_t nrays = 0, hits = 0;
   for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(work_counter, 32);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= p.n) break;
-    const int i = base + lane;
-    float ex = 0.0f, ey = 0.0f, ez = 0.0f;
-    int K = 0;
-    Cuts cuts{0.0f, 0.0f, 1};
-    if (i < p.n) {
-      ex = p.x[i];
-      ey = p.y[i];
-      ez = p.z[i];
-      RayWalk w;
-      if (ray_begin(p, ex, ey, ez, w)) {
-        cuts = plan_cuts(p, w, ex, ey, ez, seg_len);
-        K = cuts.K;
-        ++rays;
+    int b = 0;
+    if (lane == 0) b = atomicAdd(work, 32);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (b >= total) break;
+    const int g = b + lane;
+    if (g >= total) continue;
+    const SegRec sr = segs[g];
+    const RayRec rr = rays[sr.ray];
+    RayWalk w;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      w.id[a] = sr.id[a];
+      w.en[a] = rr.en[a];
+      w.st[a] = rr.st[a];
+      w.tD[a] = rr.tD[a];
+      w.tM[a] = sr.tM[a];
+      w.rel[a] = w.id[a] - p.win[a];
+      w.slot[a] = global_to_local(w.id[a], p.map[a], p.half[a]) + p.half[a];
+    }
+    w.max_steps = rr.max_steps;
+    w.clipped = rr.flags & 1;
+    const bool ends_at_l1 = (rr.flags & 2) != 0;
+    int i = sr.i;
+    bool go = i < w.max_steps;
+    if (sr.k == 0) {
+      ++nrays;
+      if (!go || at_end(w)) {
+        go = false;
+      } else if (in_window(w, p)) {
+        em.voxel(w);
+      } else if (left_for_good(w, p)) {
+        go = false;
       }
     }
-    // Inclusive warp scan of the segment counts.
-    int incl = K;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, off);
-      if (lane >= off) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    for (int g0 = 0; g0 < total; g0 += 32) {
-      const int g = g0 + lane;
-      // Smallest ray r of the chunk with incl[r] > g.
-      int r = 0;
-#pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const int v = __shfl_sync(0xffffffffu, incl, r + step - 1);
-        if (v <= g) r += step;
+    while (go) {
+      const int a = pick_axis(w);
+      if (axis_time(w, a) >= sr.tau_next) break;
+      if (a == 0) {
+        w.id[0] += w.st[0];
+        w.rel[0] += w.st[0];
+        w.slot[0] = wrap_slot(w.slot[0] + w.st[0], p.map[0]);
+        w.tM[0] = fadd(w.tM[0], w.tD[0]);
+      } else if (a == 1) {
+        w.id[1] += w.st[1];
+        w.rel[1] += w.st[1];
+        w.slot[1] = wrap_slot(w.slot[1] + w.st[1], p.map[1]);
+        w.tM[1] = fadd(w.tM[1], w.tD[1]);
+      } else {
+        w.id[2] += w.st[2];
+        w.rel[2] += w.st[2];
+        w.slot[2] = wrap_slot(w.slot[2] + w.st[2], p.map[2]);
+        w.tM[2] = fadd(w.tM[2], w.tD[2]);
       }
-      const int kr = __shfl_sync(0xffffffffu, K, r);
-      const float rx = __shfl_sync(0xffffffffu, ex, r);
-      const float ry = __shfl_sync(0xffffffffu, ey, r);
-      const float rz = __shfl_sync(0xffffffffu, ez, r);
-      const float tlo = __shfl_sync(0xffffffffu, cuts.t_lo, r);
-      const float thi = __shfl_sync(0xffffffffu, cuts.t_hi, r);
-      const int excl = __shfl_sync(0xffffffffu, incl, r) - kr;
-      if (g < total) {
-        const Cuts rc{tlo, thi, kr};
-        walk_segment<S>(p, rx, ry, rz, g - excl, rc, em, hits);
+      ++i;
+      if (i >= w.max_steps) break;
+      // Only state L1 can be the end voxel; past it the walk continues only
+      // if state L1 was not the end (a segment that started past L1 learns
+      // that from the plan).
+      if (i == rr.L1) {
+        if (at_end(w)) break;
+      } else if (i > rr.L1 && sr.i >= rr.L1 && ends_at_l1) {
+        break;
+      }
+      if (in_window(w, p)) {
+        em.voxel(w);
+      } else if (left_for_good(w, p)) {
+        break;
+      }
+    }
+    if (sr.k == 0) {
+      // Endpoint (kernels.cu:139-151).
+      const int h = end_hash(w, p);
+      if (h >= 0) {
+        const int c0 = w.en[0] - cl0, c1 = w.en[1] - cl1, c2 = w.en[2] - cl2;
+        if (S > 0 && static_cast<unsigned>(c0) < static_cast<unsigned>(S) &&
+            static_cast<unsigned>(c1) < static_cast<unsigned>(S) &&
+            static_cast<unsigned>(c2) < static_cast<unsigned>(S))
+          atomicAdd(&cube[(c0 * S + c1) * S + c2], 1u);
+        else
+          atomicAdd(p.cnt + h, 1u);
+        ++em.incs;
+        if (!w.clipped) {
+          atomicOr(p.cnt + h, kHitFlag);
+          atomicAdd(p.hit + h, 1u);
+          ++hits;
+        }
       }
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kCube; i += blockDim.x) {
-    const uint32_t v = cube[i];
+  if constexpr (S > 0)
+  for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
+    const uint32_t v = cube[q];
     if (!v) continue;
-    const int g[3] = {cl0 + i / (S * S), cl1 + (i / S) % S, cl2 + i % S};
-    const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-                   (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
+    const int gg[3] = {cl0 + q / (S * S), cl1 + (q / S) % S, cl2 + q % S};
+    const int h = ((global_to_local(gg[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
+                   (global_to_local(gg[1], p.map[1], p.half[1]) + p.half[1])) *
                       p.map[2] +
-                  (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+                  (global_to_local(gg[2], p.map[2], p.half[2]) + p.half[2]);
     atomicAdd(p.cnt + h, v);
   }
   if (p.stats) {
     uint32_t incs = em.incs;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      rays += __shfl_down_sync(0xffffffffu, rays, off);
+      nrays += __shfl_down_sync(0xffffffffu, nrays, off);
       incs += __shfl_down_sync(0xffffffffu, incs, off);
       hits += __shfl_down_sync(0xffffffffu, hits, off);
     }
     if (lane == 0) {
-      atomicAdd(p.stats + 0, static_cast<unsigned long long>(rays));
+      atomicAdd(p.stats + 0, static_cast<unsigned long long>(nrays));
       atomicAdd(p.stats + 1, static_cast<unsigned long long>(incs));
       atomicAdd(p.stats + 2, static_cast<unsigned long long>(hits));
     }
@@ -357,37 +421,45 @@ int sm_count_split() {
 }
 
 template <int S>
-void launch_split(const RayParams &p, const int clo[3], int seg_len, int *counter,
-                  cudaStream_t s) {
+void launch_seg_walk(const RayParams &p, const int clo[3], const SplitScratch &sc,
+                     cudaStream_t s) {
   const size_t smem = sizeof(uint32_t) * S * S * S;
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute(split_walk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(seg_walk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
   static int per_sm = 0;
   if (per_sm == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, split_walk_kernel<S>, 512, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, seg_walk_kernel<S>, 512, smem);
     if (per_sm < 1) per_sm = 1;
   }
   const int grid = sm_count_split() * per_sm;
-  split_walk_kernel<S><<<grid, 512, smem, s>>>(p, clo[0], clo[1], clo[2], seg_len, counter);
+  seg_walk_kernel<S><<<grid, 512, smem, s>>>(
+      p, clo[0], clo[1], clo[2], reinterpret_cast<const SegRec *>(sc.segs),
+      reinterpret_cast<const RayRec *>(sc.rays), sc.counters, sc.counters + 1);
 }
 
 }  // namespace
 
-void launch_raycast_split(const RayParams &p, int cube, int seg_len, int *counter,
+size_t split_seg_bytes() { return sizeof(SegRec); }
+size_t split_ray_bytes() { return sizeof(RayRec); }
+
+void launch_raycast_split(const RayParams &p, int cube, int seg_len, const SplitScratch &sc,
                           cudaStream_t s) {
   if (p.n <= 0) return;
-  cudaMemsetAsync(counter, 0, sizeof(int), s);
+  cudaMemsetAsync(sc.counters, 0, 2 * sizeof(int), s);
+  seg_plan_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(
+      p, seg_len, sc.max_segs, reinterpret_cast<SegRec *>(sc.segs),
+      reinterpret_cast<RayRec *>(sc.rays), sc.counters, sc.seg_cap);
   int clo[3];
   const int hc = cube / 2;
   for (int a = 0; a < 3; ++a)
     clo[a] = pos_to_global_dev(p.o[a], p.inv, p.ctr != 0, p.fp) - hc;
   if (cube >= 32)
-    launch_split<32>(p, clo, seg_len, counter, s);
+    launch_seg_walk<32>(p, clo, sc, s);
   else if (cube >= 16)
-    launch_split<16>(p, clo, seg_len, counter, s);
+    launch_seg_walk<16>(p, clo, sc, s);
   else
-    launch_split<0>(p, clo, seg_len, counter, s);
+    launch_seg_walk<0>(p, clo, sc, s);
 }
 
 }  // namespace cublox_b200
