@@ -107,6 +107,7 @@ struct cublox_grid {
   int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
   int opt_seg = 48;     // split walk: target in-window steps per lane
   int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
+  int opt_block = 512;  // split walk CTA size
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
   int opt_match = 0;    // merge duplicate voxels within a warp
   int opt_sort = 1;     // walk rays in direction-bin order
@@ -351,6 +352,10 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
       if (value != 0 && value != 1) break;
       g->opt_fold = value;
       return CUBLOX_OK;
+    case CUBLOX_OPT_BLOCK:
+      if (value != 256 && value != 512 && value != 1024) break;
+      g->opt_block = value;
+      return CUBLOX_OK;
     case CUBLOX_OPT_CUBE:
       if (value != 0 && value != 16 && value != 32) break;
       g->opt_cube = value;
@@ -376,6 +381,7 @@ int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
     case CUBLOX_OPT_SORT: *value = g->opt_sort; return CUBLOX_OK;
     case CUBLOX_OPT_SEGMENT: *value = g->opt_seg; return CUBLOX_OK;
     case CUBLOX_OPT_FOLD: *value = g->opt_fold; return CUBLOX_OK;
+    case CUBLOX_OPT_BLOCK: *value = g->opt_block; return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "get_option: unknown key");
@@ -506,7 +512,8 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
     g->split_cap = n;
   }
   if (g->opt_raycast == 2) {
-    SplitScratch sc{g->d_segs, g->d_rays, g->d_work, kMaxSegsPerRay * n, kMaxSegsPerRay};
+    SplitScratch sc{g->d_segs, g->d_rays, g->d_work, kMaxSegsPerRay * n, kMaxSegsPerRay,
+                    g->opt_block};
     launch_raycast_split(p, g->opt_cube, g->opt_seg, sc, g->stream);
   } else if (g->opt_raycast == 1) {
     BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};

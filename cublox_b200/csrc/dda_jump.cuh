@@ -13,7 +13,7 @@
 // sum's parity is fixed), and the whole stretch is an arithmetic progression
 // whose terms are exact in FP32.  Only the step that leaves the binade (or
 // one starting at or below zero) needs a real rounded add.  A query costs
-// O(number of binades crossed) adds and a few exact FP64 divisions.
+// O(number of binades crossed) adds and two integer divisions per binade.
 //
 // Everything here is __host__ __device__ and plain IEEE arithmetic, so the
 // CPU test (tests/cpp/test_dda_jump.cpp) checks the same code the kernels run.
@@ -57,17 +57,27 @@ CBX_HD float f32_pow2(int k) {
 #endif
 }
 
-// Exact steps from v stay on the grid of v's binade: with |v| in
-// [2^e, 2^(e+1)) and ulp u, in units of u (V = v/u, Dd = d/u exactly):
-//   v > 0: V + Dd < 2^24      (the sum stays below 2^(e+1))
-//   v < 0: V + Dd <= -2^23    (the sum keeps magnitude >= 2^e)
-CBX_HD bool on_grid_step(double V, double Dd, bool neg) {
-  return neg ? (V + Dd <= -8388608.0) : (V + Dd < 16777216.0);
+// Integer helpers: floor/ceil of an exact float that holds an integer or a
+// value with few fractional bits, and floor division with a positive divisor.
+CBX_HD int64_t floor_div_pos(int64_t a, int64_t b) {
+  const int64_t q = a / b;
+  return (a % b != 0 && a < 0) ? q - 1 : q;
+}
+
+CBX_HD float f32_scale(float v, int k) {  // v * 2^k, exact while normal
+  return fmul(v, f32_pow2(k));
 }
 
 // Smallest j >= 0 with s_j >= tau (the sequence starts at s_0 = s0), and s_j.
 // Also stops at j == jmax (returning s_jmax) so callers can bound work.
 // d must be > 0 and finite; s0 may be any non-NaN value.
+//
+// Inside a binade of ulp u every quantity is an exact integer multiple of u
+// except d; with F = floor(d/u), a step from v = V*u stays on the grid iff
+//   v > 0:  V + F <= 2^24 - 1         (the sum stays below 2^(e+1))
+//   v < 0:  V + F <= -2^23 - [d/u not an integer]   (magnitude >= 2^e)
+// so the number of on-grid steps and the first term >= tau are integer
+// divisions.
 CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax) {
   JumpResult r{0, s0, true};
   for (int guard = 0; guard < 4096; ++guard) {
@@ -84,40 +94,39 @@ CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax) 
     if (!f32_is_normal_pos(mag)) continue;  // zero, subnormal or infinite
     const bool neg = r.s < 0.0f;
     const int e = f32_exponent(mag);
-    if (e > 126 || e < -100) continue;
-    const double u = static_cast<double>(f32_pow2(e - 23));
-    const double Dd = static_cast<double>(d) / u;
+    if (e > 100 || e < -100) continue;
+    const float Ddf = f32_scale(d, 23 - e);  // d/u, exact
+    if (!(Ddf < 16777216.0f)) continue;     // d spans the binade: real steps
+    const float Ff = ffloor(Ddf);
+    const int64_t F = static_cast<int64_t>(Ff);
+    const int64_t frac = (Ddf != Ff) ? 1 : 0;
+    const int64_t lim = neg ? (-8388608 - frac - F) : (16777215 - F);
     // A second on-grid step: if d sits exactly halfway between two ulp
     // multiples, it rounds the sum to an even multiple, after which every
     // on-grid step rounds the same way.
-    if (!on_grid_step(static_cast<double>(r.s) / u, Dd, neg)) continue;
+    int64_t S = static_cast<int64_t>(f32_scale(r.s, 23 - e));
+    if (S > lim) continue;
     const float s2 = fadd(r.s, d);
     r.j += 1;
     r.s = s2;
     if (r.s >= tau || r.j >= jmax) return r;
-    if (!on_grid_step(static_cast<double>(r.s) / u, Dd, neg)) continue;
+    S = static_cast<int64_t>(f32_scale(r.s, 23 - e));
+    if (S > lim) continue;
     const float s3 = fadd(r.s, d);
     const float delta = fsub(s3, r.s);  // exact: both on the ulp grid
     if (!(delta > 0.0f)) continue;
-    const double S = static_cast<double>(r.s) / u;
-    const double D = static_cast<double>(delta) / u;
-    // m = number of on-grid steps from here = #{k >= 0 : S + k D on grid}
-    const double lim = neg ? (-8388608.0 - Dd) : (16777216.0 - Dd);
-    double mk = (lim - S) / D;
-    int64_t m = mk > 0.0 ? static_cast<int64_t>(mk) : 0;
-    while (m > 0 && !on_grid_step(S + static_cast<double>(m - 1) * D, Dd, neg)) --m;
-    while (on_grid_step(S + static_cast<double>(m) * D, Dd, neg)) ++m;
+    const int64_t D = static_cast<int64_t>(f32_scale(delta, 23 - e));
+    // m = number of on-grid steps from here = #{k >= 0 : S + k D <= lim}
+    const int64_t m = floor_div_pos(lim - S, D) + 1;
     if (m <= 0) continue;
-    // Within the stretch s_{j+k} = r.s + k*delta.  First k with value >= tau.
-    int64_t kt;
-    if (tau > 3.4028234e38f) {
-      kt = m + 1;
-    } else {
-      const double T = static_cast<double>(tau) / u;
-      const double kk = (T - S) / D;
-      kt = kk > 0.0 ? (kk < static_cast<double>(m + 1) ? static_cast<int64_t>(kk) : m + 1) : 0;
-      while (kt > 0 && S + static_cast<double>(kt - 1) * D >= T) --kt;
-      while (kt <= m && S + static_cast<double>(kt) * D < T) ++kt;
+    // First k with S + k D >= ceil(tau/u).
+    int64_t kt = m + 1;
+    if (tau < 3.4028234e38f) {
+      const float Tf = f32_scale(tau, 23 - e);
+      if (Tf < 1.0e15f && Tf > -1.0e15f) {
+        const int64_t T = static_cast<int64_t>(ceilf(Tf));
+        kt = T <= S ? 0 : -floor_div_pos(-(T - S), D);  // ceil((T - S) / D)
+      }
     }
     int64_t k = kt < m ? kt : m;
     if (jmax - r.j < k) k = jmax - r.j;

@@ -106,6 +106,7 @@ struct SplitScratch {
   int *counters;  // 2 ints: segments planned, work queue
   int seg_cap;
   int max_segs;   // per ray
+  int block;      // walk CTA size (256, 512 or 1024)
 };
 size_t split_seg_bytes();
 size_t split_ray_bytes();

@@ -100,8 +100,23 @@ __device__ __forceinline__ bool ev_less(float t1, int r1, float t2, int r2) {
   return t1 < t2 || (t1 == t2 && r1 < r2);
 }
 
+// T_a(j) continuing from a known (j0, s0) of the same sequence when j >= j0,
+// else from the start (t0).
+__device__ __forceinline__ JumpResult value_from(float t0, float d, int64_t j0, float s0,
+                                                 int64_t j) {
+  if (j >= j0) {
+    JumpResult r = value_at(s0, d, j - j0);
+    r.j += j0;
+    return r;
+  }
+  return value_at(t0, d, j);
+}
+
 // Does the walk's state number L1 (= |dx|+|dy|+|dz|) equal the end voxel?
-__device__ bool reaches_end(const RayWalk &w0) {
+// It does iff every event needed to reach the end voxel (the first |D_a|
+// of each axis) precedes, in (T, rank) order, every further event.  (j0,
+// s0) are known positions of each axis's sequence to continue from.
+__device__ bool reaches_end(const RayWalk &w0, const int64_t j0[3], const float s0[3]) {
   float need_t = -inf_f(), extra_t = inf_f();
   int need_r = -1, extra_r = 3;
 #pragma unroll
@@ -111,18 +126,20 @@ __device__ bool reaches_end(const RayWalk &w0) {
     if (D != 0 && (w0.st[a] == 0 || (D > 0) != (w0.st[a] > 0))) return false;
     const int n = abs(D);
     if (w0.st[a] == 0) continue;  // never steps: extra events at +inf
+    float tn;
     if (n > 0) {
-      const JumpResult v = value_at(w0.tM[a], w0.tD[a], n - 1);
+      const JumpResult v = value_from(w0.tM[a], w0.tD[a], j0[a], s0[a], n - 1);
       if (!v.ok) return false;
       if (ev_less(need_t, need_r, v.s, rank)) {
         need_t = v.s;
         need_r = rank;
       }
+      tn = fadd(v.s, w0.tD[a]);
+    } else {
+      tn = w0.tM[a];
     }
-    const JumpResult x = value_at(w0.tM[a], w0.tD[a], n);
-    if (!x.ok) return false;
-    if (ev_less(x.s, rank, extra_t, extra_r)) {
-      extra_t = x.s;
+    if (ev_less(tn, rank, extra_t, extra_r)) {
+      extra_t = tn;
       extra_r = rank;
     }
   }
@@ -242,8 +259,6 @@ __global__ void __launch_bounds__(256) seg_plan_kernel(const RayParams p, int se
   }
   rr.max_steps = w.max_steps;
   rr.L1 = abs(w.en[0] - w.id[0]) + abs(w.en[1] - w.id[1]) + abs(w.en[2] - w.id[2]);
-  rr.flags = (w.clipped ? 1 : 0) | ((K > 1 && reaches_end(w)) ? 2 : 0);
-  rays[i] = rr;
   // segment start states, cut by cut
   int64_t jc[3] = {0, 0, 0};
   float sc[3] = {w.tM[0], w.tM[1], w.tM[2]};
@@ -275,10 +290,12 @@ __global__ void __launch_bounds__(256) seg_plan_kernel(const RayParams p, int se
     sr.pad[0] = sr.pad[1] = 0;
     segs[base + k] = sr;
   }
+  rr.flags = (w.clipped ? 1 : 0) | ((K > 1 && reaches_end(w, jc, sc)) ? 2 : 0);
+  rays[i] = rr;
 }
 
 template <int S>
-__global__ void __launch_bounds__(512) seg_walk_kernel(const RayParams p, const int cl0,
+__global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const int cl0,
                                                        const int cl1, const int cl2,
                                                        const SegRec *segs, const RayRec *rays,
                                                        const int *seg_count, int *work) {
@@ -427,13 +444,15 @@ void launch_seg_walk(const RayParams &p, const int clo[3], const SplitScratch &s
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(seg_walk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, seg_walk_kernel<S>, 512, smem);
-    if (per_sm < 1) per_sm = 1;
+  const int block = sc.block == 256 || sc.block == 1024 ? sc.block : 512;
+  static int per_sm[3] = {0, 0, 0};
+  int &ps = per_sm[block == 256 ? 0 : (block == 512 ? 1 : 2)];
+  if (ps == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, seg_walk_kernel<S>, block, smem);
+    if (ps < 1) ps = 1;
   }
-  const int grid = sm_count_split() * per_sm;
-  seg_walk_kernel<S><<<grid, 512, smem, s>>>(
+  const int grid = sm_count_split() * ps;
+  seg_walk_kernel<S><<<grid, block, smem, s>>>(
       p, clo[0], clo[1], clo[2], reinterpret_cast<const SegRec *>(sc.segs),
       reinterpret_cast<const RayRec *>(sc.rays), sc.counters, sc.counters + 1);
 }

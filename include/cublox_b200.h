@@ -93,6 +93,7 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 #define CUBLOX_OPT_SORT 4    /* walk rays in direction order (default 1)    */
 #define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (48)   */
 #define CUBLOX_OPT_FOLD 6    /* fold sweep: 0 scalar, 1 16-byte (default)   */
+#define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
 int cublox_grid_set_option(cublox_grid *g, int key, int value);
 int cublox_grid_get_option(const cublox_grid *g, int key, int *value);
 
