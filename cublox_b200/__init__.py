@@ -22,7 +22,8 @@ LIB_PATH = os.path.join(HERE, "libcublox_b200.so")
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_RANGE, ERR_DEVICE = -1, -2, -3, -4, -5
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
-OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT, OPT_SEGMENT, OPT_FOLD, OPT_BLOCK = 1, 2, 3, 4, 5, 6, 7
+OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT, OPT_SEGMENT, OPT_FOLD, OPT_BLOCK, OPT_CONTIGUOUS = (
+    1, 2, 3, 4, 5, 6, 7, 8)
 
 
 class VoxelState(enum.IntEnum):

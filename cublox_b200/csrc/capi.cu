@@ -108,6 +108,7 @@ struct cublox_grid {
   int opt_seg = 48;     // split walk: target in-window steps per lane
   int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
   int opt_block = 512;  // split walk CTA size
+  int opt_contig = 1;   // split walk: contiguous segment runs per CTA
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
   int opt_match = 0;    // merge duplicate voxels within a warp
   int opt_sort = 1;     // walk rays in direction-bin order
@@ -356,8 +357,11 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
       if (value != 256 && value != 512 && value != 1024) break;
       g->opt_block = value;
       return CUBLOX_OK;
+    case CUBLOX_OPT_CONTIGUOUS:
+      g->opt_contig = value != 0;
+      return CUBLOX_OK;
     case CUBLOX_OPT_CUBE:
-      if (value != 0 && value != 16 && value != 32) break;
+      if (value != 0 && value != 8 && value != 16 && value != 32) break;
       g->opt_cube = value;
       return CUBLOX_OK;
     case CUBLOX_OPT_MATCH:
@@ -382,6 +386,7 @@ int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
     case CUBLOX_OPT_SEGMENT: *value = g->opt_seg; return CUBLOX_OK;
     case CUBLOX_OPT_FOLD: *value = g->opt_fold; return CUBLOX_OK;
     case CUBLOX_OPT_BLOCK: *value = g->opt_block; return CUBLOX_OK;
+    case CUBLOX_OPT_CONTIGUOUS: *value = g->opt_contig; return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "get_option: unknown key");
@@ -462,7 +467,7 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   p.hit = g->d_hit;
   p.stats = g->stats_on ? g->d_stats : nullptr;
   p.err = g->d_err;
-  if (g->opt_raycast == 1 && n > g->bin_cap) {
+  if ((g->opt_raycast == 1 || (g->opt_raycast == 2 && g->opt_sort)) && n > g->bin_cap) {
     CK(cudaStreamSynchronize(g->stream));
     cudaFree(g->d_bins);
     cudaFree(g->d_sorted);
@@ -513,8 +518,17 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   }
   if (g->opt_raycast == 2) {
     SplitScratch sc{g->d_segs, g->d_rays, g->d_work, kMaxSegsPerRay * n, kMaxSegsPerRay,
-                    g->opt_block};
-    launch_raycast_split(p, g->opt_cube, g->opt_seg, sc, g->stream);
+                    g->opt_block, g->opt_contig};
+    RayParams ps = p;
+    if (g->opt_sort) {
+      BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};
+      launch_direction_sort(p, b, g->stream);
+      ps.x = g->d_sorted;
+      ps.y = g->d_sorted + n;
+      ps.z = g->d_sorted + 2 * static_cast<size_t>(n);
+      ps.stride = 1;
+    }
+    launch_raycast_split(ps, g->opt_cube, g->opt_seg, sc, g->stream);
   } else if (g->opt_raycast == 1) {
     BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};
     launch_raycast_binned(p, b, g->opt_cube, g->opt_match != 0, g->opt_sort != 0, g->stream);

@@ -59,9 +59,13 @@ CBX_HD float f32_pow2(int k) {
 
 // Integer helpers: floor/ceil of an exact float that holds an integer or a
 // value with few fractional bits, and floor division with a positive divisor.
-CBX_HD int64_t floor_div_pos(int64_t a, int64_t b) {
-  const int64_t q = a / b;
-  return (a % b != 0 && a < 0) ? q - 1 : q;
+// floor(a / b) for b > 0 and |a| < 2^27: a rounded float quotient, then an
+// exact integer correction (the estimate is off by a few units at most).
+CBX_HD int32_t floor_div_pos(int32_t a, int32_t b) {
+  int32_t q = static_cast<int32_t>(ffloor(fdiv(static_cast<float>(a), static_cast<float>(b))));
+  while (static_cast<int64_t>(q) * b > a) --q;
+  while (static_cast<int64_t>(q + 1) * b <= a) ++q;
+  return q;
 }
 
 CBX_HD float f32_scale(float v, int k) {  // v * 2^k, exact while normal
@@ -98,34 +102,37 @@ CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax) 
     const float Ddf = f32_scale(d, 23 - e);  // d/u, exact
     if (!(Ddf < 16777216.0f)) continue;     // d spans the binade: real steps
     const float Ff = ffloor(Ddf);
-    const int64_t F = static_cast<int64_t>(Ff);
-    const int64_t frac = (Ddf != Ff) ? 1 : 0;
-    const int64_t lim = neg ? (-8388608 - frac - F) : (16777215 - F);
+    const int32_t F = static_cast<int32_t>(Ff);
+    const int32_t frac = (Ddf != Ff) ? 1 : 0;
+    const int32_t lim = neg ? (-8388608 - frac - F) : (16777215 - F);
     // A second on-grid step: if d sits exactly halfway between two ulp
     // multiples, it rounds the sum to an even multiple, after which every
     // on-grid step rounds the same way.
-    int64_t S = static_cast<int64_t>(f32_scale(r.s, 23 - e));
+    int32_t S = static_cast<int32_t>(f32_scale(r.s, 23 - e));
     if (S > lim) continue;
     const float s2 = fadd(r.s, d);
     r.j += 1;
     r.s = s2;
     if (r.s >= tau || r.j >= jmax) return r;
-    S = static_cast<int64_t>(f32_scale(r.s, 23 - e));
+    S = static_cast<int32_t>(f32_scale(r.s, 23 - e));
     if (S > lim) continue;
     const float s3 = fadd(r.s, d);
     const float delta = fsub(s3, r.s);  // exact: both on the ulp grid
     if (!(delta > 0.0f)) continue;
-    const int64_t D = static_cast<int64_t>(f32_scale(delta, 23 - e));
+    const int32_t D = static_cast<int32_t>(f32_scale(delta, 23 - e));
     // m = number of on-grid steps from here = #{k >= 0 : S + k D <= lim}
-    const int64_t m = floor_div_pos(lim - S, D) + 1;
+    const int32_t m = floor_div_pos(lim - S, D) + 1;
     if (m <= 0) continue;
-    // First k with S + k D >= ceil(tau/u).
-    int64_t kt = m + 1;
+    // First k with S + k D >= ceil(tau/u); anything past the stretch is m+1.
+    int32_t kt = m + 1;
     if (tau < 3.4028234e38f) {
       const float Tf = f32_scale(tau, 23 - e);
-      if (Tf < 1.0e15f && Tf > -1.0e15f) {
-        const int64_t T = static_cast<int64_t>(ceilf(Tf));
-        kt = T <= S ? 0 : -floor_div_pos(-(T - S), D);  // ceil((T - S) / D)
+      const float hi = static_cast<float>(S) + static_cast<float>(m) * static_cast<float>(D);
+      if (Tf <= static_cast<float>(S)) {
+        kt = 0;
+      } else if (Tf <= hi) {
+        const int32_t T = static_cast<int32_t>(ceilf(Tf));
+        kt = -floor_div_pos(-(T - S), D);  // ceil((T - S) / D)
       }
     }
     int64_t k = kt < m ? kt : m;

@@ -98,6 +98,8 @@ struct BinnedScratch {
   float *sorted;  // 3 * n (SoA)
 };
 int binned_bins();
+// Counting sort of the rays by octahedral direction bin into b.sorted (SoA).
+void launch_direction_sort(const RayParams &p, const BinnedScratch &b, cudaStream_t s);
 // Warp-cooperative exact walk (raycast_split.cu): rays longer than seg_len
 // in-window steps are cut into time segments walked by separate lanes.
 struct SplitScratch {
@@ -107,6 +109,7 @@ struct SplitScratch {
   int seg_cap;
   int max_segs;   // per ray
   int block;      // walk CTA size (256, 512 or 1024)
+  int contiguous; // 1: each CTA walks one contiguous run of segments
 };
 size_t split_seg_bytes();
 size_t split_ray_bytes();

@@ -327,4 +327,13 @@ void launch_raycast_binned(const RayParams &p_in, const BinnedScratch &b, int cu
 
 int binned_bins() { return kBins; }
 
+void launch_direction_sort(const RayParams &p, const BinnedScratch &b, cudaStream_t s) {
+  if (p.n <= 0) return;
+  cudaMemsetAsync(b.hist, 0, sizeof(int) * kBins, s);
+  const int grid = min((p.n + 255) / 256, sms() * 4);
+  bin_kernel<<<grid, 256, 0, s>>>(p, b.bins, b.hist);
+  bin_scan_kernel<<<1, 1024, 0, s>>>(b.hist, b.cursor);
+  scatter_kernel<<<grid, 256, 0, s>>>(p, b.bins, b.cursor, b.sorted);
+}
+
 }  // namespace cublox_b200

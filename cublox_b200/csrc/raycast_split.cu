@@ -298,23 +298,30 @@ template <int S>
 __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const int cl0,
                                                        const int cl1, const int cl2,
                                                        const SegRec *segs, const RayRec *rays,
-                                                       const int *seg_count, int *work) {
+                                                       const int *seg_count, int *work,
+                                                       const int contiguous) {
   extern __shared__ uint32_t cube[];
   constexpr int kCube = S * S * S;
+  __shared__ int cta_next;
   for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
     reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
+  if (threadIdx.x == 0) cta_next = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int total = *seg_count;
+  // contiguous: CTA c owns segments [lo, hi); warps share them via cta_next.
+  const int per = (total + gridDim.x - 1) / gridDim.x;
+  const int lo = contiguous ? min(total, blockIdx.x * per) : 0;
+  const int hi = contiguous ? min(total, lo + per) : total;
   Emitter<S> em{p, cube, cl0, cl1, cl2, 0u};
   uint32_t nrays = 0, hits = 0;
   for (;;) {
     int b = 0;
-    if (lane == 0) b = atomicAdd(work, 32);
+    if (lane == 0) b = contiguous ? lo + atomicAdd(&cta_next, 32) : atomicAdd(work, 32);
     b = __shfl_sync(0xffffffffu, b, 0);
-    if (b >= total) break;
+    if (b >= hi) break;
     const int g = b + lane;
-    if (g >= total) continue;
+    if (g >= hi) continue;
     const SegRec sr = segs[g];
     const RayRec rr = rays[sr.ray];
     RayWalk w;
@@ -454,7 +461,7 @@ void launch_seg_walk(const RayParams &p, const int clo[3], const SplitScratch &s
   const int grid = sm_count_split() * ps;
   seg_walk_kernel<S><<<grid, block, smem, s>>>(
       p, clo[0], clo[1], clo[2], reinterpret_cast<const SegRec *>(sc.segs),
-      reinterpret_cast<const RayRec *>(sc.rays), sc.counters, sc.counters + 1);
+      reinterpret_cast<const RayRec *>(sc.rays), sc.counters, sc.counters + 1, sc.contiguous);
 }
 
 }  // namespace
@@ -477,6 +484,8 @@ void launch_raycast_split(const RayParams &p, int cube, int seg_len, const Split
     launch_seg_walk<32>(p, clo, sc, s);
   else if (cube >= 16)
     launch_seg_walk<16>(p, clo, sc, s);
+  else if (cube >= 8)
+    launch_seg_walk<8>(p, clo, sc, s);
   else
     launch_seg_walk<0>(p, clo, sc, s);
 }

@@ -88,12 +88,15 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
                                 warp walk; 2: rays split between lanes at
                                 exact time cuts (default)                  */
 #define CUBLOX_OPT_CUBE 2    /* shared-memory counter cube side around the
-                                sensor: 0, 16 or 32 (default 32)            */
+                                sensor: 0, 8, 16 or 32 (default 32; 8 is
+                                split walk only)                           */
 #define CUBLOX_OPT_MATCH 3   /* merge duplicate voxels per warp (default 0) */
 #define CUBLOX_OPT_SORT 4    /* walk rays in direction order (default 1)    */
 #define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (48)   */
 #define CUBLOX_OPT_FOLD 6    /* fold sweep: 0 scalar, 1 16-byte (default)   */
 #define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
+#define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
+                                   consecutive segments (default 1)         */
 int cublox_grid_set_option(cublox_grid *g, int key, int value);
 int cublox_grid_get_option(const cublox_grid *g, int key, int *value);
 

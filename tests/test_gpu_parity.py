@@ -310,8 +310,8 @@ def test_readme_scale_scan_exact():
 
 VARIANTS = [dict(raycast=0), dict(raycast=1, cube=32, match=1, sort=1),
             dict(raycast=1, cube=16, match=0, sort=1), dict(raycast=1, cube=0, match=1, sort=0),
-            dict(raycast=2, cube=32, seg=48), dict(raycast=2, cube=0, seg=4),
-            dict(raycast=2, cube=16, seg=7)]
+            dict(raycast=2, cube=32, seg=48), dict(raycast=2, cube=0, seg=4, sort=0),
+            dict(raycast=2, cube=16, seg=7, contig=0), dict(raycast=2, cube=8, seg=16, sort=1)]
 
 
 def set_variant(g, v):
@@ -323,6 +323,8 @@ def set_variant(g, v):
         g.set_option(C.OPT_SORT, v["sort"])
     if v["raycast"] == 2:
         g.set_option(C.OPT_SEGMENT, v["seg"])
+        g.set_option(C.OPT_SORT, v.get("sort", 1))
+        g.set_option(C.OPT_CONTIGUOUS, v.get("contig", 1))
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=lambda v: "-".join(f"{k}{x}" for k, x in v.items()))
