@@ -8,7 +8,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcublox_b200.so")
-SOURCES = ["csrc/kernels.cu", "csrc/raycast_binned.cu", "csrc/raycast_split.cu", "csrc/capi.cu"]
+SOURCES = ["csrc/kernels.cu", "csrc/raycast_binned.cu", "csrc/raycast_split.cu", "csrc/capi.cu",
+           "csrc/noalloc.cu"]
 HEADERS = ["csrc/kernels.cuh", "csrc/exact_fp.cuh", "csrc/ray_walk.cuh", "csrc/dda_jump.cuh", "../include/cublox_b200.h"]
 
 NVCC_FLAGS = [

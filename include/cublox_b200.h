@@ -199,6 +199,46 @@ int cublox_grid_reference_steps(cublox_grid *g, const float *xyz, int n,
  * index (a bug, never expected).  Reading it clears it.                    */
 int cublox_grid_check(cublox_grid *g, uint32_t *error_word);
 
+/* ---- allocation-free integration ------------------------------------------
+ * No counterpart in the reference: it exists for callers that must not
+ * allocate device memory while running (a real-time mapping loop that
+ * reserves all GPU memory at start-up, code inside a host framework that is
+ * handed only a stream and buffers it owns).  The caller owns every buffer:
+ * the map view's occ / cnt / hit arrays (voxel_num elements each, in the
+ * ring-buffer hash order; cnt and hit must be zero before the first call
+ * and are left zero by every call) and the points, a device array of n x,
+ * then n y, then n z.  The call integrates one scan exactly as
+ * cublox_grid_update does for the same window origin (there is no
+ * first-run origin snap: origin_index is used as given), enqueues on
+ * `stream` (a cudaStream_t, NULL for the default stream) and returns.
+ *
+ * Its only scratch is a fixed area of about 4 MiB in a file-scope device
+ * array that every GPU loading this library holds until exit; it allocates
+ * nothing and calls no allocating routine.  At most
+ * CUBLOX_NOALLOC_MAX_POINTS points per call; more are rejected with
+ * CUBLOX_ERR_INVALID.  The first call on each device looks the scratch
+ * array's address up (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the scratch: calls whose GPU work
+ * overlaps in time race and give wrong maps.  Errors: the message is in
+ * cublox_noalloc_last_error().                                             */
+#define CUBLOX_NOALLOC_MAX_POINTS 262144
+
+typedef struct {
+  float *occ;                /* stored log-odds, device                    */
+  uint32_t *cnt;             /* per-scan traversal counters, device        */
+  uint32_t *hit;             /* per-scan hit counters, device              */
+  int half_map_size[3];
+  int origin_index[3];       /* sliding-window origin, global voxel index  */
+  float resolution;
+  int origin_at_center;
+  float max_range;
+  float l_hit, l_miss, l_min, l_max;  /* log-odds parameters               */
+} cublox_map_view;
+
+int cublox_integrate_noalloc(const cublox_map_view *map, const float *xyz_soa, int n,
+                             const float sensor_origin[3], void *stream);
+const char *cublox_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
