@@ -100,6 +100,19 @@ def lib():
             "cublox_grid_last_stats": ([G, ctypes.POINTER(ScanStats)], ctypes.c_int),
             "cublox_grid_check": ([G, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
             "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
+            "cublox_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+            "cublox_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
+            "cublox_batch_add_grid": ([ctypes.c_void_p, i, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, f, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+            "cublox_batch_set_option": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+            "cublox_batch_get_option": ([ctypes.c_void_p, ctypes.c_int, i], ctypes.c_int),
+            "cublox_batch_update": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), f, i64, f],
+                                    ctypes.c_int),
+            "cublox_batch_recenter": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), f, i],
+                                      ctypes.c_int),
+            "cublox_batch_synchronize": ([ctypes.c_void_p], ctypes.c_int),
+            "cublox_batch_last_timing": ([ctypes.c_void_p, f, f], ctypes.c_int),
+            "cublox_batch_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
             "cublox_grid_enable_timing": ([G, ctypes.c_int], ctypes.c_int),
             "cublox_grid_set_option": ([G, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "cublox_grid_get_option": ([G, ctypes.c_int, i], ctypes.c_int),
@@ -144,15 +157,21 @@ class OccupancyGrid:
     VoxelState = VoxelState
 
     def __init__(self, half_map_size_i, resolution: float, origin_at_center: bool = False,
-                 recenter_threshold: float | None = None, origin=(0.0, 0.0, 0.0), stream=None):
+                 recenter_threshold: float | None = None, origin=(0.0, 0.0, 0.0), stream=None,
+                 _handle=None):
         L = lib()
-        h = ctypes.c_void_p()
-        rc = L.cublox_grid_create((ctypes.c_int * 3)(*[int(v) for v in half_map_size_i]),
-                                  float(resolution), int(bool(origin_at_center)),
-                                  int(recenter_threshold is not None),
-                                  float(recenter_threshold or 0.0), _f3(origin),
-                                  ctypes.c_void_p(stream or 0), ctypes.byref(h))
-        _check(rc, "OccupancyGrid")
+        if _handle is None:
+            h = ctypes.c_void_p()
+            rc = L.cublox_grid_create((ctypes.c_int * 3)(*[int(v) for v in half_map_size_i]),
+                                      float(resolution), int(bool(origin_at_center)),
+                                      int(recenter_threshold is not None),
+                                      float(recenter_threshold or 0.0), _f3(origin),
+                                      ctypes.c_void_p(stream or 0), ctypes.byref(h))
+            _check(rc, "OccupancyGrid")
+            self._owned = True
+        else:
+            h = _handle
+            self._owned = False
         self._h = h
         m = (ctypes.c_int * 3)()
         hf = (ctypes.c_int * 3)()
@@ -174,7 +193,8 @@ class OccupancyGrid:
     # ---- lifetime ----
     def close(self):
         if getattr(self, "_h", None):
-            lib().cublox_grid_destroy(self._h)
+            if getattr(self, "_owned", True):
+                lib().cublox_grid_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -442,6 +462,106 @@ class OccupancyGrid:
     reset_voxel = resetVoxel
 
 
+BATCH_OPT_GRAPHS, BATCH_OPT_AUTOTUNE, BATCH_OPT_SHAPE, BATCH_OPT_TIMING, BATCH_OPT_NUM_SHAPES = 1, 2, 3, 4, 5
+
+
+class Batch:
+    """Many grids integrated together (cublox_batch_*): one walk launch and
+    one fold launch per update, optional CUDA-graph replay, online choice of
+    the launch shape.  Grids made by add_grid belong to the batch."""
+
+    def __init__(self, stream=None):
+        self._b = ctypes.c_void_p()
+        _check(lib().cublox_batch_create(ctypes.c_void_p(stream or 0), ctypes.byref(self._b)),
+               "Batch")
+        self.grids = []
+
+    def close(self):
+        if getattr(self, "_b", None):
+            for g in self.grids:
+                g._h = None
+            lib().cublox_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_grid(self, half_map_size_i, resolution, origin_at_center=False,
+                 recenter_threshold=None, origin=(0.0, 0.0, 0.0)) -> OccupancyGrid:
+        h = ctypes.c_void_p()
+        _check(lib().cublox_batch_add_grid(self._b, (ctypes.c_int * 3)(*[int(v) for v in half_map_size_i]),
+                                           float(resolution), int(bool(origin_at_center)),
+                                           int(recenter_threshold is not None),
+                                           float(recenter_threshold or 0.0), _f3(origin),
+                                           ctypes.byref(h)), "add_grid")
+        g = OccupancyGrid(half_map_size_i, resolution, origin_at_center, recenter_threshold, origin,
+                          _handle=h)
+        self.grids.append(g)
+        return g
+
+    def set_option(self, key, value):
+        _check(lib().cublox_batch_set_option(self._b, int(key), int(value)), "batch set_option")
+
+    def get_option(self, key) -> int:
+        v = ctypes.c_int()
+        _check(lib().cublox_batch_get_option(self._b, int(key), ctypes.byref(v)), "batch get_option")
+        return v.value
+
+    def update(self, grids, clouds, sensors, offsets=None):
+        """One scan into each grid.  `clouds`: a list of (N_i, 3) float32 host
+        arrays, or one concatenated (sum N_i, 3) host array / CUDA tensor with
+        `offsets` (n+1 int64)."""
+        n = len(grids)
+        handles = (ctypes.c_void_p * n)(*[g._h.value if isinstance(g._h, ctypes.c_void_p) else g._h
+                                           for g in grids])
+        if offsets is None:
+            arrs = [np.ascontiguousarray(np.asarray(c, dtype=np.float32).reshape(-1, 3)) for c in clouds]
+            offsets = np.zeros(n + 1, dtype=np.int64)
+            offsets[1:] = np.cumsum([a.shape[0] for a in arrs])
+            xyz = np.ascontiguousarray(np.concatenate(arrs, axis=0)) if arrs else np.zeros((0, 3), np.float32)
+            ptr = _fp(xyz)
+        else:
+            offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+            dp = _dev_ptr(clouds)
+            if dp is not None:
+                ptr = ctypes.cast(dp, ctypes.POINTER(ctypes.c_float))
+            else:
+                xyz = np.ascontiguousarray(np.asarray(clouds, dtype=np.float32))
+                ptr = _fp(xyz)
+        so = np.ascontiguousarray(np.asarray(sensors, dtype=np.float32).reshape(-1, 3))
+        _check(lib().cublox_batch_update(self._b, n, handles, ptr,
+                                         offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _fp(so)),
+               "batch update")
+
+    def recenter(self, grids, positions):
+        n = len(grids)
+        handles = (ctypes.c_void_p * n)(*[g._h.value if isinstance(g._h, ctypes.c_void_p) else g._h
+                                           for g in grids])
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1, 3))
+        acts = np.zeros(max(n, 1), dtype=np.int32)
+        _check(lib().cublox_batch_recenter(self._b, n, handles, _fp(pos),
+                                           acts.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+               "batch recenter")
+        return acts[:n]
+
+    def synchronize(self):
+        _check(lib().cublox_batch_synchronize(self._b), "batch synchronize")
+
+    def last_timing(self):
+        a = ctypes.c_float()
+        b = ctypes.c_float()
+        _check(lib().cublox_batch_last_timing(self._b, ctypes.byref(a), ctypes.byref(b)), "batch timing")
+        return a.value, b.value
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().cublox_batch_stream(self._b, ctypes.byref(s)), "batch stream")
+        return s.value or 0
+
+
 _libm = None
 
 
@@ -465,4 +585,4 @@ def yaml_log_odds():
     return tuple(logit(p) for p in (0.9, 0.49, 0.12, 0.98, 0.499, 0.85))
 
 
-__all__ = ["OccupancyGrid", "VoxelState", "CubloxError", "lib", "logit", "LIB_PATH"]
+__all__ = ["OccupancyGrid", "Batch", "VoxelState", "CubloxError", "lib", "logit", "LIB_PATH"]

@@ -16,14 +16,17 @@
 
 #include "../../include/cublox_b200.h"
 #include "exact_fp.cuh"
+#include "grid_internal.hpp"
 #include "kernels.cuh"
 
 using namespace cublox_b200;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
 
+namespace cublox_b200 {
+namespace detail {
 int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
@@ -31,9 +34,16 @@ int fail(int code, const std::string &msg) {
 
 int cuda_fail(cudaError_t e, const char *what, int line) {
   g_err = std::string("cublox_b200: ") + what + ": " + cudaGetErrorString(e) +
-          " (capi.cu:" + std::to_string(line) + ")";
+          " (line " + std::to_string(line) + ")";
   return CUBLOX_ERR_CUDA;
 }
+}  // namespace detail
+}  // namespace cublox_b200
+
+using cublox_b200::detail::cuda_fail;
+using cublox_b200::detail::fail;
+
+namespace {
 
 #define CK(call)                                                     \
   do {                                                               \
@@ -84,75 +94,6 @@ int mem_kind(const void *p) {
 
 }  // namespace
 
-struct cublox_grid {
-  // Grid::Config (Grid.hpp:44-53)
-  int half[3] = {0, 0, 0};
-  int map[3] = {0, 0, 0};
-  int voxel_num = 0;
-  float res = 0.0f, res_inv = 0.0f;
-  bool ctr = false;
-  bool has_thr = false;
-  float thr_sq = 0.0f;
-  int origin_i[3] = {0, 0, 0};
-  float origin_f[3] = {0.0f, 0.0f, 0.0f};
-  bool first_run = true;
-  float max_range = 25.0f;
-  // OccupancyGrid.hpp:162-168 defaults
-  float l_hit = 0.847f, l_miss = -0.405f, l_min = -1.992f, l_max = 3.476f;
-  float l_free = -0.0004f, l_occ = 1.7346f, l_unknown = 0.0f;
-  unsigned fp = kFpPinned;
-  int recenter_mode = 0;
-  bool stats_on = false;
-  // kernel options (cublox_grid_set_option)
-  int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
-  int opt_seg = 48;     // split walk: target in-window steps per lane
-  int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
-  int opt_block = 512;  // split walk CTA size
-  int opt_contig = 1;   // split walk: contiguous segment runs per CTA
-  int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
-  int opt_match = 0;    // merge duplicate voxels within a warp
-  int opt_sort = 1;     // walk rays in direction-bin order
-  void *d_segs = nullptr;  // split walk: segment records
-  void *d_rays = nullptr;  // split walk: ray records
-  int *d_work = nullptr;   // split walk: 2 counters
-  int split_cap = 0;       // rays the split scratch holds
-  int *d_bins = nullptr;
-  int *d_hist = nullptr;
-  float *d_sorted = nullptr;
-  int bin_cap = 0;
-  bool timing_on = false;
-  cudaEvent_t tev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  bool tev_used[3] = {false, false, false};
-
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-
-  float *d_occ = nullptr;
-  uint32_t *d_cnt = nullptr;
-  uint32_t *d_hit = nullptr;
-  unsigned long long *d_stats = nullptr;  // 4
-  uint32_t *d_err = nullptr;
-  uint32_t *d_masks = nullptr;  // recenter slab masks
-  int mask_words[3] = {0, 0, 0};
-
-  float *d_cloud = nullptr;  // SoA [x|y|z]
-  int cloud_cap = 0;
-  float *h_stage[2] = {nullptr, nullptr};
-  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
-  int stage_cap = 0;
-  int stage_idx = 0;
-
-  // fetch scratch
-  void *d_fq = nullptr;  // centers | qbox | qr2 | counts | offsets | limits
-  size_t fq_bytes = 0;
-  float *d_fpos = nullptr;
-  uint8_t *d_fstate = nullptr;
-  int64_t fcap = 0;
-  uint8_t *d_qout = nullptr;
-  float *d_qin = nullptr;
-  int qcap = 0;
-};
 
 extern "C" {
 
@@ -558,13 +499,47 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   return CUBLOX_OK;
 }
 
-static void snap_first_run(cublox_grid *g, const float sensor[3]) {
+}  // extern "C"
+
+void cublox_b200::detail::snap_first_run(cublox_grid *g, const float sensor[3]) {
   if (!g->first_run) return;
   int o[3];
   for (int a = 0; a < 3; ++a) o[a] = host_p2g(sensor[a], g->res_inv, g->ctr);
   set_origin(g, o);
   g->first_run = false;
 }
+
+RayParams cublox_b200::detail::ray_params(const cublox_grid *g, const float *x,
+                                          const float *y, const float *z, int n, int stride,
+                                          const float sensor[3]) {
+  RayParams p{};
+  p.x = x;
+  p.y = y;
+  p.z = z;
+  p.n = n;
+  p.stride = stride;
+  for (int a = 0; a < 3; ++a) {
+    p.o[a] = sensor[a];
+    p.win[a] = g->origin_i[a];
+    p.half[a] = g->half[a];
+    p.map[a] = g->map[a];
+  }
+  p.res = g->res;
+  p.inv = g->res_inv;
+  p.max_range = g->max_range;
+  p.vnum = g->voxel_num;
+  p.ctr = g->ctr ? 1 : 0;
+  p.fp = g->fp;
+  p.cnt = g->d_cnt;
+  p.hit = g->d_hit;
+  p.stats = g->stats_on ? g->d_stats : nullptr;
+  p.err = g->d_err;
+  return p;
+}
+
+using cublox_b200::detail::snap_first_run;
+
+extern "C" {
 
 static int update_impl(cublox_grid *g, const float *x, const float *y,
                        const float *z, const float *xyz, int layout, int n,

@@ -1,0 +1,93 @@
+// Internal view of a cublox_grid, shared by capi.cu and batch.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "exact_fp.cuh"
+#include "kernels.cuh"
+
+struct cublox_grid {
+  // Grid::Config (Grid.hpp:44-53)
+  int half[3] = {0, 0, 0};
+  int map[3] = {0, 0, 0};
+  int voxel_num = 0;
+  float res = 0.0f, res_inv = 0.0f;
+  bool ctr = false;
+  bool has_thr = false;
+  float thr_sq = 0.0f;
+  int origin_i[3] = {0, 0, 0};
+  float origin_f[3] = {0.0f, 0.0f, 0.0f};
+  bool first_run = true;
+  float max_range = 25.0f;
+  // OccupancyGrid.hpp:162-168 defaults
+  float l_hit = 0.847f, l_miss = -0.405f, l_min = -1.992f, l_max = 3.476f;
+  float l_free = -0.0004f, l_occ = 1.7346f, l_unknown = 0.0f;
+  unsigned fp = cublox_b200::kFpPinned;
+  int recenter_mode = 0;
+  bool stats_on = false;
+  // kernel options (cublox_grid_set_option)
+  int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
+  int opt_seg = 48;     // split walk: target in-window steps per lane
+  int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
+  int opt_block = 512;  // split walk CTA size
+  int opt_contig = 1;   // split walk: contiguous segment runs per CTA
+  int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
+  int opt_match = 0;    // merge duplicate voxels within a warp
+  int opt_sort = 1;     // walk rays in direction-bin order
+  void *d_segs = nullptr;  // split walk: segment records
+  void *d_rays = nullptr;  // split walk: ray records
+  int *d_work = nullptr;   // split walk: 2 counters
+  int split_cap = 0;       // rays the split scratch holds
+  int *d_bins = nullptr;
+  int *d_hist = nullptr;
+  float *d_sorted = nullptr;
+  int bin_cap = 0;
+  bool timing_on = false;
+  cudaEvent_t tev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool tev_used[3] = {false, false, false};
+
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  float *d_occ = nullptr;
+  uint32_t *d_cnt = nullptr;
+  uint32_t *d_hit = nullptr;
+  unsigned long long *d_stats = nullptr;  // 4
+  uint32_t *d_err = nullptr;
+  uint32_t *d_masks = nullptr;  // recenter slab masks
+  int mask_words[3] = {0, 0, 0};
+
+  float *d_cloud = nullptr;  // SoA [x|y|z]
+  int cloud_cap = 0;
+  float *h_stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  int stage_cap = 0;
+  int stage_idx = 0;
+
+  // fetch scratch
+  void *d_fq = nullptr;  // centers | qbox | qr2 | counts | offsets | limits
+  size_t fq_bytes = 0;
+  float *d_fpos = nullptr;
+  uint8_t *d_fstate = nullptr;
+  int64_t fcap = 0;
+  uint8_t *d_qout = nullptr;
+  float *d_qin = nullptr;
+  int qcap = 0;
+};
+
+namespace cublox_b200 {
+namespace detail {
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what, int line);
+// First update: snap the window origin to the sensor voxel
+// (OccupancyGrid.cpp:192-198).
+void snap_first_run(cublox_grid *g, const float sensor[3]);
+// RayParams of one scan on this grid (points and counters filled in).
+RayParams ray_params(const cublox_grid *g, const float *x, const float *y, const float *z,
+                     int n, int stride, const float sensor[3]);
+}  // namespace detail
+}  // namespace cublox_b200

@@ -235,6 +235,72 @@ def stress(n_scans: int = 300) -> Workload:
                     poses, 0.5, seed=4, fetch_centres=10000, fetch_radius=2.0)
 
 
+BATCH_DIMS = ((128, 128, 32), (200, 200, 40), (256, 256, 64))  # 257x257x65, 401x401x81, 513x513x129
+
+
+@dataclass
+class BatchWorkload:
+    """Many independent maps, one scan per map per step, uneven point counts.
+
+    Map m has grid half-size `halves[m]`, its own box scene and a straight
+    line trajectory; at step k its scan has `counts[m, k]` points from a
+    `beams`-beam sensor (counts[m, k] / beams azimuths)."""
+    name: str
+    halves: list
+    resolution: float
+    beams: int
+    elev: tuple
+    max_range: float
+    sigma: float
+    scenes: list
+    poses: list
+    counts: np.ndarray
+    threshold: float | None
+    seed: int
+
+    @property
+    def n_maps(self) -> int:
+        return len(self.halves)
+
+    def sensor(self, m: int, k: int) -> Sensor:
+        return Sensor(self.beams, int(self.counts[m, k]) // self.beams, self.elev[0], self.elev[1],
+                      self.max_range, self.sigma)
+
+    def sensor_origin(self, m: int, k: int) -> np.ndarray:
+        return np.asarray(self.poses[m][k][:3], dtype=np.float32)
+
+    def scan(self, m: int, k: int) -> np.ndarray:
+        x, y, z, yaw = self.poses[m][k]
+        return scan(self.scenes[m], self.sensor(m, k), (x, y, z), yaw,
+                    seed=(self.seed * 1000 + m) * 100003 + k)
+
+    def step(self, k: int):
+        """All maps' scans of step k: (list of (N_m, 3) arrays, (n_maps, 3) sensors)."""
+        return ([self.scan(m, k) for m in range(self.n_maps)],
+                np.stack([self.sensor_origin(m, k) for m in range(self.n_maps)]))
+
+
+def batching(n_maps: int = 32, n_steps: int = 100, dims=BATCH_DIMS, n_min: int = 8192,
+             n_max: int = 131072, beams: int = 32, max_range: float = 30.0, speed: float = 2.0,
+             rate_hz: float = 10.0, threshold: float | None = 4.0, n_boxes: int = 200,
+             seed: int = 2) -> BatchWorkload:
+    """`n_maps` grids drawn from `dims` at 0.1 m, point counts uniform in
+    [n_min, n_max] (rounded down to whole azimuth columns), 32-beam sensor
+    over +-15 deg, 30 m range, straight lines at 2 m/s, 10 Hz."""
+    rng = np.random.default_rng(seed)
+    halves = [tuple(dims[i]) for i in rng.integers(0, len(dims), size=n_maps)]
+    counts = rng.integers(n_min, n_max + 1, size=(n_maps, n_steps))
+    counts = np.maximum(counts // beams, 1) * beams
+    scenes, poses = [], []
+    for m in range(n_maps):
+        y0 = float(rng.uniform(-5.0, 5.0))
+        scenes.append(make_scene(seed * 1000 + m, n_boxes, 45.0, keepout=_keepout_line(y0, 1.5)))
+        poses.append(line_trajectory(n_steps, speed, rate_hz, 1.8, start=(-10.0, y0)))
+    return BatchWorkload(f"batch{n_maps}_" + "|".join(f"{2*a+1}x{2*b+1}x{2*c+1}" for a, b, c in dims),
+                         halves, 0.1, beams, (-15.0, 15.0), max_range, 0.02, scenes, poses,
+                         counts, threshold, seed)
+
+
 def perf_test_cloud(n: int = 500000, r_min: float = 1.5, r_max: float = 8.0, seed: int = 42):
     """Spherical-shell cloud with the shape of the reference's perf test
     (test/test_occupancy_grid_perf.cpp:31-50): radius uniform in

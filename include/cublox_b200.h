@@ -199,6 +199,45 @@ int cublox_grid_reference_steps(cublox_grid *g, const float *xyz, int n,
  * index (a bug, never expected).  Reading it clears it.                    */
 int cublox_grid_check(cublox_grid *g, uint32_t *error_word);
 
+/* ---- batched integration ----------------------------------------------------
+ * No single counterpart in the reference, whose caller integrates one map's
+ * scan at a time (OccupancyGrid::update per map).  A batch owns grids created
+ * through it (they share its stream and stay usable through every
+ * cublox_grid_* call) and integrates one scan into each of many of them in
+ * one walk launch and one fold launch.  Results are identical to calling
+ * cublox_grid_update on each grid.                                          */
+typedef struct cublox_batch cublox_batch;
+
+#define CUBLOX_BATCH_OPT_GRAPHS 1     /* replay the launch sequence from a CUDA
+                                         graph (default 0)                  */
+#define CUBLOX_BATCH_OPT_AUTOTUNE 2   /* choose the launch shape over the
+                                         first updates (default 1)          */
+#define CUBLOX_BATCH_OPT_SHAPE 3      /* fix the launch shape (0 .. n-1)    */
+#define CUBLOX_BATCH_OPT_TIMING 4     /* record walk/fold device times      */
+#define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
+
+int cublox_batch_create(void *stream, cublox_batch **out);
+int cublox_batch_destroy(cublox_batch *b);
+/* A grid integrated by this batch (same arguments as cublox_grid_create).   */
+int cublox_batch_add_grid(cublox_batch *b, const int half_map_size[3], float resolution,
+                          int origin_at_center, int has_recenter_threshold,
+                          double recenter_threshold, const float origin[3],
+                          cublox_grid **out);
+int cublox_batch_set_option(cublox_batch *b, int key, int value);
+int cublox_batch_get_option(const cublox_batch *b, int key, int *value);
+/* One scan into each of grids[0..n): scan i is points [offsets[i],
+ * offsets[i+1]) of xyz (x0 y0 z0 x1 ..., host or device) from sensor
+ * origin sensors[3i..3i+2].  A grid may appear once per call.               */
+int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const float *xyz,
+                        const int64_t *offsets, const float *sensors);
+/* recenter(pos) of each grid (OccupancyGrid.cpp:141-179); actions may be
+ * NULL.                                                                      */
+int cublox_batch_recenter(cublox_batch *b, int n, cublox_grid *const *grids,
+                          const float *positions, int *actions);
+int cublox_batch_synchronize(cublox_batch *b);
+int cublox_batch_last_timing(cublox_batch *b, float *walk_ms, float *fold_ms);
+int cublox_batch_stream(const cublox_batch *b, void **stream);
+
 /* ---- allocation-free integration ------------------------------------------
  * No counterpart in the reference: it exists for callers that must not
  * allocate device memory while running (a real-time mapping loop that
