@@ -463,6 +463,7 @@ class OccupancyGrid:
 
 
 BATCH_OPT_GRAPHS, BATCH_OPT_AUTOTUNE, BATCH_OPT_SHAPE, BATCH_OPT_TIMING, BATCH_OPT_NUM_SHAPES = 1, 2, 3, 4, 5
+BATCH_OPT_FOLD = 6
 
 
 class Batch:

@@ -27,6 +27,7 @@
 
 #include "../../include/cublox_b200.h"
 #include "exact_fp.cuh"
+#include "fold.cuh"
 #include "grid_internal.hpp"
 #include "kernels.cuh"
 #include "ray_walk.cuh"
@@ -42,7 +43,7 @@ struct MapDesc {
   float *occ;
   float l_hit, l_miss, l_min, l_max, l_unknown;
   int clo[3];  // cube corner, global voxel index
-  int pad;
+  int n_walk;  // walk items of this map (fused launch: its folds wait for them)
 };
 
 struct WalkItem {
@@ -53,27 +54,242 @@ struct FoldItem {
   int map, g4_start, g4_count, tail;  // tail: handle the vnum % 4 voxels
 };
 
-// counters: [0] walk queue, [1] walk items, [2] fold queue, [3] fold items
-constexpr int kCounters = 4;
+// counters: [0] walk queue, [1] walk items, [2] fold queue, [3] fold items,
+// [4] a fused launch's fold wait gave up (the rest of the launch then skips
+// its waits and folds)
+constexpr int kCounters = 5;
+constexpr int kFoldItemGroups = 1 << 12;  // 16-byte counter groups per fold item
+// Fused launch: how long a fold item waits for its map's walk items
+// (iterations of a ~256 ns sleep, about 2 s) before it gives up and flags
+// kErrWaitTimeout in the map's error word.
+constexpr int kWaitIters = 1 << 23;
+
+// ---- the walk of one ray, in two phases -----------------------------------
+// Near phase: the exact walk of ray_walk.cuh (the reference's loop,
+// kernels.cu:105-137) while the voxel is inside the S^3 shared-memory cube
+// around the sensor, or outside the window.  Far phase, from the first
+// in-window voxel outside the cube on: the same loop on per-axis step
+// counters.  The cube and the window are boxes and a ray moves monotonically
+// on every axis, so once it has left either it never comes back: the far
+// phase needs no per-step box tests, only "steps left on this axis"
+// counters, and keeps the voxel's hash incrementally, with the ring
+// buffer's wrap.  The voxels visited, and so the counts, are those of the
+// single loop.
+
+struct FarWalk {
+  float tM[3], tD[3];  // as in RayWalk
+  int e[3];     // steps to the endpoint's coordinate on the axis (all 0: at the endpoint)
+  int out[3];   // steps the walk can still take on the axis inside the window
+  int wrap[3];  // steps on the axis before its ring-buffer slot wraps
+  int dh[3];    // hash change of one step on the axis
+  int left;     // loop iterations left (max_steps - k)
+  int h;        // hash of the current voxel
+};
+
+// The update after the loop (kernels.cu:138-151), fixed at the ray's start:
+// endpoint hash (-1: endpoint outside the window), its cube cell (-1: not in
+// the cube), and whether it counts a hit (not clipped at max range).
+struct RayEnd {
+  int h, c;
+  bool hit;
+};
+
+constexpr int kNever = 0x7fffffff;  // counters of an axis the ray never steps on
 
 template <int S>
-__device__ __forceinline__ void emit(const RayParams &p, uint32_t *cube, const int clo[3],
-                                     int g0, int g1, int g2, int h) {
+__device__ __forceinline__ int cube_cell(int g0, int g1, int g2, const int clo[3]) {
   const int c0 = g0 - clo[0], c1 = g1 - clo[1], c2 = g2 - clo[2];
   if (S > 0 && static_cast<unsigned>(c0) < static_cast<unsigned>(S) &&
       static_cast<unsigned>(c1) < static_cast<unsigned>(S) &&
       static_cast<unsigned>(c2) < static_cast<unsigned>(S))
-    atomicAdd(&cube[(c0 * S + c1) * S + c2], 1u);
-  else
-    atomicAdd(p.cnt + h, 1u);
+    return (c0 * S + c1) * S + c2;
+  return -1;
 }
 
 template <int S>
-__global__ void __launch_bounds__(1024) batch_walk_kernel(const MapDesc *maps,
-                                                          const WalkItem *items,
-                                                          int *counters) {
-  extern __shared__ uint32_t cube[];
+__device__ __forceinline__ RayEnd ray_end_of(const RayParams &p, const RayWalk &w,
+                                             const int clo[3]) {
+  RayEnd r;
+  r.h = end_hash(w, p);
+  r.c = r.h >= 0 ? cube_cell<S>(w.en[0], w.en[1], w.en[2], clo) : -1;
+  r.hit = !w.clipped;
+  return r;
+}
+
+template <int S>
+__device__ __forceinline__ void apply_end(const RayParams &p, uint32_t *cube, const RayEnd &r,
+                                          uint32_t &incs, uint32_t &hits) {
+  if (r.h < 0) return;
+  if (S > 0 && r.c >= 0)
+    atomicAdd(&cube[r.c], 1u);
+  else
+    atomicAdd(p.cnt + r.h, 1u);
+  ++incs;
+  if (r.hit) {
+    atomicOr(p.cnt + r.h, kHitFlag);
+    atomicAdd(p.hit + r.h, 1u);
+    ++hits;
+  }
+}
+
+// Far-phase state of a walk whose current voxel (loop iteration k, not yet
+// counted) is inside the window.
+__device__ __forceinline__ void to_far(const RayParams &p, const RayWalk &w, int k, FarWalk &f) {
+  const int stride[3] = {p.map[1] * p.map[2], p.map[2], 1};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int d = w.en[a] - w.id[a];
+    const int st = w.st[a];
+    f.tM[a] = w.tM[a];
+    f.tD[a] = w.tD[a];
+    f.e[a] = st > 0 ? d : (st < 0 ? -d : d);
+    f.out[a] = st > 0 ? p.half[a] - w.rel[a] : (st < 0 ? p.half[a] + w.rel[a] : kNever);
+    f.wrap[a] = st > 0 ? p.map[a] - 1 - w.slot[a] : (st < 0 ? w.slot[a] : kNever);
+    f.dh[a] = st * stride[a];
+  }
+  f.left = w.max_steps - k;
+  f.h = walk_hash(w, p);
+}
+
+// Near phase.  Returns true if the ray's loop ended in it; false once the
+// walk is inside the window and outside the cube (f then holds it).
+template <int S>
+__device__ __forceinline__ bool walk_near(const RayParams &p, uint32_t *cube, const int clo[3],
+                                          RayWalk &w, FarWalk &f, uint32_t &incs) {
+  for (int k = 0;; ++k) {
+    if (k >= w.max_steps || at_end(w)) return true;
+    if (in_window(w, p)) {
+      const int c = cube_cell<S>(w.id[0], w.id[1], w.id[2], clo);
+      if (c < 0) {
+        to_far(p, w, k, f);
+        return false;
+      }
+      atomicAdd(&cube[c], 1u);
+      ++incs;
+    } else if (left_for_good(w, p)) {
+      return true;
+    }
+    ray_step(w, p);
+  }
+}
+
+// One step on axis A (the tie rule picked it).  Returns true if the new
+// voxel is outside the window, which ends the loop: the next iteration would
+// break at its step limit, at the endpoint or as out of the window for good.
+template <int A>
+__device__ __forceinline__ bool far_step(FarWalk &f, int map_a) {
+  f.tM[A] = fadd(f.tM[A], f.tD[A]);
+  --f.e[A];
+  if (f.wrap[A] == 0) {
+    f.h += f.dh[A] * (1 - map_a);
+    f.wrap[A] = map_a - 1;
+  } else {
+    f.h += f.dh[A];
+    --f.wrap[A];
+  }
+  return f.out[A]-- == 0;
+}
+
+// Far phase to the end of the ray's loop.
+__device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, uint32_t &incs) {
+  for (;;) {
+    if (f.left <= 0 || (f.e[0] | f.e[1] | f.e[2]) == 0) return;
+    atomicAdd(p.cnt + f.h, 1u);
+    ++incs;
+    --f.left;
+    bool gone;
+    if (f.tM[0] < f.tM[1]) {
+      gone = f.tM[0] < f.tM[2] ? far_step<0>(f, p.map[0]) : far_step<2>(f, p.map[2]);
+    } else {
+      gone = f.tM[1] < f.tM[2] ? far_step<1>(f, p.map[1]) : far_step<2>(f, p.map[2]);
+    }
+    if (gone) return;
+  }
+}
+
+// One walk item: zero the cube, walk the item's rays (one thread per ray),
+// flush the cube into the map's counters.  Ends with a CTA barrier.
+template <int S>
+__device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &item,
+                                          uint32_t *cube) {
   constexpr int kCube = S * S * S;
+  const RayParams p = md.ray;
+  const int clo[3] = {md.clo[0], md.clo[1], md.clo[2]};
+  for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
+    reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  uint32_t rays = 0, incs = 0, hits = 0;
+  for (int i = item.start + threadIdx.x; i < item.start + item.count; i += blockDim.x) {
+    const size_t k = static_cast<size_t>(i) * p.stride;
+    RayWalk w;
+    if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;
+    ++rays;
+    const RayEnd re = ray_end_of<S>(p, w, clo);
+    FarWalk f;
+    if (!walk_near<S>(p, cube, clo, w, f, incs)) walk_far(p, f, incs);
+    apply_end<S>(p, cube, re, incs, hits);
+  }
+  __syncthreads();
+  if constexpr (S > 0) {
+    // Only in-window voxels reach the cube, so every non-zero cell hashes
+    // inside the map.
+    for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
+      const uint32_t v = cube[q];
+      if (!v) continue;
+      const int g[3] = {clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S};
+      const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
+                     (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
+                        p.map[2] +
+                    (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+      atomicAdd(p.cnt + h, v);
+    }
+  }
+  if (p.stats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      rays += __shfl_down_sync(0xffffffffu, rays, off);
+      incs += __shfl_down_sync(0xffffffffu, incs, off);
+      hits += __shfl_down_sync(0xffffffffu, hits, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(p.stats + 0, static_cast<unsigned long long>(rays));
+      atomicAdd(p.stats + 1, static_cast<unsigned long long>(incs));
+      atomicAdd(p.stats + 2, static_cast<unsigned long long>(hits));
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ FoldView fold_view(const MapDesc &m) {
+  return FoldView{m.occ, m.ray.cnt, m.ray.hit, m.ray.vnum, m.l_hit, m.l_miss, m.l_min, m.l_max,
+                  m.l_unknown, m.ray.fp};
+}
+
+// One fold item: counter groups [g4_start, g4_start + g4_count), plus the
+// vnum % 4 tail on the map's first item.
+template <int U, bool kL2>
+__device__ __forceinline__ uint32_t fold_item(const MapDesc &m, const FoldItem &item) {
+  const FoldView v = fold_view(m);
+  uint32_t touched = fold_groups<U, kL2>(v, item.g4_start + threadIdx.x,
+                                         item.g4_start + item.g4_count, blockDim.x);
+  if (item.tail) touched += fold_tail(v);
+  return touched;
+}
+
+__device__ __forceinline__ void add_touched(const MapDesc &m, uint32_t t) {
+  if (!m.ray.stats) return;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+  if ((threadIdx.x & 31) == 0 && t) atomicAdd(m.ray.stats + 3, static_cast<unsigned long long>(t));
+}
+
+// Persistent walk: CTAs take walk items from counters[0] until none is left.
+// kMinCtas 2 caps registers so that two 1024-thread CTAs share an SM.
+template <int S, int kMinCtas>
+__global__ void __launch_bounds__(1024, kMinCtas) batch_walk_kernel(const MapDesc *maps,
+                                                                    const WalkItem *items,
+                                                                    int *counters) {
+  extern __shared__ uint32_t cube[];
   __shared__ int s_item;
   const int n_items = counters[1];
   for (;;) {
@@ -82,95 +298,18 @@ __global__ void __launch_bounds__(1024) batch_walk_kernel(const MapDesc *maps,
     const int it = s_item;
     if (it >= n_items) break;
     const WalkItem item = items[it];
-    const MapDesc &md = maps[item.map];
-    const RayParams p = md.ray;
-    const int clo[3] = {md.clo[0], md.clo[1], md.clo[2]};
-    for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
-      reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
-    __syncthreads();
-    uint32_t rays = 0, incs = 0, hits = 0;
-    for (int i = item.start + threadIdx.x; i < item.start + item.count; i += blockDim.x) {
-      const size_t k = static_cast<size_t>(i) * p.stride;
-      RayWalk w;
-      if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;
-      ++rays;
-      for (int step = 0; step < w.max_steps; ++step) {
-        if (at_end(w)) break;
-        if (in_window(w, p)) {
-          emit<S>(p, cube, clo, w.id[0], w.id[1], w.id[2], walk_hash(w, p));
-          ++incs;
-        } else if (left_for_good(w, p)) {
-          break;
-        }
-        ray_step(w, p);
-      }
-      const int h = end_hash(w, p);
-      if (h >= 0) {
-        emit<S>(p, cube, clo, w.en[0], w.en[1], w.en[2], h);
-        ++incs;
-        if (!w.clipped) {
-          atomicOr(p.cnt + h, kHitFlag);
-          atomicAdd(p.hit + h, 1u);
-          ++hits;
-        }
-      }
-    }
-    __syncthreads();
-    if constexpr (S > 0) {
-      for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
-        const uint32_t v = cube[q];
-        if (!v) continue;
-        const int g[3] = {clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S};
-        const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-                       (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
-                          p.map[2] +
-                      (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
-        atomicAdd(p.cnt + h, v);
-      }
-    }
-    if (p.stats) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        rays += __shfl_down_sync(0xffffffffu, rays, off);
-        incs += __shfl_down_sync(0xffffffffu, incs, off);
-        hits += __shfl_down_sync(0xffffffffu, hits, off);
-      }
-      if ((threadIdx.x & 31) == 0) {
-        atomicAdd(p.stats + 0, static_cast<unsigned long long>(rays));
-        atomicAdd(p.stats + 1, static_cast<unsigned long long>(incs));
-        atomicAdd(p.stats + 2, static_cast<unsigned long long>(hits));
-      }
-    }
-    __syncthreads();
+    walk_item<S>(maps[item.map], item, cube);
   }
 }
 
-__device__ __forceinline__ float fold_one(const MapDesc &m, int h, uint32_t c, float s0) {
-  const int op = static_cast<int>(c & kOpMask);
-  int hit = 0;
-  if (c & kHitFlag) {
-    hit = static_cast<int>(m.ray.hit[h]);
-    m.ray.hit[h] = 0u;
-  }
-  const int miss = op > hit ? op - hit : 0;
-  const unsigned fp = m.ray.fp;
-  float l = fadd(s0, m.l_unknown);
-  l = (fp & kFpMissFma) ? ffma(m.l_miss, static_cast<float>(miss), l)
-                        : fadd(l, fmul(m.l_miss, static_cast<float>(miss)));
-  l = (fp & kFpHitFma) ? ffma(m.l_hit, static_cast<float>(hit), l)
-                       : fadd(l, fmul(m.l_hit, static_cast<float>(hit)));
-  if (l < m.l_min) l = m.l_min;
-  if (l > m.l_max) l = m.l_max;
-  return fsub(l, m.l_unknown);
-}
-
+// Persistent fold: CTAs take fold items from counters[2].  U: counter
+// groups in flight per thread (fewer registers, more resident warps).
+template <int U>
 __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
                                                          const FoldItem *items,
                                                          int *counters) {
   __shared__ int s_item;
   const int n_items = counters[3];
-  uint32_t touched = 0;
-  unsigned long long *stats = nullptr;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(&counters[2], 1);
     __syncthreads();
@@ -179,58 +318,77 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
     if (it >= n_items) break;
     const FoldItem item = items[it];
     const MapDesc &m = maps[item.map];
-    stats = m.ray.stats;
-    uint4 *c4 = reinterpret_cast<uint4 *>(m.ray.cnt);
-    float4 *o4 = reinterpret_cast<float4 *>(m.occ);
-    const int g_end = item.g4_start + item.g4_count;
-    for (int i0 = item.g4_start + threadIdx.x; i0 < g_end; i0 += 4 * blockDim.x) {
-      uint4 c[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u * blockDim.x;
-        c[u] = i < g_end ? c4[i] : make_uint4(0u, 0u, 0u, 0u);
+    add_touched(m, fold_item<U, false>(m, item));
+  }
+}
+
+// Walk and fold in one persistent launch.  Items come from one queue: every
+// walk item (ordered by map), then every fold item (ordered by map).  A fold
+// item of map m starts once all of m's walk items have finished, so later
+// maps' walks overlap earlier maps' folds.  A CTA waits only on walk items
+// that running CTAs have already taken, so the wait always ends; it is
+// bounded all the same, and once one wait gives up the launch skips the
+// remaining waits and folds (the map's error word says so).
+template <int S>
+__global__ void __launch_bounds__(1024) batch_fused_kernel(const MapDesc *maps,
+                                                           const WalkItem *witems,
+                                                           const FoldItem *fitems,
+                                                           int *counters, int *done) {
+  extern __shared__ uint32_t cube[];
+  __shared__ int s_item, s_ok;
+  const int n_w = counters[1];
+  const int n_all = n_w + counters[3];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_all) break;
+    if (it < n_w) {
+      const WalkItem item = witems[it];
+      walk_item<S>(maps[item.map], item, cube);  // ends with a barrier
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(done + item.map, 1);
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if ((c[u].x | c[u].y | c[u].z | c[u].w) == 0u) continue;
-        const int i = i0 + u * blockDim.x;
-        const int h = i << 2;
-        float4 o = o4[i];
-        if (c[u].x) { o.x = fold_one(m, h + 0, c[u].x, o.x); ++touched; }
-        if (c[u].y) { o.y = fold_one(m, h + 1, c[u].y, o.y); ++touched; }
-        if (c[u].z) { o.z = fold_one(m, h + 2, c[u].z, o.z); ++touched; }
-        if (c[u].w) { o.w = fold_one(m, h + 3, c[u].w, o.w); ++touched; }
-        o4[i] = o;
-        c4[i] = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+      const FoldItem item = fitems[it - n_w];
+      const MapDesc &m = maps[item.map];
+      if (threadIdx.x == 0) {
+        volatile int *vd = done + item.map;
+        volatile int *gave_up = counters + 4;
+        int ok = 0;
+        for (int k = 0; k < kWaitIters && !*gave_up; ++k) {
+          if (*vd >= m.n_walk) {
+            ok = 1;
+            break;
+          }
+          __nanosleep(256);
+        }
+        __threadfence();
+        if (!ok) {
+          *gave_up = 1;
+          atomicOr(m.ray.err, kErrWaitTimeout);
+        }
+        s_ok = ok;
       }
+      __syncthreads();
+      if (s_ok) add_touched(m, fold_item<2, true>(m, item));
+      __syncthreads();
     }
-    if (item.tail && threadIdx.x < (m.ray.vnum & 3)) {
-      const int h = ((m.ray.vnum >> 2) << 2) + threadIdx.x;
-      const uint32_t c = m.ray.cnt[h];
-      if (c) {
-        m.occ[h] = fold_one(m, h, c, m.occ[h]);
-        m.ray.cnt[h] = 0u;
-        ++touched;
-      }
-    }
-    if (stats) {
-      uint32_t t = touched;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
-      if ((threadIdx.x & 31) == 0 && t) atomicAdd(stats + 3, static_cast<unsigned long long>(t));
-    }
-    touched = 0;
   }
 }
 
 struct Shape {
-  int cube;   // 0, 16, 32
-  int rays;   // rays per work item
-  int block;  // walk CTA size
+  int cube;      // 0, 16, 32
+  int rays;      // rays per walk item; 0: about two items per resident CTA
+  int block;     // walk (or fused) CTA size
+  int fused;     // 1: one launch, folds overlap later maps' walks
+  int min_ctas;  // 2: registers capped for two CTAs per SM (cube <= 16)
 };
 
-const Shape kShapes[] = {{32, 1024, 512}, {16, 512, 256}, {32, 2048, 1024},
-                         {0, 1024, 512},  {32, 512, 512}, {16, 1024, 512}};
+const Shape kShapes[] = {{32, 512, 512, 0, 1},    {32, 1024, 1024, 0, 1}, {16, 512, 256, 0, 1},
+                         {16, 1024, 1024, 0, 2},  {16, 2048, 1024, 0, 2}, {0, 1024, 1024, 0, 2},
+                         {32, 1024, 1024, 1, 1},  {16, 512, 512, 1, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 int sm_count_batch() {
@@ -244,35 +402,75 @@ int sm_count_batch() {
   return n;
 }
 
-// Resident CTAs per SM of batch_walk_kernel<S> at a CTA size; sets the
-// shared-memory attribute on first use.  Called for every shape before any
-// graph capture, so capture itself only enqueues launches.
 template <int S>
-int walk_ctas_per_sm(int block) {
-  static int cached[3] = {0, 0, 0};  // block 256, 512, 1024
-  const int slot = block >= 1024 ? 2 : (block >= 512 ? 1 : 0);
-  if (cached[slot] == 0) {
-    const size_t smem = sizeof(uint32_t) * S * S * S;
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(batch_walk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
+const void *shape_kernel_s(const Shape &sh) {
+  if (sh.fused) return reinterpret_cast<const void *>(batch_fused_kernel<S>);
+  if constexpr (S < 32) {
+    if (sh.min_ctas >= 2) return reinterpret_cast<const void *>(batch_walk_kernel<S, 2>);
+  }
+  return reinterpret_cast<const void *>(batch_walk_kernel<S, 1>);
+}
+
+// The walk (or fused) kernel of a shape.
+const void *shape_kernel(const Shape &sh) {
+  return sh.cube >= 32 ? shape_kernel_s<32>(sh)
+                       : (sh.cube >= 16 ? shape_kernel_s<16>(sh) : shape_kernel_s<0>(sh));
+}
+
+size_t shape_smem(const Shape &sh) {
+  return sizeof(uint32_t) * sh.cube * sh.cube * sh.cube;
+}
+
+// CTAs of a shape's persistent launch: resident CTAs per SM x SMs.  Sets
+// the shared-memory attribute on first use; every shape is prepared when a
+// batch is created, so a graph capture only enqueues launches.
+int shape_grid(int shape) {
+  static int cached[kNumShapes] = {};
+  if (cached[shape] == 0) {
+    const Shape &sh = kShapes[shape];
+    const void *fn = shape_kernel(sh);
+    const size_t smem = shape_smem(sh);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      cudaGetLastError();
     int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_walk_kernel<S>, block,
-                                                      smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, sh.block, smem) !=
+        cudaSuccess) {
       cudaGetLastError();
       per_sm = 1;
     }
-    cached[slot] = per_sm < 1 ? 1 : per_sm;
+    cached[shape] = sm_count_batch() * (per_sm < 1 ? 1 : per_sm);
   }
-  return cached[slot];
+  return cached[shape];
 }
 
-template <int S>
-cudaError_t launch_batch_walk(const MapDesc *maps, const WalkItem *items, int *counters,
-                              int block, cudaStream_t s) {
-  const size_t smem = sizeof(uint32_t) * S * S * S;
-  batch_walk_kernel<S><<<sm_count_batch() * walk_ctas_per_sm<S>(block), block, smem, s>>>(
-      maps, items, counters);
+// Rays per walk item of a shape for a step of `total` rays.
+int shape_rays(int shape, int64_t total) {
+  const Shape &sh = kShapes[shape];
+  if (sh.rays > 0) return sh.rays;
+  const int64_t items = 2 * static_cast<int64_t>(shape_grid(shape));
+  const int64_t per = (total + items - 1) / items;
+  return static_cast<int>(std::min<int64_t>(1 << 20, std::max<int64_t>(256, (per + 31) & ~31)));
+}
+
+cudaError_t launch_walk(const MapDesc *maps, const WalkItem *witems, const FoldItem *fitems,
+                        int *counters, int *done, int shape, cudaStream_t s) {
+  const Shape &sh = kShapes[shape];
+  void *walk_args[] = {&maps, &witems, &counters};
+  void *fused_args[] = {&maps, &witems, &fitems, &counters, &done};
+  return cudaLaunchKernel(shape_kernel(sh), dim3(shape_grid(shape)), dim3(sh.block),
+                          sh.fused ? fused_args : walk_args, shape_smem(sh), s);
+}
+
+cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counters,
+                        int variant, cudaStream_t s) {
+  const dim3 grid(sm_count_batch() * 8), block(256);
+  switch (variant) {
+    case 1: batch_fold_kernel<4><<<grid, block, 0, s>>>(maps, fitems, counters); break;
+    case 2: batch_fold_kernel<1><<<grid, block, 0, s>>>(maps, fitems, counters); break;
+    default: batch_fold_kernel<2><<<grid, block, 0, s>>>(maps, fitems, counters); break;
+  }
   return cudaGetLastError();
 }
 
@@ -290,6 +488,7 @@ struct cublox_batch {
   FoldItem *d_fitems = nullptr;
   int fitems_cap = 0;
   int *d_counters = nullptr;
+  int *d_done = nullptr;  // per map: walk items finished (fused launch)
   float *d_points = nullptr;
   size_t points_cap = 0;  // floats
   // pinned host staging
@@ -307,6 +506,7 @@ struct cublox_batch {
   int tune_rounds = 2;
   std::vector<float> tune_ms;
   bool graphs = false;
+  int fold_variant = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_shape = -1;
   // timing
@@ -345,6 +545,7 @@ int ensure_capacity(cublox_batch *b, int n_maps, int n_witems, int n_fitems) {
     const int fc = std::max(n_fitems, 2 * b->fitems_cap);
     int rc;
     if ((rc = ensure_dev(reinterpret_cast<void **>(&b->d_maps), sizeof(MapDesc) * mc)) ||
+        (rc = ensure_dev(reinterpret_cast<void **>(&b->d_done), sizeof(int) * mc)) ||
         (rc = ensure_dev(reinterpret_cast<void **>(&b->d_witems), sizeof(WalkItem) * wc)) ||
         (rc = ensure_dev(reinterpret_cast<void **>(&b->d_fitems), sizeof(FoldItem) * fc)) ||
         (rc = ensure_pinned(reinterpret_cast<void **>(&b->h_maps), sizeof(MapDesc) * mc)) ||
@@ -363,27 +564,45 @@ int ensure_capacity(cublox_batch *b, int n_maps, int n_witems, int n_fitems) {
   return CUBLOX_OK;
 }
 
-// The per-step launch sequence (captured into a graph when enabled).
-cudaError_t enqueue_step(cublox_batch *b, int shape) {
+// The per-step launch sequence (captured into a graph when enabled, so it
+// depends on nothing that changes between steps but the shape and the fold
+// variant).  On failure *what names the call.
+cudaError_t enqueue_step(cublox_batch *b, int shape, const char **what) {
   const Shape &sh = kShapes[shape];
-  cudaError_t e = cudaMemsetAsync(b->d_counters, 0, sizeof(int), b->stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(b->d_counters + 2, 0, sizeof(int), b->stream);
-  if (e != cudaSuccess) return e;
-  if (b->timed) cudaEventRecord(b->ev[0], b->stream);
-  if (sh.cube >= 32)
-    e = launch_batch_walk<32>(b->d_maps, b->d_witems, b->d_counters, sh.block, b->stream);
-  else if (sh.cube >= 16)
-    e = launch_batch_walk<16>(b->d_maps, b->d_witems, b->d_counters, sh.block, b->stream);
-  else
-    e = launch_batch_walk<0>(b->d_maps, b->d_witems, b->d_counters, sh.block, b->stream);
-  if (e != cudaSuccess) return e;
-  if (b->timed) cudaEventRecord(b->ev[1], b->stream);
-  batch_fold_kernel<<<sm_count_batch() * 8, 256, 0, b->stream>>>(b->d_maps, b->d_fitems,
-                                                                 b->d_counters);
-  e = cudaGetLastError();
-  if (b->timed) cudaEventRecord(b->ev[2], b->stream);
-  return e;
+  cudaError_t e;
+  *what = "an earlier CUDA call left an error";
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  *what = "counter reset";
+  if ((e = cudaMemsetAsync(b->d_counters, 0, sizeof(int), b->stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(b->d_counters + 2, 0, sizeof(int), b->stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(b->d_counters + 4, 0, sizeof(int), b->stream)) != cudaSuccess)
+    return e;
+  if (sh.fused &&
+      (e = cudaMemsetAsync(b->d_done, 0, sizeof(int) * b->maps_cap, b->stream)) != cudaSuccess)
+    return e;
+  *what = "timing event";
+  if (b->timed && (e = cudaEventRecord(b->ev[0], b->stream)) != cudaSuccess) return e;
+  *what = sh.fused ? "fused walk+fold launch" : "walk launch";
+  if ((e = launch_walk(b->d_maps, b->d_witems, b->d_fitems, b->d_counters, b->d_done, shape,
+                       b->stream)) != cudaSuccess)
+    return e;
+  *what = "timing event";
+  if (b->timed && (e = cudaEventRecord(b->ev[1], b->stream)) != cudaSuccess) return e;
+  if (!sh.fused) {
+    *what = "fold launch";
+    if ((e = launch_fold(b->d_maps, b->d_fitems, b->d_counters, b->fold_variant, b->stream)) !=
+        cudaSuccess)
+      return e;
+  }
+  *what = "timing event";
+  if (b->timed && (e = cudaEventRecord(b->ev[2], b->stream)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+void drop_graph(cublox_batch *b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_shape = -1;
 }
 
 }  // namespace
@@ -412,15 +631,7 @@ int cublox_batch_create(void *stream, cublox_batch **out) {
     return fail(CUBLOX_ERR_NOMEM, "batch_create: allocation failed");
   }
   for (int i = 0; i < 4; ++i) cudaEventCreate(&b->ev[i]);
-  sm_count_batch();
-  for (const Shape &sh : kShapes) {
-    if (sh.cube >= 32)
-      walk_ctas_per_sm<32>(sh.block);
-    else if (sh.cube >= 16)
-      walk_ctas_per_sm<16>(sh.block);
-    else
-      walk_ctas_per_sm<0>(sh.block);
-  }
+  for (int i = 0; i < kNumShapes; ++i) shape_grid(i);
   *out = b;
   return CUBLOX_OK;
 }
@@ -434,6 +645,7 @@ int cublox_batch_destroy(cublox_batch *b) {
   cudaFree(b->d_witems);
   cudaFree(b->d_fitems);
   cudaFree(b->d_counters);
+  cudaFree(b->d_done);
   cudaFree(b->d_points);
   if (b->h_maps) cudaFreeHost(b->h_maps);
   if (b->h_witems) cudaFreeHost(b->h_witems);
@@ -478,6 +690,11 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
     case CUBLOX_BATCH_OPT_TIMING:
       b->timed = value != 0;
       return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_FOLD:
+      if (value < 0 || value > 2) break;
+      b->fold_variant = value;
+      drop_graph(b);
+      return CUBLOX_OK;
     default:
       break;
   }
@@ -492,6 +709,7 @@ int cublox_batch_get_option(const cublox_batch *b, int key, int *value) {
     case CUBLOX_BATCH_OPT_SHAPE: *value = b->shape; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_TIMING: *value = b->timed; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_NUM_SHAPES: *value = kNumShapes; return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_FOLD: *value = b->fold_variant; return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "batch_get_option: unknown key");
@@ -517,13 +735,14 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   const bool tuning = b->autotune && b->tune_step < kNumShapes * b->tune_rounds;
   const int active_shape = tuning ? shape : b->shape;
   const Shape &sh = kShapes[active_shape];
+  const int rays_per_item = shape_rays(active_shape, total);
   // work items
   int n_w = 0, n_f = 0;
   for (int i = 0; i < n; ++i) {
     const int64_t c = offsets[i + 1] - offsets[i];
-    n_w += static_cast<int>((c + sh.rays - 1) / sh.rays);
+    n_w += static_cast<int>((c + rays_per_item - 1) / rays_per_item);
     const int64_t g4 = grids[i]->voxel_num >> 2;
-    n_f += static_cast<int>((g4 + (1 << 16) - 1) >> 16) + 1;
+    n_f += static_cast<int>((g4 + kFoldItemGroups - 1) / kFoldItemGroups) + 1;
   }
   int rc = ensure_capacity(b, n, std::max(n_w, 1), std::max(n_f, 1));
   if (rc) return rc;
@@ -545,11 +764,6 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
       if ((rc = ensure_dev(reinterpret_cast<void **>(&b->d_points), floats * sizeof(float))))
         return rc;
       b->points_cap = floats;
-      if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-        b->graph_shape = -1;
-      }
     }
     if (floats > b->h_points_cap) {
       if ((rc = ensure_pinned(reinterpret_cast<void **>(&b->h_points), floats * sizeof(float))))
@@ -589,16 +803,17 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     md.l_unknown = g->l_unknown;
     for (int a = 0; a < 3; ++a)
       md.clo[a] = pos_to_global_dev(sensors[3 * i + a], g->res_inv, g->ctr, g->fp) - sh.cube / 2;
-    md.pad = 0;
-    for (int s0 = 0; s0 < c; s0 += sh.rays)
-      b->h_witems[w++] = WalkItem{d, s0, std::min(sh.rays, c - s0), 0};
+    md.n_walk = 0;
+    for (int s0 = 0; s0 < c; s0 += rays_per_item, ++md.n_walk)
+      b->h_witems[w++] = WalkItem{d, s0, std::min(rays_per_item, c - s0), 0};
     const int g4 = g->voxel_num >> 2;
-    for (int s0 = 0; s0 < g4 || (s0 == 0 && g4 == 0); s0 += (1 << 16)) {
-      b->h_fitems[f++] = FoldItem{d, s0, std::min(1 << 16, g4 - s0), s0 == 0 ? 1 : 0};
+    for (int s0 = 0; s0 < g4 || (s0 == 0 && g4 == 0); s0 += kFoldItemGroups) {
+      b->h_fitems[f++] = FoldItem{d, s0, std::min(kFoldItemGroups, g4 - s0), s0 == 0 ? 1 : 0};
       if (g4 == 0) break;
     }
     ++d;
   }
+  b->h_counters[0] = b->h_counters[2] = b->h_counters[4] = 0;
   b->h_counters[1] = w;
   b->h_counters[3] = f;
   cudaError_t e;
@@ -618,14 +833,15 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   if (tuning) b->timed = true;
   if (b->graphs && !tuning && !b->timed) {
     if (!b->graph || b->graph_shape != active_shape) {
-      if (b->graph) cudaGraphExecDestroy(b->graph);
-      b->graph = nullptr;
+      drop_graph(b);
       cudaGraph_t gr;
       if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
         return cuda_fail(e, "batch graph capture", __LINE__);
-      cudaError_t le = enqueue_step(b, active_shape);
+      const char *what = "";
+      cudaError_t le = enqueue_step(b, active_shape, &what);
       e = cudaStreamEndCapture(b->stream, &gr);
-      if (le != cudaSuccess) return cuda_fail(le, "batch graph capture launch", __LINE__);
+      if (le != cudaSuccess)
+        return cuda_fail(le, (std::string("batch graph capture: ") + what).c_str(), __LINE__);
       if (e != cudaSuccess) return cuda_fail(e, "batch graph end capture", __LINE__);
       e = cudaGraphInstantiate(&b->graph, gr, 0);
       cudaGraphDestroy(gr);
@@ -635,14 +851,16 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     if ((e = cudaGraphLaunch(b->graph, b->stream)) != cudaSuccess)
       return cuda_fail(e, "batch graph launch", __LINE__);
   } else {
-    if ((e = enqueue_step(b, active_shape)) != cudaSuccess)
-      return cuda_fail(e, "batch step launch", __LINE__);
+    const char *what = "";
+    if ((e = enqueue_step(b, active_shape, &what)) != cudaSuccess)
+      return cuda_fail(e, (std::string("batch step (shape ") + std::to_string(active_shape) +
+                           "): " + what).c_str(), __LINE__);
   }
   b->timed = timed_before;
   if (tuning) {
-    float ms = 0.0f;
-    cudaEventSynchronize(b->ev[1]);
-    cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+    float ms = 0.0f;  // walk + fold
+    cudaEventSynchronize(b->ev[2]);
+    cudaEventElapsedTime(&ms, b->ev[0], b->ev[2]);
     if (static_cast<int>(b->tune_ms.size()) < kNumShapes) b->tune_ms.assign(kNumShapes, 0.0f);
     b->tune_ms[active_shape] += ms;
     ++b->tune_step;

@@ -1,0 +1,98 @@
+// Fold of a scan's per-voxel counters into the stored log-odds
+// (the reference's applyUpdateKernel, src/kernels.cu:167-208), shared by the
+// single-grid sweep and the batched launches.
+//
+// Counter word: bits 0..30 traversal count, bit 31 "has a hit"; the hit count
+// itself sits in a second array, read only for flagged voxels.
+#pragma once
+
+#include <cstdint>
+
+#include "exact_fp.cuh"
+#include "kernels.cuh"
+
+namespace cublox_b200 {
+
+struct FoldView {
+  float *occ;
+  uint32_t *cnt;
+  uint32_t *hit;
+  int vnum;
+  float l_hit, l_miss, l_min, l_max, l_unknown;
+  unsigned fp;
+};
+
+// One voxel: miss = op - hit (never negative), stored value shifted by
+// l_unknown, miss then hit added (fused or not as the pinned contraction
+// says), clamped, shifted back (kernels.cu:179-200).  The hit count is read
+// at L2 (ld.global.cg): in a fused launch other CTAs of the same kernel
+// wrote it.
+__device__ __forceinline__ float fold_counter(const FoldView &v, int h, uint32_t c, float s0) {
+  const int op = static_cast<int>(c & kOpMask);
+  int hit = 0;
+  if (c & kHitFlag) {
+    hit = static_cast<int>(__ldcg(v.hit + h));
+    v.hit[h] = 0u;
+  }
+  const int miss = op > hit ? op - hit : 0;
+  float l = fadd(s0, v.l_unknown);
+  l = (v.fp & kFpMissFma) ? ffma(v.l_miss, static_cast<float>(miss), l)
+                          : fadd(l, fmul(v.l_miss, static_cast<float>(miss)));
+  l = (v.fp & kFpHitFma) ? ffma(v.l_hit, static_cast<float>(hit), l)
+                         : fadd(l, fmul(v.l_hit, static_cast<float>(hit)));
+  if (l < v.l_min) l = v.l_min;
+  if (l > v.l_max) l = v.l_max;
+  return fsub(l, v.l_unknown);
+}
+
+__device__ __forceinline__ bool any_set(const uint4 &c) { return (c.x | c.y | c.z | c.w) != 0u; }
+
+// Sweep of 16-byte counter groups first, first + stride, ... (< end): the U
+// counter loads of a round are issued together, then each group with a set
+// counter loads its stored values, folds and writes them back with its
+// counters zeroed.  kL2: counters are loaded at L2 (ld.global.cg), as a
+// launch that also wrote them from other CTAs needs.  Returns the voxels
+// folded.
+template <int U, bool kL2>
+__device__ __forceinline__ uint32_t fold_groups(const FoldView &v, int first, int end,
+                                                int stride) {
+  const uint4 *c4r = reinterpret_cast<const uint4 *>(v.cnt);
+  uint4 *c4 = reinterpret_cast<uint4 *>(v.cnt);
+  float4 *o4 = reinterpret_cast<float4 *>(v.occ);
+  uint32_t touched = 0;
+  for (int i0 = first; i0 < end; i0 += U * stride) {
+    uint4 c[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * stride;
+      c[u] = i < end ? (kL2 ? __ldcg(c4r + i) : c4r[i]) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!any_set(c[u])) continue;
+      const int i = i0 + u * stride;
+      const int h = i << 2;
+      float4 o = o4[i];
+      if (c[u].x) { o.x = fold_counter(v, h + 0, c[u].x, o.x); ++touched; }
+      if (c[u].y) { o.y = fold_counter(v, h + 1, c[u].y, o.y); ++touched; }
+      if (c[u].z) { o.z = fold_counter(v, h + 2, c[u].z, o.z); ++touched; }
+      if (c[u].w) { o.w = fold_counter(v, h + 3, c[u].w, o.w); ++touched; }
+      o4[i] = o;
+      c4[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+  return touched;
+}
+
+// The vnum % 4 voxels after the last whole group, one per thread 0..2.
+__device__ __forceinline__ uint32_t fold_tail(const FoldView &v) {
+  if (threadIdx.x >= static_cast<unsigned>(v.vnum & 3)) return 0;
+  const int h = ((v.vnum >> 2) << 2) + threadIdx.x;
+  const uint32_t c = __ldcg(v.cnt + h);
+  if (!c) return 0;
+  v.occ[h] = fold_counter(v, h, c, v.occ[h]);
+  v.cnt[h] = 0u;
+  return 1;
+}
+
+}  // namespace cublox_b200

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdint>
 
+#include "fold.cuh"
 #include "kernels.cuh"
 #include "ray_walk.cuh"
 
@@ -91,24 +92,14 @@ __global__ void __launch_bounds__(256) step_count_kernel(const RayParams p) {
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(p.stats, v);
 }
 
-// Fold one voxel's counters (applyUpdateKernel, kernels.cu:179-200).
+__device__ __forceinline__ FoldView fold_view(const ApplyParams &p) {
+  return FoldView{p.occ, p.cnt, p.hit, p.vnum, p.l_hit, p.l_miss, p.l_min, p.l_max,
+                  p.l_unknown, p.fp};
+}
+
+// Fold one voxel's counters in place (applyUpdateKernel, kernels.cu:179-200).
 __device__ __forceinline__ void fold(const ApplyParams &p, int h, uint32_t c) {
-  const int op = static_cast<int>(c & kOpMask);
-  int hit = 0;
-  if (c & kHitFlag) {
-    hit = static_cast<int>(p.hit[h]);
-    p.hit[h] = 0u;
-  }
-  const int miss = op > hit ? op - hit : 0;
-  const float s0 = p.occ[h];
-  float l = fadd(s0, p.l_unknown);
-  l = (p.fp & kFpMissFma) ? ffma(p.l_miss, static_cast<float>(miss), l)
-                          : fadd(l, fmul(p.l_miss, static_cast<float>(miss)));
-  l = (p.fp & kFpHitFma) ? ffma(p.l_hit, static_cast<float>(hit), l)
-                         : fadd(l, fmul(p.l_hit, static_cast<float>(hit)));
-  if (l < p.l_min) l = p.l_min;
-  if (l > p.l_max) l = p.l_max;
-  p.occ[h] = fsub(l, p.l_unknown);
+  p.occ[h] = fold_counter(fold_view(p), h, c, p.occ[h]);
 }
 
 template <bool kStats>
@@ -146,65 +137,14 @@ __global__ void __launch_bounds__(256) apply_sweep_kernel(const ApplyParams p) {
   }
 }
 
-// Fold of one counter word into a stored value already in a register.
-__device__ __forceinline__ float fold_value(const ApplyParams &p, int h, uint32_t c, float s0) {
-  const int op = static_cast<int>(c & kOpMask);
-  int hit = 0;
-  if (c & kHitFlag) {
-    hit = static_cast<int>(p.hit[h]);
-    p.hit[h] = 0u;
-  }
-  const int miss = op > hit ? op - hit : 0;
-  float l = fadd(s0, p.l_unknown);
-  l = (p.fp & kFpMissFma) ? ffma(p.l_miss, static_cast<float>(miss), l)
-                          : fadd(l, fmul(p.l_miss, static_cast<float>(miss)));
-  l = (p.fp & kFpHitFma) ? ffma(p.l_hit, static_cast<float>(hit), l)
-                         : fadd(l, fmul(p.l_hit, static_cast<float>(hit)));
-  if (l < p.l_min) l = p.l_min;
-  if (l > p.l_max) l = p.l_max;
-  return fsub(l, p.l_unknown);
-}
-
-// Sweep with 16-byte accesses and four independent counter loads in flight
-// per thread; a group of four voxels is read and written back only if one
-// of its counters is set.
+// Grid-stride sweep of 16-byte counter groups, four counter loads in flight
+// per thread (fold_groups); the vnum % 4 tail by block 0.
 template <bool kStats>
 __global__ void __launch_bounds__(256) fold_vec_kernel(const ApplyParams p) {
-  const int n4 = p.vnum >> 2;
-  const int stride = gridDim.x * blockDim.x;
-  uint4 *c4 = reinterpret_cast<uint4 *>(p.cnt);
-  float4 *o4 = reinterpret_cast<float4 *>(p.occ);
-  uint32_t touched = 0;
-  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n4; i0 += 4 * stride) {
-    uint4 c[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = i0 + u * stride;
-      c[u] = i < n4 ? c4[i] : make_uint4(0u, 0u, 0u, 0u);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if ((c[u].x | c[u].y | c[u].z | c[u].w) == 0u) continue;
-      const int i = i0 + u * stride;
-      const int h = i << 2;
-      float4 o = o4[i];
-      if (c[u].x) { o.x = fold_value(p, h + 0, c[u].x, o.x); ++touched; }
-      if (c[u].y) { o.y = fold_value(p, h + 1, c[u].y, o.y); ++touched; }
-      if (c[u].z) { o.z = fold_value(p, h + 2, c[u].z, o.z); ++touched; }
-      if (c[u].w) { o.w = fold_value(p, h + 3, c[u].w, o.w); ++touched; }
-      o4[i] = o;
-      c4[i] = make_uint4(0u, 0u, 0u, 0u);
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x < (p.vnum & 3)) {
-    const int h = (n4 << 2) + threadIdx.x;
-    const uint32_t c = p.cnt[h];
-    if (c) {
-      p.occ[h] = fold_value(p, h, c, p.occ[h]);
-      p.cnt[h] = 0u;
-      ++touched;
-    }
-  }
+  const FoldView v = fold_view(p);
+  uint32_t touched = fold_groups<4, false>(v, blockIdx.x * blockDim.x + threadIdx.x,
+                                           p.vnum >> 2, gridDim.x * blockDim.x);
+  if (blockIdx.x == 0) touched += fold_tail(v);
   if (kStats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)

@@ -21,6 +21,7 @@ constexpr uint32_t kOpMask = 0x7fffffffu;
 constexpr uint32_t kErrHashRange = 1u << 0;
 constexpr uint32_t kErrFetchOverflow = 1u << 1;
 constexpr uint32_t kErrJumpStall = 1u << 2;
+constexpr uint32_t kErrWaitTimeout = 1u << 3;  // fused batch launch: a fold wait gave up
 
 struct RayParams {
   const float *x, *y, *z;  // point i is (x[i*stride], y[i*stride], z[i*stride])

@@ -196,7 +196,8 @@ int cublox_grid_reference_steps(cublox_grid *g, const float *xyz, int n,
                                 int64_t *voxel_steps);
 
 /* Device error word: nonzero if a kernel's own bounds checks rejected an
- * index (a bug, never expected).  Reading it clears it.                    */
+ * index (a bug, never expected), or (bit 3) a fused batch launch stopped
+ * waiting for the map's walk and skipped its fold.  Reading it clears it. */
 int cublox_grid_check(cublox_grid *g, uint32_t *error_word);
 
 /* ---- batched integration ----------------------------------------------------
@@ -204,8 +205,9 @@ int cublox_grid_check(cublox_grid *g, uint32_t *error_word);
  * scan at a time (OccupancyGrid::update per map).  A batch owns grids created
  * through it (they share its stream and stay usable through every
  * cublox_grid_* call) and integrates one scan into each of many of them in
- * one walk launch and one fold launch.  Results are identical to calling
- * cublox_grid_update on each grid.                                          */
+ * one persistent walk launch and one fold launch, or (fused shapes) in one
+ * persistent launch that folds each map as soon as its walk is done.
+ * Results are identical to calling cublox_grid_update on each grid.         */
 typedef struct cublox_batch cublox_batch;
 
 #define CUBLOX_BATCH_OPT_GRAPHS 1     /* replay the launch sequence from a CUDA
@@ -215,6 +217,9 @@ typedef struct cublox_batch cublox_batch;
 #define CUBLOX_BATCH_OPT_SHAPE 3      /* fix the launch shape (0 .. n-1)    */
 #define CUBLOX_BATCH_OPT_TIMING 4     /* record walk/fold device times      */
 #define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
+#define CUBLOX_BATCH_OPT_FOLD 6       /* fold sweep: counter groups in flight
+                                         per thread, 0: two (default),
+                                         1: four, 2: one                    */
 
 int cublox_batch_create(void *stream, cublox_batch **out);
 int cublox_batch_destroy(cublox_batch *b);

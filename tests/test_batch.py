@@ -58,6 +58,8 @@ def run_and_compare(w, batch, bg, solo, feed, skip=()):
         for m in range(w.n_maps):
             assert tuple(bg[m].getOriginIndex()) == tuple(solo[m].getOriginIndex()), (k, m)
             assert same_bits(bg[m].export(), solo[m].export()), (k, m)
+    for m in range(w.n_maps):
+        assert bg[m].check() == 0, m
 
 
 def feed_lists(batch, bg, clouds, sensors):
@@ -84,7 +86,7 @@ def feed_pinned(batch, bg, clouds, sensors):
 
 @pytest.mark.parametrize("graphs", [False, True])
 def test_batch_matches_solo_updates_through_tuning(graphs):
-    w = small_workload(n_steps=14)  # 6 shapes x 2 tuning rounds, then the chosen one
+    w = small_workload(n_steps=18)  # 8 shapes x 2 tuning rounds, then the chosen one
     b = C.Batch()
     b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
     bg, solo = setup(w, b)
@@ -93,11 +95,13 @@ def test_batch_matches_solo_updates_through_tuning(graphs):
     b.close()
 
 
-@pytest.mark.parametrize("shape", range(6))
+@pytest.mark.parametrize("shape", range(8))
 def test_every_shape_gives_the_same_maps(shape):
     w = small_workload(n_maps=4, n_steps=3, seed=7)
     b = C.Batch()
+    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 8
     b.set_option(C.BATCH_OPT_SHAPE, shape)
+    b.set_option(C.BATCH_OPT_FOLD, shape % 3)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
     bg, solo = setup(w, b)
     run_and_compare(w, b, bg, solo, feed_lists)
@@ -149,5 +153,7 @@ def test_batch_rejects_bad_calls():
         b.update([g], pts, so, offsets=np.array([4, 0], np.int64))
     with pytest.raises(C.CubloxError):
         b.set_option(C.BATCH_OPT_SHAPE, 99)
+    with pytest.raises(C.CubloxError):
+        b.set_option(C.BATCH_OPT_FOLD, 3)
     b.update([], [], np.zeros((0, 3), np.float32))
     b.close()
