@@ -46,6 +46,21 @@ class ScanStats(ctypes.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
+class ServerConfig(ctypes.Structure):
+    """cublox_server_config."""
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_tick_points", ctypes.c_int),
+                ("max_tick_maps", ctypes.c_int), ("max_inflight_ticks", ctypes.c_int),
+                ("graphs", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    """cublox_server_stats."""
+    _fields_ = [("ticks", ctypes.c_int64), ("scans", ctypes.c_int64), ("fetches", ctypes.c_int64),
+                ("points", ctypes.c_int64), ("admissions", ctypes.c_int64),
+                ("evictions", ctypes.c_int64), ("resident_bytes", ctypes.c_uint64),
+                ("peak_resident_bytes", ctypes.c_uint64), ("resident_maps", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -113,6 +128,24 @@ def lib():
             "cublox_batch_synchronize": ([ctypes.c_void_p], ctypes.c_int),
             "cublox_batch_last_timing": ([ctypes.c_void_p, f, f], ctypes.c_int),
             "cublox_batch_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+            "cublox_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)],
+                                     ctypes.c_int),
+            "cublox_server_destroy": ([ctypes.c_void_p], ctypes.c_int),
+            "cublox_server_add_map": ([ctypes.c_void_p, i, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, f, ctypes.c_float, f, i], ctypes.c_int),
+            "cublox_server_submit_scan": ([ctypes.c_void_p, ctypes.c_int, f, ctypes.c_int, f, ctypes.c_int,
+                                           i64], ctypes.c_int),
+            "cublox_server_submit_fetch": ([ctypes.c_void_p, ctypes.c_int, f, ctypes.c_int, ctypes.c_float,
+                                            ctypes.c_int, ctypes.c_int, i64], ctypes.c_int),
+            "cublox_server_wait": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, i], ctypes.c_int),
+            "cublox_server_drain": ([ctypes.c_void_p], ctypes.c_int),
+            "cublox_server_request_times": ([ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+            "cublox_server_fetch_result": ([ctypes.c_void_p, ctypes.c_int64, i64, f,
+                                            ctypes.POINTER(ctypes.c_uint8), ctypes.c_int64, i64], ctypes.c_int),
+            "cublox_server_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+            "cublox_server_export": ([ctypes.c_void_p, ctypes.c_int, f, i], ctypes.c_int),
+            "cublox_server_get_stats": ([ctypes.c_void_p, ctypes.POINTER(ServerStats)], ctypes.c_int),
             "cublox_grid_enable_timing": ([G, ctypes.c_int], ctypes.c_int),
             "cublox_grid_set_option": ([G, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "cublox_grid_get_option": ([G, ctypes.c_int, i], ctypes.c_int),
@@ -563,6 +596,109 @@ class Batch:
         return s.value or 0
 
 
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """The served form (cublox_server_*): many robots' maps kept on the
+    device under an HBM budget, scans and fetches submitted from any thread
+    and integrated in continuously formed batches by a worker thread."""
+
+    def __init__(self, hbm_budget_bytes: int = 120 << 30, max_tick_points: int = 1 << 20,
+                 max_tick_maps: int = 0, max_inflight_ticks: int = 2, graphs: bool = False):
+        cfg = ServerConfig(int(hbm_budget_bytes), int(max_tick_points), int(max_tick_maps),
+                           int(max_inflight_ticks), int(bool(graphs)))
+        self._s = ctypes.c_void_p()
+        _check(lib().cublox_server_create(ctypes.byref(cfg), ctypes.byref(self._s)), "Server")
+        self.maps = []
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().cublox_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_map(self, half_map_size_i, resolution, origin_at_center=False, recenter_threshold=None,
+                origin=(0.0, 0.0, 0.0), max_range=25.0, log_odds=None) -> int:
+        mid = ctypes.c_int()
+        lo = None if log_odds is None else (ctypes.c_float * 6)(*[float(v) for v in log_odds])
+        _check(lib().cublox_server_add_map(self._s, (ctypes.c_int * 3)(*[int(v) for v in half_map_size_i]),
+                                           float(resolution), int(bool(origin_at_center)),
+                                           int(recenter_threshold is not None),
+                                           float(recenter_threshold or 0.0), _f3(origin), float(max_range),
+                                           lo, ctypes.byref(mid)), "add_map")
+        self.maps.append(mid.value)
+        return mid.value
+
+    def submit_scan(self, map_id: int, points, sensor_origin, recenter: bool = True) -> int:
+        p = np.ascontiguousarray(np.asarray(points, dtype=np.float32).reshape(-1, 3))
+        rid = ctypes.c_int64()
+        _check(lib().cublox_server_submit_scan(self._s, int(map_id), _fp(p), p.shape[0], _f3(sensor_origin),
+                                               int(bool(recenter)), ctypes.byref(rid)), "submit_scan")
+        return rid.value
+
+    def submit_fetch(self, map_id: int, centers, radius: float, state_filter=None,
+                     max_results: int = 0) -> int:
+        c = np.ascontiguousarray(np.asarray(centers, dtype=np.float32).reshape(-1, 3))
+        rid = ctypes.c_int64()
+        flt = -1 if state_filter is None else int(state_filter)
+        _check(lib().cublox_server_submit_fetch(self._s, int(map_id), _fp(c), c.shape[0], float(radius), flt,
+                                                int(max_results), ctypes.byref(rid)), "submit_fetch")
+        return rid.value
+
+    def wait(self, request_id: int, timeout_s: float = -1.0) -> int:
+        st = ctypes.c_int()
+        _check(lib().cublox_server_wait(self._s, int(request_id), float(timeout_s), ctypes.byref(st)),
+               "wait")
+        return st.value
+
+    def drain(self):
+        _check(lib().cublox_server_drain(self._s), "drain")
+
+    def times(self, request_id: int):
+        """(submission-to-start ms, submission-to-done ms) of a finished request."""
+        q, l = ctypes.c_double(), ctypes.c_double()
+        _check(lib().cublox_server_request_times(self._s, int(request_id), ctypes.byref(q), ctypes.byref(l)),
+               "request_times")
+        return q.value, l.value
+
+    def fetch_result(self, request_id: int, n_centers: int):
+        """(offsets (n+1,), positions, states) of a finished fetch."""
+        n = ctypes.c_int64()
+        off = np.zeros(n_centers + 1, dtype=np.int64)
+        L = lib()
+        _check(L.cublox_server_fetch_result(self._s, int(request_id),
+                                            off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), None, None, 0,
+                                            ctypes.byref(n)), "fetch_result")
+        pos = np.empty((max(n.value, 1), 3), dtype=np.float32)
+        st = np.empty(max(n.value, 1), dtype=np.uint8)
+        _check(L.cublox_server_fetch_result(self._s, int(request_id),
+                                            off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _fp(pos),
+                                            st.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n.value,
+                                            ctypes.byref(n)), "fetch_result")
+        return off, pos[: n.value], st[: n.value]
+
+    def release(self, request_id: int):
+        _check(lib().cublox_server_release(self._s, int(request_id)), "release")
+
+    def export(self, map_id: int, voxel_num: int):
+        """(stored log-odds (voxel_num,), window origin index) after draining."""
+        occ = np.empty(voxel_num, dtype=np.float32)
+        o = (ctypes.c_int * 3)()
+        _check(lib().cublox_server_export(self._s, int(map_id), _fp(occ), o), "server export")
+        return occ, tuple(o)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().cublox_server_get_stats(self._s, ctypes.byref(st)), "server stats")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
 _libm = None
 
 
@@ -586,4 +722,4 @@ def yaml_log_odds():
     return tuple(logit(p) for p in (0.9, 0.49, 0.12, 0.98, 0.499, 0.85))
 
 
-__all__ = ["OccupancyGrid", "Batch", "VoxelState", "CubloxError", "lib", "logit", "LIB_PATH"]
+__all__ = ["OccupancyGrid", "Batch", "Server", "VoxelState", "CubloxError", "lib", "logit", "LIB_PATH"]

@@ -107,6 +107,8 @@ static void free_all(cublox_grid *g) {
   cudaFree(g->d_stats);
   cudaFree(g->d_err);
   cudaFree(g->d_masks);
+  if (g->h_masks) cudaFreeHost(g->h_masks);
+  if (g->mask_ev) cudaEventDestroy(g->mask_ev);
   cudaFree(g->d_cloud);
   cudaFree(g->d_bins);
   cudaFree(g->d_work);
@@ -537,6 +539,66 @@ RayParams cublox_b200::detail::ray_params(const cublox_grid *g, const float *x,
   return p;
 }
 
+size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
+  size_t b = 12 * static_cast<size_t>(g->d_occ ? g->voxel_num : 0);
+  b += sizeof(float) * 3 * static_cast<size_t>(g->cloud_cap);
+  b += g->fq_bytes + 13 * static_cast<size_t>(g->fcap) + 13 * static_cast<size_t>(g->qcap);
+  b += static_cast<size_t>(g->split_cap) * (16 * split_seg_bytes() + 64);  // 16 segments a ray
+  b += static_cast<size_t>(g->bin_cap) * 16;
+  return b;
+}
+
+int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e == cudaSuccess && occ_host && g->d_occ)
+    e = cudaMemcpy(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->voxel_num),
+                   cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "release_device", __LINE__);
+  void **bufs[] = {reinterpret_cast<void **>(&g->d_occ),   reinterpret_cast<void **>(&g->d_cnt),
+                   reinterpret_cast<void **>(&g->d_hit),   reinterpret_cast<void **>(&g->d_cloud),
+                   reinterpret_cast<void **>(&g->d_bins),  reinterpret_cast<void **>(&g->d_work),
+                   reinterpret_cast<void **>(&g->d_segs),  reinterpret_cast<void **>(&g->d_rays),
+                   reinterpret_cast<void **>(&g->d_hist),  reinterpret_cast<void **>(&g->d_sorted),
+                   reinterpret_cast<void **>(&g->d_fq),    reinterpret_cast<void **>(&g->d_fpos),
+                   reinterpret_cast<void **>(&g->d_fstate), reinterpret_cast<void **>(&g->d_qout),
+                   reinterpret_cast<void **>(&g->d_qin)};
+  for (void **b : bufs) {
+    cudaFree(*b);
+    *b = nullptr;
+  }
+  g->cloud_cap = g->split_cap = g->bin_cap = g->qcap = 0;
+  g->fcap = 0;
+  g->fq_bytes = 0;
+  return CUBLOX_OK;
+}
+
+int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host) {
+  const size_t n = static_cast<size_t>(g->voxel_num);
+  cudaError_t e = cudaSuccess;
+  if (!g->d_occ) e = cudaMalloc(&g->d_occ, n * sizeof(float));
+  if (e == cudaSuccess && !g->d_cnt) e = cudaMalloc(&g->d_cnt, n * sizeof(uint32_t));
+  if (e == cudaSuccess && !g->d_hit) e = cudaMalloc(&g->d_hit, n * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(g->d_occ);
+    cudaFree(g->d_cnt);
+    cudaFree(g->d_hit);
+    g->d_occ = nullptr;
+    g->d_cnt = g->d_hit = nullptr;
+    return fail(CUBLOX_ERR_NOMEM, "acquire_device: voxel buffers do not fit");
+  }
+  if ((e = cudaMemsetAsync(g->d_cnt, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(g->d_hit, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess)
+    return cuda_fail(e, "acquire_device", __LINE__);
+  if (occ_host)
+    e = cudaMemcpyAsync(g->d_occ, occ_host, n * sizeof(float), cudaMemcpyHostToDevice, g->stream);
+  else
+    e = cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "acquire_device", __LINE__);
+  return CUBLOX_OK;
+}
+
 using cublox_b200::detail::snap_first_run;
 
 extern "C" {
@@ -682,7 +744,17 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
     if (a == 2) any_z = true;
   }
   const size_t mb = masks.size() * sizeof(uint32_t);
-  CK(cudaMemcpyAsync(g->d_masks, masks.data(), mb, cudaMemcpyHostToDevice, g->stream));
+  // Pinned staging, reused once the previous recenter's copy has run, so the
+  // host does not wait for the stream.
+  if (!g->h_masks) {
+    CK(cudaMallocHost(&g->h_masks, mb));
+    CK(cudaEventCreateWithFlags(&g->mask_ev, cudaEventDisableTiming));
+  } else {
+    CK(cudaEventSynchronize(g->mask_ev));
+  }
+  std::memcpy(g->h_masks, masks.data(), mb);
+  CK(cudaMemcpyAsync(g->d_masks, g->h_masks, mb, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaEventRecord(g->mask_ev, g->stream));
   ClearParams cp{};
   cp.occ = g->d_occ;
   cp.xmask = g->d_masks;
@@ -694,8 +766,6 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
   launch_clear(cp, g->stream);
   CK_LAUNCH();
   tmark(g, 2, 1);
-  // masks is a host vector: wait for the async copy before it goes away.
-  CK(cudaStreamSynchronize(g->stream));
   set_origin(g, no);
   if (action) *action = 1;
   return CUBLOX_OK;

@@ -59,6 +59,8 @@ struct cublox_grid {
   unsigned long long *d_stats = nullptr;  // 4
   uint32_t *d_err = nullptr;
   uint32_t *d_masks = nullptr;  // recenter slab masks
+  uint32_t *h_masks = nullptr;  // pinned staging of the masks
+  cudaEvent_t mask_ev = nullptr;  // staging free again
   int mask_words[3] = {0, 0, 0};
 
   float *d_cloud = nullptr;  // SoA [x|y|z]
@@ -89,5 +91,16 @@ void snap_first_run(cublox_grid *g, const float sensor[3]);
 // RayParams of one scan on this grid (points and counters filled in).
 RayParams ray_params(const cublox_grid *g, const float *x, const float *y, const float *z,
                      int n, int stride, const float sensor[3]);
+// Device memory a grid holds now: voxel buffers plus the per-call scratch
+// it has grown.
+size_t device_bytes(const cublox_grid *g);
+// Give back every device buffer of a grid but the few bytes of bookkeeping,
+// copying the stored log-odds to occ_host first (if not null).  The grid
+// keeps its host state (window origin, parameters) and must not be used
+// until acquire_device.
+int release_device(cublox_grid *g, float *occ_host);
+// Allocate the voxel buffers again, stored log-odds from occ_host (all
+// unknown if null), counters zero.
+int acquire_device(cublox_grid *g, const float *occ_host);
 }  // namespace detail
 }  // namespace cublox_b200

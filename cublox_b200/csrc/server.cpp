@@ -1,0 +1,624 @@
+// Served integration: a request loop over many resident maps
+// (include/cublox_b200.h, cublox_server_*).
+//
+// Callers (one per robot, any thread) submit scans and sphere fetches; the
+// call copies the request and returns.  One worker thread forms "ticks":
+// every map whose oldest pending request is a scan contributes that scan,
+// up to the tick's point budget, and the tick is integrated by one batched
+// launch sequence (cublox_batch_update, then each map's recenter).  A tick
+// is enqueued while the previous one still runs on the device, so requests
+// that arrive meanwhile join the next launch instead of waiting for a queue
+// to drain (continuous batching); per-map order is kept because every map
+// lives on the one stream and takes at most one scan per tick.  A second
+// thread waits on each tick's event and stamps its requests done.
+//
+// Device memory is admitted against a budget: a map's voxel buffers (12 B a
+// voxel) are allocated when its first request is served; if they do not fit
+// beside the maps already resident, the least recently used maps with no
+// work in the current tick are evicted (stored log-odds copied to host
+// memory, buffers freed) and brought back, bit for bit, when their next
+// request is served.  A map larger than the whole budget fails its requests.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/cublox_b200.h"
+#include "grid_internal.hpp"
+
+using cublox_b200::detail::fail;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+enum ReqKind { kScan = 0, kFetch = 1 };
+
+struct Request {
+  int64_t id = 0;
+  int kind = kScan;
+  int map = 0;
+  // scan
+  std::vector<float> pts;  // x0 y0 z0 x1 ...
+  float sensor[3] = {0, 0, 0};
+  int recenter = 0;
+  // fetch
+  std::vector<float> centers;
+  float radius = 0.0f;
+  int filter = CUBLOX_FILTER_ALL;
+  int max_results = 0;
+  std::vector<int64_t> offsets;
+  std::vector<float> fpos;
+  std::vector<uint8_t> fstate;
+  // progress
+  int state = CUBLOX_REQ_QUEUED;
+  int error = CUBLOX_OK;
+  std::string message;
+  Clock::time_point t_submit, t_start, t_done;
+};
+
+struct MapState {
+  int half[3];
+  float res;
+  int ctr, has_thr;
+  double thr;
+  float origin[3];
+  float max_range;
+  float lo[6];
+  bool has_lo = false;
+  cublox_grid *g = nullptr;  // created at first admission
+  bool resident = false;
+  std::vector<float> snapshot;  // stored log-odds while evicted
+  size_t vox_bytes = 0;
+  uint64_t last_use = 0;
+  std::deque<Request *> queue;  // pending requests, arrival order
+};
+
+struct Tick {
+  cudaEvent_t done = nullptr;
+  std::vector<Request *> reqs;
+};
+
+}  // namespace
+
+struct cublox_server {
+  cublox_server_config cfg{};
+  cublox_batch *batch = nullptr;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv_work;      // new requests, or stop
+  std::condition_variable cv_done;      // a request finished
+  std::condition_variable cv_inflight;  // a tick left the device
+  std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
+  std::vector<std::unique_ptr<MapState>> maps;  // reserved: never reallocated
+  std::atomic<int> n_maps{0};                    // maps[0, n_maps) are published
+  std::deque<Tick> inflight;
+  std::vector<cudaEvent_t> free_events;
+  int64_t next_id = 1;
+  int64_t pending = 0;  // requests not yet done
+  uint64_t clock = 0;   // use counter for LRU
+  size_t resident_bytes = 0;
+  cublox_server_stats stats{};
+  bool stop = false;
+  std::thread worker, completer;
+  int rr = 0;  // round-robin start of tick formation
+};
+
+namespace {
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+void finish(cublox_server *s, Request *r, int error, const std::string &msg) {
+  r->t_done = Clock::now();
+  r->error = error;
+  r->message = msg;
+  r->state = error ? CUBLOX_REQ_FAILED : CUBLOX_REQ_DONE;
+  --s->pending;
+}
+
+size_t scratch_bytes(cublox_server *s) {
+  // batch point buffer at the tick budget, plus descriptors
+  return 12 * static_cast<size_t>(s->cfg.max_tick_points) + (1u << 20);
+}
+
+constexpr int kMaxMaps = 4096;
+
+size_t used_bytes(cublox_server *s) {
+  size_t b = scratch_bytes(s);
+  const int nm = s->n_maps.load();
+  for (int j = 0; j < nm; ++j)
+    if (s->maps[j]->resident) b += cublox_b200::detail::device_bytes(s->maps[j]->g);
+  return b;
+}
+
+// Make map `mi` resident, evicting least recently used maps not in `busy`
+// (the maps already admitted for the launch being formed).  *later is set
+// when the map fits the budget but not beside the busy maps: the request
+// waits for a later tick.  Runs on the worker thread, without the lock.
+int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) {
+  *later = false;
+  MapState &m = *s->maps[mi];
+  m.last_use = ++s->clock;
+  if (m.resident) return CUBLOX_OK;
+  const size_t need = m.vox_bytes;
+  if (need + scratch_bytes(s) > s->cfg.hbm_budget_bytes)
+    return fail(CUBLOX_ERR_NOMEM, "server: map needs " + std::to_string(need) +
+                                      " bytes, more than the budget allows");
+  while (used_bytes(s) + need > s->cfg.hbm_budget_bytes) {
+    int victim = -1;
+    for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
+      MapState &o = *s->maps[j];
+      if (j == mi || !o.resident || busy[j]) continue;
+      if (victim < 0 || o.last_use < s->maps[victim]->last_use) victim = j;
+    }
+    if (victim < 0) {
+      *later = true;
+      return fail(CUBLOX_ERR_NOMEM, "server: no map can be evicted");
+    }
+    MapState &v = *s->maps[victim];
+    v.snapshot.resize(static_cast<size_t>(v.g->voxel_num));
+    int rc = cublox_b200::detail::release_device(v.g, v.snapshot.data());
+    if (rc) return rc;
+    v.resident = false;
+    std::lock_guard<std::mutex> lk(s->mu);
+    ++s->stats.evictions;
+  }
+  int rc;
+  if (!m.g) {
+    rc = cublox_grid_create(m.half, m.res, m.ctr, m.has_thr, m.thr, m.origin, s->stream, &m.g);
+    if (rc) return rc;
+    cublox_grid_set_max_range(m.g, m.max_range);
+    if (m.has_lo) cublox_grid_set_log_odds(m.g, m.lo[0], m.lo[1], m.lo[2], m.lo[3], m.lo[4], m.lo[5]);
+  } else {
+    rc = cublox_b200::detail::acquire_device(m.g, m.snapshot.empty() ? nullptr : m.snapshot.data());
+    if (rc) return rc;
+    std::vector<float>().swap(m.snapshot);
+  }
+  m.resident = true;
+  const size_t used = used_bytes(s);
+  std::lock_guard<std::mutex> lk(s->mu);
+  ++s->stats.admissions;
+  s->stats.resident_bytes = used;
+  s->stats.peak_resident_bytes = std::max(s->stats.peak_resident_bytes, used);
+  return CUBLOX_OK;
+}
+
+cudaEvent_t take_event(cublox_server *s) {
+  if (!s->free_events.empty()) {
+    cudaEvent_t e = s->free_events.back();
+    s->free_events.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  return e;
+}
+
+// Put a request back at the head of its map's queue.
+void defer(cublox_server *s, Request *r) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->state = CUBLOX_REQ_QUEUED;
+  s->maps[r->map]->queue.push_front(r);
+}
+
+// One fetch request, synchronously on the worker thread, after the tick's
+// launches are queued (nothing else is waiting to launch).
+void run_fetch(cublox_server *s, Request *r) {
+  std::vector<char> busy(static_cast<size_t>(s->n_maps.load()), 0);
+  bool later = false;
+  int rc = admit(s, r->map, busy, &later);
+  MapState &m = *s->maps[r->map];
+  const int nc = static_cast<int>(r->centers.size() / 3);
+  std::vector<int64_t> counts(static_cast<size_t>(nc));
+  if (!rc)
+    rc = cublox_grid_fetch_counts(m.g, r->centers.data(), nc, r->radius, r->filter,
+                                  r->max_results, counts.data());
+  if (!rc) {
+    int64_t total = 0;
+    for (int64_t c : counts) total += c;
+    r->offsets.assign(static_cast<size_t>(nc) + 1, 0);
+    r->fpos.resize(3 * static_cast<size_t>(total));
+    r->fstate.resize(static_cast<size_t>(total));
+    rc = cublox_grid_fetch_batch(m.g, r->centers.data(), nc, r->radius, r->filter,
+                                 r->max_results, r->offsets.data(), r->fpos.data(),
+                                 r->fstate.data(), total);
+  }
+  const std::string msg = rc ? cublox_last_error() : "";
+  std::lock_guard<std::mutex> lk(s->mu);
+  ++s->stats.fetches;
+  finish(s, r, rc, msg);
+  s->cv_done.notify_all();
+}
+
+void worker_loop(cublox_server *s) {
+  cudaSetDevice(s->device);
+  const int max_inflight = s->cfg.max_inflight_ticks > 0 ? s->cfg.max_inflight_ticks : 2;
+  for (;;) {
+    std::vector<Request *> scans, fetches;
+    int nm = 0;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      for (;;) {
+        if (s->stop) return;
+        // heads of the per-map queues
+        nm = s->n_maps.load();
+        int64_t pts = 0;
+        for (int k = 0; k < nm; ++k) {
+          const int mi = (s->rr + k) % nm;
+          MapState &m = *s->maps[mi];
+          if (m.queue.empty()) continue;
+          Request *r = m.queue.front();
+          if (r->kind == kFetch) {
+            fetches.push_back(r);
+            m.queue.pop_front();
+            continue;
+          }
+          const int64_t n = static_cast<int64_t>(r->pts.size() / 3);
+          if (!scans.empty() && (pts + n > s->cfg.max_tick_points ||
+                                 (s->cfg.max_tick_maps > 0 &&
+                                  static_cast<int>(scans.size()) >= s->cfg.max_tick_maps)))
+            continue;
+          scans.push_back(r);
+          m.queue.pop_front();
+          pts += n;
+        }
+        if (nm) s->rr = (s->rr + 1) % nm;
+        if (!scans.empty() || !fetches.empty()) break;
+        s->cv_work.wait(lk);
+      }
+      // bound the launches queued on the device
+      s->cv_inflight.wait(lk, [&] {
+        return s->stop || static_cast<int>(s->inflight.size()) < max_inflight;
+      });
+      if (s->stop) return;
+      const auto now = Clock::now();
+      for (Request *r : scans) r->state = CUBLOX_REQ_RUNNING, r->t_start = now;
+      for (Request *r : fetches) r->state = CUBLOX_REQ_RUNNING, r->t_start = now;
+    }
+    // A map gives a tick one request, its oldest: a scan or a fetch.
+    // scans: admit, concatenate, one batched update, recenters
+    std::vector<char> busy(static_cast<size_t>(nm), 0);
+    std::vector<Request *> ok;
+    for (Request *r : scans) {
+      bool later = false;
+      const int rc = admit(s, r->map, busy, &later);
+      if (later) {
+        defer(s, r);
+        continue;
+      }
+      busy[r->map] = 1;
+      if (rc) {
+        const std::string msg = cublox_last_error();
+        std::lock_guard<std::mutex> lk(s->mu);
+        finish(s, r, rc, msg);
+        s->cv_done.notify_all();
+        continue;
+      }
+      ok.push_back(r);
+    }
+    if (!ok.empty()) {
+      std::vector<cublox_grid *> grids;
+      std::vector<int64_t> offsets(1, 0);
+      std::vector<float> sensors;
+      size_t floats = 0;
+      for (Request *r : ok) floats += r->pts.size();
+      std::vector<float> xyz(floats);
+      size_t at = 0;
+      for (Request *r : ok) {
+        grids.push_back(s->maps[r->map]->g);
+        std::memcpy(xyz.data() + at, r->pts.data(), r->pts.size() * sizeof(float));
+        at += r->pts.size();
+        offsets.push_back(static_cast<int64_t>(at / 3));
+        sensors.insert(sensors.end(), r->sensor, r->sensor + 3);
+      }
+      int rc = cublox_batch_update(s->batch, static_cast<int>(ok.size()), grids.data(),
+                                   xyz.data(), offsets.data(), sensors.data());
+      for (size_t i = 0; !rc && i < ok.size(); ++i) {
+        if (!ok[i]->recenter) continue;
+        int action = 0;
+        rc = cublox_grid_recenter(grids[i], ok[i]->sensor, &action);
+      }
+      cudaEvent_t ev = rc ? nullptr : take_event(s);
+      if (!rc && cudaEventRecord(ev, s->stream) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(CUBLOX_ERR_CUDA, "server: event record failed");
+      }
+      std::lock_guard<std::mutex> lk(s->mu);
+      ++s->stats.ticks;
+      s->stats.scans += static_cast<int64_t>(ok.size());
+      s->stats.points += offsets.back();
+      if (rc) {
+        const std::string msg = cublox_last_error();
+        for (Request *r : ok) finish(s, r, rc, msg);
+        s->cv_done.notify_all();
+      } else {
+        s->inflight.push_back(Tick{ev, ok});
+        s->cv_work.notify_all();  // wakes the completer
+      }
+    }
+    // fetches run after the tick's launches are queued, on the same stream
+    for (Request *r : fetches) run_fetch(s, r);
+  }
+}
+
+void completer_loop(cublox_server *s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    cudaEvent_t ev;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return s->stop || !s->inflight.empty(); });
+      if (s->inflight.empty()) return;  // stop, nothing in flight
+      ev = s->inflight.front().done;
+    }
+    const cudaError_t e = cudaEventSynchronize(ev);
+    std::lock_guard<std::mutex> lk(s->mu);
+    Tick t = std::move(s->inflight.front());
+    s->inflight.pop_front();
+    for (Request *r : t.reqs)
+      finish(s, r, e == cudaSuccess ? CUBLOX_OK : CUBLOX_ERR_CUDA,
+             e == cudaSuccess ? "" : cudaGetErrorString(e));
+    s->free_events.push_back(ev);
+    s->cv_done.notify_all();
+    s->cv_inflight.notify_all();
+  }
+}
+
+Request *find(cublox_server *s, int64_t id) {
+  auto it = s->reqs.find(id);
+  return it == s->reqs.end() ? nullptr : it->second.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+int cublox_server_create(const cublox_server_config *cfg, cublox_server **out) {
+  if (!cfg || !out) return fail(CUBLOX_ERR_INVALID, "server_create: null argument");
+  *out = nullptr;
+  auto s = std::make_unique<cublox_server>();
+  s->cfg = *cfg;
+  s->maps.reserve(kMaxMaps);
+  if (s->cfg.max_tick_points <= 0) s->cfg.max_tick_points = 1 << 20;
+  if (s->cfg.hbm_budget_bytes < scratch_bytes(s.get()))
+    return fail(CUBLOX_ERR_INVALID, "server_create: budget below the tick scratch");
+  cudaGetDevice(&s->device);
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUBLOX_ERR_CUDA, "server_create: stream creation failed");
+  }
+  int rc = cublox_batch_create(s->stream, &s->batch);
+  if (rc) {
+    cudaStreamDestroy(s->stream);
+    return rc;
+  }
+  cublox_batch_set_option(s->batch, CUBLOX_BATCH_OPT_GRAPHS, s->cfg.graphs ? 1 : 0);
+  cublox_server *raw = s.release();
+  raw->worker = std::thread(worker_loop, raw);
+  raw->completer = std::thread(completer_loop, raw);
+  *out = raw;
+  return CUBLOX_OK;
+}
+
+int cublox_server_destroy(cublox_server *s) {
+  if (!s) return CUBLOX_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  s->cv_inflight.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  cudaStreamSynchronize(s->stream);
+  if (s->completer.joinable()) s->completer.join();
+  for (Tick &t : s->inflight) s->free_events.push_back(t.done);
+  for (cudaEvent_t e : s->free_events)
+    if (e) cudaEventDestroy(e);
+  for (auto &m : s->maps)
+    if (m->g) cublox_grid_destroy(m->g);
+  cublox_batch_destroy(s->batch);
+  cudaStreamDestroy(s->stream);
+  delete s;
+  return CUBLOX_OK;
+}
+
+int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float resolution,
+                          int origin_at_center, int has_recenter_threshold,
+                          double recenter_threshold, const float origin[3], float max_range,
+                          const float log_odds[6], int *map_id) {
+  if (!s || !half_map_size || !origin || !map_id)
+    return fail(CUBLOX_ERR_INVALID, "server_add_map: null argument");
+  int64_t vox = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (half_map_size[a] < 0) return fail(CUBLOX_ERR_INVALID, "server_add_map: negative half");
+    vox *= 2 * static_cast<int64_t>(half_map_size[a]) + 1;
+  }
+  if (!(resolution > 0.0f) || vox > 0x7fffffff)
+    return fail(CUBLOX_ERR_INVALID, "server_add_map: bad resolution or size");
+  auto m = std::make_unique<MapState>();
+  for (int a = 0; a < 3; ++a) {
+    m->half[a] = half_map_size[a];
+    m->origin[a] = origin[a];
+  }
+  m->res = resolution;
+  m->ctr = origin_at_center;
+  m->has_thr = has_recenter_threshold;
+  m->thr = recenter_threshold;
+  m->max_range = max_range;
+  if (log_odds) {
+    std::memcpy(m->lo, log_odds, sizeof(m->lo));
+    m->has_lo = true;
+  }
+  m->vox_bytes = 12 * static_cast<size_t>(vox);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (static_cast<int>(s->maps.size()) >= kMaxMaps)
+    return fail(CUBLOX_ERR_INVALID, "server_add_map: at most 4096 maps");
+  *map_id = static_cast<int>(s->maps.size());
+  s->maps.push_back(std::move(m));
+  s->n_maps.store(static_cast<int>(s->maps.size()));
+  return CUBLOX_OK;
+}
+
+static int submit(cublox_server *s, std::unique_ptr<Request> r, int64_t *request_id) {
+  r->t_submit = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (r->map < 0 || r->map >= static_cast<int>(s->maps.size()))
+    return fail(CUBLOX_ERR_INVALID, "server: unknown map id");
+  r->id = s->next_id++;
+  if (request_id) *request_id = r->id;
+  s->maps[r->map]->queue.push_back(r.get());
+  s->reqs[r->id] = std::move(r);
+  ++s->pending;
+  s->cv_work.notify_all();
+  return CUBLOX_OK;
+}
+
+int cublox_server_submit_scan(cublox_server *s, int map_id, const float *xyz, int n,
+                              const float sensor_origin[3], int recenter, int64_t *request_id) {
+  if (!s || !sensor_origin || (n > 0 && !xyz))
+    return fail(CUBLOX_ERR_INVALID, "server_submit_scan: null argument");
+  if (n < 0) return fail(CUBLOX_ERR_INVALID, "server_submit_scan: negative point count");
+  auto r = std::make_unique<Request>();
+  r->kind = kScan;
+  r->map = map_id;
+  r->pts.assign(xyz, xyz + 3 * static_cast<size_t>(n));
+  std::memcpy(r->sensor, sensor_origin, sizeof(r->sensor));
+  r->recenter = recenter;
+  return submit(s, std::move(r), request_id);
+}
+
+int cublox_server_submit_fetch(cublox_server *s, int map_id, const float *centers,
+                               int n_centers, float radius, int filter, int max_results,
+                               int64_t *request_id) {
+  if (!s || (n_centers > 0 && !centers))
+    return fail(CUBLOX_ERR_INVALID, "server_submit_fetch: null argument");
+  if (n_centers < 0) return fail(CUBLOX_ERR_INVALID, "server_submit_fetch: negative count");
+  auto r = std::make_unique<Request>();
+  r->kind = kFetch;
+  r->map = map_id;
+  r->centers.assign(centers, centers + 3 * static_cast<size_t>(n_centers));
+  r->radius = radius;
+  r->filter = filter;
+  r->max_results = max_results;
+  return submit(s, std::move(r), request_id);
+}
+
+int cublox_server_wait(cublox_server *s, int64_t request_id, double timeout_s, int *state) {
+  if (!s) return fail(CUBLOX_ERR_INVALID, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  Request *r = find(s, request_id);
+  if (!r) return fail(CUBLOX_ERR_INVALID, "server_wait: unknown request");
+  auto done = [&] { return r->state == CUBLOX_REQ_DONE || r->state == CUBLOX_REQ_FAILED; };
+  if (timeout_s < 0)
+    s->cv_done.wait(lk, done);
+  else
+    s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
+  if (state) *state = r->state;
+  if (r->state == CUBLOX_REQ_FAILED) return fail(r->error, "server request: " + r->message);
+  return CUBLOX_OK;
+}
+
+int cublox_server_drain(cublox_server *s) {
+  if (!s) return fail(CUBLOX_ERR_INVALID, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  s->cv_done.wait(lk, [&] { return s->pending == 0; });
+  return CUBLOX_OK;
+}
+
+int cublox_server_request_times(cublox_server *s, int64_t request_id, double *queued_ms,
+                                double *latency_ms) {
+  if (!s) return fail(CUBLOX_ERR_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Request *r = find(s, request_id);
+  if (!r) return fail(CUBLOX_ERR_INVALID, "request_times: unknown request");
+  if (r->state != CUBLOX_REQ_DONE && r->state != CUBLOX_REQ_FAILED)
+    return fail(CUBLOX_ERR_INVALID, "request_times: request not finished");
+  if (queued_ms) *queued_ms = ms_between(r->t_submit, r->t_start);
+  if (latency_ms) *latency_ms = ms_between(r->t_submit, r->t_done);
+  return CUBLOX_OK;
+}
+
+int cublox_server_fetch_result(cublox_server *s, int64_t request_id, int64_t *offsets,
+                               float *out_pos, uint8_t *out_state, int64_t capacity,
+                               int64_t *n_samples) {
+  if (!s) return fail(CUBLOX_ERR_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Request *r = find(s, request_id);
+  if (!r || r->kind != kFetch) return fail(CUBLOX_ERR_INVALID, "fetch_result: not a fetch");
+  if (r->state != CUBLOX_REQ_DONE) return fail(CUBLOX_ERR_INVALID, "fetch_result: not done");
+  const int64_t n = static_cast<int64_t>(r->fstate.size());
+  if (n_samples) *n_samples = n;
+  if (offsets) std::copy(r->offsets.begin(), r->offsets.end(), offsets);
+  if (out_pos || out_state) {
+    if (capacity < n) return fail(CUBLOX_ERR_INVALID, "fetch_result: capacity too small");
+    if (out_pos) std::copy(r->fpos.begin(), r->fpos.end(), out_pos);
+    if (out_state) std::copy(r->fstate.begin(), r->fstate.end(), out_state);
+  }
+  return CUBLOX_OK;
+}
+
+int cublox_server_release(cublox_server *s, int64_t request_id) {
+  if (!s) return fail(CUBLOX_ERR_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Request *r = find(s, request_id);
+  if (!r) return fail(CUBLOX_ERR_INVALID, "release: unknown request");
+  if (r->state != CUBLOX_REQ_DONE && r->state != CUBLOX_REQ_FAILED)
+    return fail(CUBLOX_ERR_INVALID, "release: request not finished");
+  s->reqs.erase(request_id);
+  return CUBLOX_OK;
+}
+
+int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int origin_index[3]) {
+  if (!s || !occ_host) return fail(CUBLOX_ERR_INVALID, "server_export: null argument");
+  int rc = cublox_server_drain(s);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (map_id < 0 || map_id >= static_cast<int>(s->maps.size()))
+    return fail(CUBLOX_ERR_INVALID, "server_export: unknown map id");
+  MapState &m = *s->maps[map_id];
+  const size_t vox = m.vox_bytes / 12;
+  if (!m.g) {
+    std::fill(occ_host, occ_host + vox, 0.0f);
+    if (origin_index) {
+      cublox_grid *tmp = nullptr;  // a never-served map: its constructor origin
+      rc = cublox_grid_create(m.half, m.res, m.ctr, m.has_thr, m.thr, m.origin, s->stream, &tmp);
+      if (rc) return rc;
+      cublox_grid_origin(tmp, origin_index, nullptr);
+      cublox_grid_destroy(tmp);
+    }
+    return CUBLOX_OK;
+  }
+  if (m.resident) {
+    rc = cublox_grid_export(m.g, occ_host);
+    if (rc) return rc;
+  } else {
+    std::copy(m.snapshot.begin(), m.snapshot.end(), occ_host);
+  }
+  if (origin_index) cublox_grid_origin(m.g, origin_index, nullptr);
+  return CUBLOX_OK;
+}
+
+int cublox_server_get_stats(cublox_server *s, cublox_server_stats *out) {
+  if (!s || !out) return fail(CUBLOX_ERR_INVALID, "server_stats: null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
+  int resident = 0;
+  for (auto &m : s->maps) resident += m->resident ? 1 : 0;
+  out->resident_maps = resident;
+  return CUBLOX_OK;
+}
+
+}  // extern "C"

@@ -301,6 +301,87 @@ def batching(n_maps: int = 32, n_steps: int = 100, dims=BATCH_DIMS, n_min: int =
                          counts, threshold, seed)
 
 
+SERVE_DIMS = ((200, 200, 40), (350, 350, 75))  # 401x401x81, 701x701x151
+SERVE_SENSORS = ((16, 1024, 15.0), (64, 1024, 22.5), (128, 2048, 22.5))  # beams, azimuths, +-elev
+
+
+@dataclass
+class ServeWorkload:
+    """Requests of many robots arriving over time.
+
+    Robot r has map half-size `halves[r]`, a box scene and a circle
+    trajectory; its scans come from `pool[r][c][j]` = (points, sensor
+    origin), size class c, pose j, reused cyclically along the trajectory.
+    `events` is a time-ordered list of (t_seconds, kind, robot, c, j) with
+    kind "scan" or "fetch" (c, j unused for fetches; `fetch_centres(i)`
+    gives the i-th fetch's centres)."""
+    name: str
+    halves: list
+    resolution: float
+    max_range: float
+    threshold: float | None
+    pool: list
+    events: list
+    fetch_n: int
+    fetch_radius: float
+    seed: int
+
+    @property
+    def n_robots(self) -> int:
+        return len(self.halves)
+
+    def fetch_centres(self, i: int, robot: int, origin) -> np.ndarray:
+        rng = np.random.default_rng((self.seed * 7919 + i) & 0xffffffff)
+        c = np.empty((self.fetch_n, 3), dtype=np.float32)
+        c[:, 0] = origin[0] + rng.uniform(-10.0, 10.0, self.fetch_n)
+        c[:, 1] = origin[1] + rng.uniform(-10.0, 10.0, self.fetch_n)
+        c[:, 2] = rng.uniform(0.0, 3.0, self.fetch_n)
+        return c
+
+
+def serving(n_robots: int = 16, seconds: float = 60.0, scan_rate: float = 400.0,
+            fetch_rate: float = 100.0, dims=SERVE_DIMS, sensors=SERVE_SENSORS,
+            probs=(0.5, 0.35, 0.15), poses: int = 6, max_range: float = 50.0,
+            threshold: float | None = 4.0, fetch_n: int = 256, fetch_radius: float = 1.5,
+            n_boxes: int = 200, seed: int = 3) -> ServeWorkload:
+    """Poisson arrivals of scans (aggregate `scan_rate`/s, point counts by
+    `sensors` with probabilities `probs`) and fetches (`fetch_rate`/s, each
+    `fetch_n` centres around the robot), robots picked uniformly."""
+    rng = np.random.default_rng(seed)
+    halves = [tuple(dims[i]) for i in rng.integers(0, len(dims), size=n_robots)]
+    pool = []
+    for r in range(n_robots):
+        scene = make_scene(seed * 1000 + r, n_boxes, 60.0, keepout=_keepout_circle(15.0, 1.5))
+        traj = circle_trajectory(poses, 15.0, 1.5, 10.0, 1.8)
+        classes = []
+        for c, (beams, az, el) in enumerate(sensors):
+            sen = Sensor(beams, az, -el, el, max_range, 0.02)
+            classes.append([(scan(scene, sen, tuple(traj[j][:3]), traj[j][3],
+                                  seed=(seed * 100 + r) * 1009 + c * 101 + j),
+                             np.asarray(traj[j][:3], dtype=np.float32)) for j in range(poses)])
+        pool.append(classes)
+    events = []
+    for kind, rate in (("scan", scan_rate), ("fetch", fetch_rate)):
+        t = 0.0
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t >= seconds:
+                break
+            events.append((t, kind, int(rng.integers(0, n_robots)),
+                           int(rng.choice(len(sensors), p=probs)), 0))
+    events.sort(key=lambda e: e[0])
+    count = [0] * n_robots
+    out = []
+    for t, kind, r, c, _ in events:
+        if kind == "scan":
+            out.append((t, kind, r, c, count[r] % poses))
+            count[r] += 1
+        else:
+            out.append((t, kind, r, 0, 0))
+    return ServeWorkload(f"serve{n_robots}_" + "|".join(f"{2*a+1}x{2*b+1}x{2*c+1}" for a, b, c in dims),
+                         halves, 0.1, max_range, threshold, pool, out, fetch_n, fetch_radius, seed)
+
+
 def perf_test_cloud(n: int = 500000, r_min: float = 1.5, r_max: float = 8.0, seed: int = 42):
     """Spherical-shell cloud with the shape of the reference's perf test
     (test/test_occupancy_grid_perf.cpp:31-50): radius uniform in

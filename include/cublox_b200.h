@@ -243,6 +243,77 @@ int cublox_batch_synchronize(cublox_batch *b);
 int cublox_batch_last_timing(cublox_batch *b, float *walk_ms, float *fold_ms);
 int cublox_batch_stream(const cublox_batch *b, void **stream);
 
+/* ---- served integration -----------------------------------------------------
+ * No single counterpart in the reference, whose ROS driver serialises one
+ * robot's callbacks on one grid (main.cpp:464-491).  A server keeps many
+ * robots' maps and serves their scan and fetch requests from a worker
+ * thread: requests are copied and queued at submission; each "tick"
+ * integrates the oldest pending scan of every map that has one (up to
+ * max_tick_points) in one batched launch sequence, the next tick being
+ * queued while the previous one still runs.  Maps are admitted to device
+ * memory against hbm_budget_bytes (12 B a voxel plus scratch): when a map's
+ * buffers do not fit, least recently used idle maps are evicted to host
+ * memory and restored bit for bit when next used.  Per map, requests take
+ * effect in submission order, and every result equals that of the same
+ * requests on a lone cublox_grid.                                           */
+typedef struct cublox_server cublox_server;
+
+typedef struct cublox_server_config {
+  uint64_t hbm_budget_bytes; /* device bytes for resident maps + scratch     */
+  int max_tick_points;       /* points per batched launch (0: 1 << 20)       */
+  int max_tick_maps;         /* scans per batched launch (0: no limit)       */
+  int max_inflight_ticks;    /* ticks queued on the device (0: 2)            */
+  int graphs;                /* replay batched launches from CUDA graphs     */
+} cublox_server_config;
+
+typedef struct cublox_server_stats {
+  int64_t ticks, scans, fetches, points; /* served so far                  */
+  int64_t admissions, evictions;         /* maps brought in / sent to host */
+  uint64_t resident_bytes, peak_resident_bytes;
+  int resident_maps;
+} cublox_server_stats;
+
+#define CUBLOX_REQ_QUEUED 0
+#define CUBLOX_REQ_RUNNING 1
+#define CUBLOX_REQ_DONE 2
+#define CUBLOX_REQ_FAILED 3
+
+int cublox_server_create(const cublox_server_config *cfg, cublox_server **out);
+int cublox_server_destroy(cublox_server *s);
+/* A robot's map: the OccupancyGrid constructor's arguments, its max raycast
+ * range and log-odds (setLogOddsParams order; NULL keeps the defaults).     */
+int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float resolution,
+                          int origin_at_center, int has_recenter_threshold,
+                          double recenter_threshold, const float origin[3], float max_range,
+                          const float log_odds[6], int *map_id);
+/* update(cloud, sensor_origin) (OccupancyGrid.cpp:181-238) on the map, then
+ * recenter(sensor_origin) if `recenter`; xyz is x0 y0 z0 x1 ... on the host,
+ * copied before the call returns.                                           */
+int cublox_server_submit_scan(cublox_server *s, int map_id, const float *xyz, int n,
+                              const float sensor_origin[3], int recenter,
+                              int64_t *request_id);
+/* fetchOccupancyAround for each centre (OccupancyGrid.cpp:240-356).         */
+int cublox_server_submit_fetch(cublox_server *s, int map_id, const float *centers,
+                               int n_centers, float radius, int filter, int max_results,
+                               int64_t *request_id);
+/* Wait until the request is done or failed (timeout_s < 0: no limit); state
+ * gets CUBLOX_REQ_*.  A failed request returns its error.                   */
+int cublox_server_wait(cublox_server *s, int64_t request_id, double timeout_s, int *state);
+int cublox_server_drain(cublox_server *s); /* every submitted request done  */
+/* Submission-to-start and submission-to-done times of a finished request. */
+int cublox_server_request_times(cublox_server *s, int64_t request_id, double *queued_ms,
+                                double *latency_ms);
+/* A finished fetch's samples, as cublox_grid_fetch_batch returns them; with
+ * out_pos and out_state NULL only n_samples is set.                         */
+int cublox_server_fetch_result(cublox_server *s, int64_t request_id, int64_t *offsets,
+                               float *out_pos, uint8_t *out_state, int64_t capacity,
+                               int64_t *n_samples);
+int cublox_server_release(cublox_server *s, int64_t request_id); /* forget */
+/* After draining: the map's stored log-odds (dense, reference layout) and
+ * window origin.                                                            */
+int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int origin_index[3]);
+int cublox_server_get_stats(cublox_server *s, cublox_server_stats *out);
+
 /* ---- allocation-free integration ------------------------------------------
  * No counterpart in the reference: it exists for callers that must not
  * allocate device memory while running (a real-time mapping loop that
