@@ -564,6 +564,26 @@ int ensure_capacity(cublox_batch *b, int n_maps, int n_witems, int n_fitems) {
   return CUBLOX_OK;
 }
 
+// Point staging (pinned) and device buffers for `floats` floats, grown
+// geometrically: freeing memory waits for the whole device.
+int reserve_points(cublox_batch *b, size_t floats) {
+  int rc;
+  if (floats > b->points_cap) {
+    floats = std::max(floats, 2 * b->points_cap);
+    cudaStreamSynchronize(b->stream);
+    if ((rc = ensure_dev(reinterpret_cast<void **>(&b->d_points), floats * sizeof(float))))
+      return rc;
+    b->points_cap = floats;
+  }
+  if (floats > b->h_points_cap) {
+    floats = std::max(floats, 2 * b->h_points_cap);
+    if ((rc = ensure_pinned(reinterpret_cast<void **>(&b->h_points), floats * sizeof(float))))
+      return rc;
+    b->h_points_cap = floats;
+  }
+  return CUBLOX_OK;
+}
+
 // The per-step launch sequence (captured into a graph when enabled, so it
 // depends on nothing that changes between steps but the shape and the fold
 // variant).  On failure *what names the call.
@@ -759,17 +779,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   if (cudaEventSynchronize(b->staged) != cudaSuccess) cudaGetLastError();
   if (!on_device && total > 0) {
     const size_t floats = 3 * static_cast<size_t>(total);
-    if (floats > b->points_cap) {
-      cudaStreamSynchronize(b->stream);
-      if ((rc = ensure_dev(reinterpret_cast<void **>(&b->d_points), floats * sizeof(float))))
-        return rc;
-      b->points_cap = floats;
-    }
-    if (floats > b->h_points_cap) {
-      if ((rc = ensure_pinned(reinterpret_cast<void **>(&b->h_points), floats * sizeof(float))))
-        return rc;
-      b->h_points_cap = floats;
-    }
+    if ((rc = reserve_points(b, floats))) return rc;
     if (pa.type != cudaMemoryTypeHost) {
       std::memcpy(b->h_points, base, floats * sizeof(float));
       cudaError_t e = cudaMemcpyAsync(b->d_points, b->h_points, floats * sizeof(float),
@@ -872,6 +882,15 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     }
   }
   return CUBLOX_OK;
+}
+
+int cublox_batch_reserve(cublox_batch *b, int64_t points, int maps) {
+  if (!b || points < 0 || maps < 0) return fail(CUBLOX_ERR_INVALID, "batch_reserve: bad argument");
+  if (cudaEventSynchronize(b->staged) != cudaSuccess) cudaGetLastError();
+  int rc = reserve_points(b, 3 * static_cast<size_t>(points));
+  if (rc) return rc;
+  const int items = maps + static_cast<int>(points / 256) + 1;
+  return ensure_capacity(b, std::max(maps, 1), items, maps * 64 + 1);
 }
 
 int cublox_batch_recenter(cublox_batch *b, int n, cublox_grid *const *grids,

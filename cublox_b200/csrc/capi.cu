@@ -827,9 +827,12 @@ QueryBox plan_query(const cublox_grid *g, const float c[3], float radius) {
 }
 }  // namespace
 
-static int ensure_fq(cublox_grid *g, size_t bytes) {
+// Fetch scratch grows geometrically: a reallocation frees memory, which
+// waits for the whole device.
+static int ensure_fq(cublox_grid *g, cudaStream_t st, size_t bytes) {
   if (bytes <= g->fq_bytes) return CUBLOX_OK;
-  CK(cudaStreamSynchronize(g->stream));
+  bytes = std::max({bytes, 2 * g->fq_bytes, static_cast<size_t>(64) << 10});
+  CK(cudaStreamSynchronize(st));
   cudaFree(g->d_fq);
   g->d_fq = nullptr;
   g->fq_bytes = 0;
@@ -841,9 +844,10 @@ static int ensure_fq(cublox_grid *g, size_t bytes) {
   return CUBLOX_OK;
 }
 
-static int ensure_fout(cublox_grid *g, int64_t n) {
+static int ensure_fout(cublox_grid *g, cudaStream_t st, int64_t n) {
   if (n <= g->fcap) return CUBLOX_OK;
-  CK(cudaStreamSynchronize(g->stream));
+  n = std::max({n, 2 * g->fcap, static_cast<int64_t>(1) << 16});
+  CK(cudaStreamSynchronize(st));
   cudaFree(g->d_fpos);
   cudaFree(g->d_fstate);
   g->d_fpos = nullptr;
@@ -860,10 +864,13 @@ static int ensure_fout(cublox_grid *g, int64_t n) {
 
 // Plans, counts and (if out_pos) writes.  counts_out gets the kept count per
 // query (min(count, cap) as fetchOccupancyAround returns it).
-static int fetch_impl(cublox_grid *g, const float *centers, int nq, float radius,
-                      int filter, int max_results, int64_t *kept, int64_t *offsets,
-                      float *out_pos, uint8_t *out_state, int64_t capacity,
-                      bool write) {
+// On stream st (the grid's own, or a caller's ordered after the grid's
+// work).  With vpos / vstate the outputs are sized there after counting.
+static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int nq,
+                      float radius, int filter, int max_results, int64_t *kept,
+                      int64_t *offsets, float *out_pos, uint8_t *out_state, int64_t capacity,
+                      bool write, std::vector<float> *vpos = nullptr,
+                      std::vector<uint8_t> *vstate = nullptr) {
   if (!g || (nq > 0 && !centers)) return fail(CUBLOX_ERR_INVALID, "fetch: null argument");
   if (filter < -1 || filter > 2) return fail(CUBLOX_ERR_INVALID, "fetch: bad filter");
   if (nq <= 0) {
@@ -882,12 +889,12 @@ static int fetch_impl(cublox_grid *g, const float *centers, int nq, float radius
   auto al = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
   const size_t o_box = al(b_cent), o_r2 = o_box + al(b_box), o_cnt = o_r2 + al(b_r2),
                o_off = o_cnt + al(b_ll), o_lim = o_off + al(b_ll), total = o_lim + al(b_ll);
-  int rc = ensure_fq(g, total);
+  int rc = ensure_fq(g, st, total);
   if (rc) return rc;
   char *base = static_cast<char *>(g->d_fq);
-  CK(cudaMemcpyAsync(base, centers, b_cent, cudaMemcpyHostToDevice, g->stream));
-  CK(cudaMemcpyAsync(base + o_box, boxes.data(), b_box, cudaMemcpyHostToDevice, g->stream));
-  CK(cudaMemcpyAsync(base + o_r2, r2.data(), b_r2, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaMemcpyAsync(base, centers, b_cent, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_box, boxes.data(), b_box, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_r2, r2.data(), b_r2, cudaMemcpyHostToDevice, st));
   FetchParams p{};
   p.occ = g->d_occ;
   p.centers = reinterpret_cast<const float *>(base);
@@ -910,11 +917,11 @@ static int fetch_impl(cublox_grid *g, const float *centers, int nq, float radius
   p.offsets = reinterpret_cast<const long long *>(base + o_off);
   p.limits = reinterpret_cast<const long long *>(base + o_lim);
   p.err = g->d_err;
-  launch_fetch(p, 1, g->stream);
+  launch_fetch(p, 1, st);
   CK_LAUNCH();
   std::vector<long long> cnt(nq), off(nq + 1), lim(nq);
-  CK(cudaMemcpyAsync(cnt.data(), p.counts, b_ll, cudaMemcpyDeviceToHost, g->stream));
-  CK(cudaStreamSynchronize(g->stream));
+  CK(cudaMemcpyAsync(cnt.data(), p.counts, b_ll, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   const long long cap_q = max_results > 0 ? max_results : 500000;  // OccupancyGrid.cpp:292
   off[0] = 0;
   for (int q = 0; q < nq; ++q) {
@@ -926,27 +933,47 @@ static int fetch_impl(cublox_grid *g, const float *centers, int nq, float radius
     for (int q = 0; q <= nq; ++q) offsets[q] = off[q];
   if (!write) return CUBLOX_OK;
   const long long total_s = off[nq];
+  if (vpos && vstate) {
+    vpos->resize(3 * static_cast<size_t>(total_s));
+    vstate->resize(static_cast<size_t>(total_s));
+    out_pos = vpos->data();
+    out_state = vstate->data();
+    capacity = total_s;
+  }
   if (total_s > capacity)
     return fail(CUBLOX_ERR_INVALID, "fetch: output capacity " + std::to_string(capacity) +
                                         " < " + std::to_string(total_s) + " samples");
   if (total_s == 0) return CUBLOX_OK;
-  rc = ensure_fout(g, total_s);
+  rc = ensure_fout(g, st, total_s);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(base + o_off, off.data(), b_ll, cudaMemcpyHostToDevice, g->stream));
-  CK(cudaMemcpyAsync(base + o_lim, lim.data(), b_ll, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaMemcpyAsync(base + o_off, off.data(), b_ll, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_lim, lim.data(), b_ll, cudaMemcpyHostToDevice, st));
   p.out_pos = g->d_fpos;
   p.out_state = g->d_fstate;
-  launch_fetch(p, 2, g->stream);
+  launch_fetch(p, 2, st);
   CK_LAUNCH();
   if (out_pos)
     CK(cudaMemcpyAsync(out_pos, g->d_fpos, sizeof(float) * 3 * static_cast<size_t>(total_s),
-                       cudaMemcpyDeviceToHost, g->stream));
+                       cudaMemcpyDeviceToHost, st));
   if (out_state)
     CK(cudaMemcpyAsync(out_state, g->d_fstate, static_cast<size_t>(total_s),
-                       cudaMemcpyDeviceToHost, g->stream));
-  CK(cudaStreamSynchronize(g->stream));
+                       cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return CUBLOX_OK;
 }
+
+}  // extern "C"
+
+int cublox_b200::detail::fetch_into(cublox_grid *g, cudaStream_t st, const float *centers,
+                                    int nq, float radius, int filter, int max_results,
+                                    std::vector<int64_t> &offsets, std::vector<float> &pos,
+                                    std::vector<uint8_t> &state) {
+  offsets.assign(static_cast<size_t>(nq) + 1, 0);
+  return fetch_impl(g, st, centers, nq, radius, filter, max_results, nullptr, offsets.data(),
+                    nullptr, nullptr, 0, true, &pos, &state);
+}
+
+extern "C" {
 
 int cublox_grid_fetch(cublox_grid *g, const float center[3], float radius,
                       int filter, int max_results, float *out_pos,
@@ -954,15 +981,15 @@ int cublox_grid_fetch(cublox_grid *g, const float center[3], float radius,
   if (n_out) *n_out = 0;
   if (!g || !center) return fail(CUBLOX_ERR_INVALID, "cublox_grid_fetch: null argument");
   int64_t kept = 0;
-  int rc = fetch_impl(g, center, 1, radius, filter, max_results, &kept, nullptr, nullptr,
-                      nullptr, 0, false);
+  int rc = fetch_impl(g, g->stream, center, 1, radius, filter, max_results, &kept, nullptr,
+                      nullptr, nullptr, 0, false);
   if (rc) return rc;
   if (kept > capacity)
     return fail(CUBLOX_ERR_INVALID, "cublox_grid_fetch: capacity " + std::to_string(capacity) +
                                         " < " + std::to_string(kept) + " samples");
   int64_t off[2];
-  rc = fetch_impl(g, center, 1, radius, filter, max_results, nullptr, off, out_pos, out_state,
-                  capacity, true);
+  rc = fetch_impl(g, g->stream, center, 1, radius, filter, max_results, nullptr, off, out_pos,
+                  out_state, capacity, true);
   if (rc) return rc;
   if (n_out) *n_out = off[1];
   return CUBLOX_OK;
@@ -974,16 +1001,16 @@ int cublox_grid_fetch_batch(cublox_grid *g, const float *centers,
                             float *out_pos, uint8_t *out_state,
                             int64_t capacity) {
   if (!out_offsets) return fail(CUBLOX_ERR_INVALID, "fetch_batch: null offsets");
-  return fetch_impl(g, centers, n_centers, radius, filter, max_results, nullptr, out_offsets,
-                    out_pos, out_state, capacity, true);
+  return fetch_impl(g, g ? g->stream : nullptr, centers, n_centers, radius, filter,
+                    max_results, nullptr, out_offsets, out_pos, out_state, capacity, true);
 }
 
 int cublox_grid_fetch_counts(cublox_grid *g, const float *centers,
                              int n_centers, float radius, int filter,
                              int max_results, int64_t *out_counts) {
   if (!out_counts) return fail(CUBLOX_ERR_INVALID, "fetch_counts: null output");
-  return fetch_impl(g, centers, n_centers, radius, filter, max_results, out_counts, nullptr,
-                    nullptr, nullptr, 0, false);
+  return fetch_impl(g, g ? g->stream : nullptr, centers, n_centers, radius, filter,
+                    max_results, out_counts, nullptr, nullptr, nullptr, 0, false);
 }
 
 // ---- queries / state access ---------------------------------------------------

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "exact_fp.cuh"
 #include "kernels.cuh"
@@ -102,5 +103,10 @@ int release_device(cublox_grid *g, float *occ_host);
 // Allocate the voxel buffers again, stored log-odds from occ_host (all
 // unknown if null), counters zero.
 int acquire_device(cublox_grid *g, const float *occ_host);
+// fetch_batch on stream st (ordered after the grid's work by the caller),
+// outputs sized to the samples found.
+int fetch_into(cublox_grid *g, cudaStream_t st, const float *centers, int nq, float radius,
+               int filter, int max_results, std::vector<int64_t> &offsets,
+               std::vector<float> &pos, std::vector<uint8_t> &state);
 }  // namespace detail
 }  // namespace cublox_b200

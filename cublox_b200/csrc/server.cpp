@@ -82,6 +82,12 @@ struct MapState {
   size_t vox_bytes = 0;
   uint64_t last_use = 0;
   std::deque<Request *> queue;  // pending requests, arrival order
+  std::atomic<bool> fetching{false};  // a fetch of this map is in flight
+};
+
+struct FetchJob {
+  Request *r;
+  cudaEvent_t after;  // the map's earlier work, on the server stream
 };
 
 struct Tick {
@@ -104,6 +110,9 @@ struct cublox_server {
   std::vector<std::unique_ptr<MapState>> maps;  // reserved: never reallocated
   std::atomic<int> n_maps{0};                    // maps[0, n_maps) are published
   std::deque<Tick> inflight;
+  std::deque<FetchJob> fetch_jobs;
+  std::condition_variable cv_fetch;  // a fetch job, or stop
+  cudaStream_t fstream = nullptr;    // fetches, ordered after their map's work
   std::vector<cudaEvent_t> free_events;
   int64_t next_id = 1;
   int64_t pending = 0;  // requests not yet done
@@ -111,7 +120,7 @@ struct cublox_server {
   size_t resident_bytes = 0;
   cublox_server_stats stats{};
   bool stop = false;
-  std::thread worker, completer;
+  std::thread worker, completer, fetcher;
   int rr = 0;  // round-robin start of tick formation
 };
 
@@ -161,7 +170,7 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
     int victim = -1;
     for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
       MapState &o = *s->maps[j];
-      if (j == mi || !o.resident || busy[j]) continue;
+      if (j == mi || !o.resident || busy[j] || o.fetching.load()) continue;
       if (victim < 0 || o.last_use < s->maps[victim]->last_use) victim = j;
     }
     if (victim < 0) {
@@ -196,6 +205,7 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
   return CUBLOX_OK;
 }
 
+// Caller holds the lock.
 cudaEvent_t take_event(cublox_server *s) {
   if (!s->free_events.empty()) {
     cudaEvent_t e = s->free_events.back();
@@ -214,33 +224,41 @@ void defer(cublox_server *s, Request *r) {
   s->maps[r->map]->queue.push_front(r);
 }
 
-// One fetch request, synchronously on the worker thread, after the tick's
-// launches are queued (nothing else is waiting to launch).
-void run_fetch(cublox_server *s, Request *r) {
-  std::vector<char> busy(static_cast<size_t>(s->n_maps.load()), 0);
-  bool later = false;
-  int rc = admit(s, r->map, busy, &later);
-  MapState &m = *s->maps[r->map];
-  const int nc = static_cast<int>(r->centers.size() / 3);
-  std::vector<int64_t> counts(static_cast<size_t>(nc));
-  if (!rc)
-    rc = cublox_grid_fetch_counts(m.g, r->centers.data(), nc, r->radius, r->filter,
-                                  r->max_results, counts.data());
-  if (!rc) {
-    int64_t total = 0;
-    for (int64_t c : counts) total += c;
-    r->offsets.assign(static_cast<size_t>(nc) + 1, 0);
-    r->fpos.resize(3 * static_cast<size_t>(total));
-    r->fstate.resize(static_cast<size_t>(total));
-    rc = cublox_grid_fetch_batch(m.g, r->centers.data(), nc, r->radius, r->filter,
-                                 r->max_results, r->offsets.data(), r->fpos.data(),
-                                 r->fstate.data(), total);
+// Fetches run on their own thread and stream: the job waits (on the device)
+// for the work queued on its map before it, and the map takes no new tick
+// until the fetch is done, so later scans cannot overtake it.
+void fetcher_loop(cublox_server *s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    FetchJob job;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_fetch.wait(lk, [&] { return s->stop || !s->fetch_jobs.empty(); });
+      if (s->fetch_jobs.empty()) return;
+      job = s->fetch_jobs.front();
+      s->fetch_jobs.pop_front();
+    }
+    Request *r = job.r;
+    MapState &m = *s->maps[r->map];
+    int rc = CUBLOX_OK;
+    if (cudaStreamWaitEvent(s->fstream, job.after, 0) != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(CUBLOX_ERR_CUDA, "server: fetch ordering failed");
+    }
+    if (!rc)
+      rc = cublox_b200::detail::fetch_into(m.g, s->fstream, r->centers.data(),
+                                           static_cast<int>(r->centers.size() / 3), r->radius,
+                                           r->filter, r->max_results, r->offsets, r->fpos,
+                                           r->fstate);
+    const std::string msg = rc ? cublox_last_error() : "";
+    std::lock_guard<std::mutex> lk(s->mu);
+    ++s->stats.fetches;
+    finish(s, r, rc, msg);
+    s->free_events.push_back(job.after);
+    m.fetching = false;
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
   }
-  const std::string msg = rc ? cublox_last_error() : "";
-  std::lock_guard<std::mutex> lk(s->mu);
-  ++s->stats.fetches;
-  finish(s, r, rc, msg);
-  s->cv_done.notify_all();
 }
 
 void worker_loop(cublox_server *s) {
@@ -259,11 +277,12 @@ void worker_loop(cublox_server *s) {
         for (int k = 0; k < nm; ++k) {
           const int mi = (s->rr + k) % nm;
           MapState &m = *s->maps[mi];
-          if (m.queue.empty()) continue;
+          if (m.queue.empty() || m.fetching) continue;
           Request *r = m.queue.front();
           if (r->kind == kFetch) {
             fetches.push_back(r);
             m.queue.pop_front();
+            m.fetching = true;
             continue;
           }
           const int64_t n = static_cast<int64_t>(r->pts.size() / 3);
@@ -331,7 +350,11 @@ void worker_loop(cublox_server *s) {
         int action = 0;
         rc = cublox_grid_recenter(grids[i], ok[i]->sensor, &action);
       }
-      cudaEvent_t ev = rc ? nullptr : take_event(s);
+      cudaEvent_t ev = nullptr;
+      if (!rc) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        ev = take_event(s);
+      }
       if (!rc && cudaEventRecord(ev, s->stream) != cudaSuccess) {
         cudaGetLastError();
         rc = fail(CUBLOX_ERR_CUDA, "server: event record failed");
@@ -349,8 +372,39 @@ void worker_loop(cublox_server *s) {
         s->cv_work.notify_all();  // wakes the completer
       }
     }
-    // fetches run after the tick's launches are queued, on the same stream
-    for (Request *r : fetches) run_fetch(s, r);
+    // fetches: admitted beside the tick's maps, handed to the fetch thread
+    for (Request *r : fetches) {
+      MapState &m = *s->maps[r->map];
+      bool later = false;
+      int rc = admit(s, r->map, busy, &later);
+      if (later) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->state = CUBLOX_REQ_QUEUED;
+        m.queue.push_front(r);
+        m.fetching = false;
+        continue;
+      }
+      busy[r->map] = 1;
+      cudaEvent_t ev = nullptr;
+      if (!rc) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        ev = take_event(s);
+      }
+      if (!rc && cudaEventRecord(ev, s->stream) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(CUBLOX_ERR_CUDA, "server: event record failed");
+      }
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (rc) {
+        if (ev) s->free_events.push_back(ev);
+        finish(s, r, rc, cublox_last_error());
+        m.fetching = false;
+        s->cv_done.notify_all();
+        continue;
+      }
+      s->fetch_jobs.push_back(FetchJob{r, ev});
+      s->cv_fetch.notify_one();
+    }
   }
 }
 
@@ -396,19 +450,30 @@ int cublox_server_create(const cublox_server_config *cfg, cublox_server **out) {
   if (s->cfg.hbm_budget_bytes < scratch_bytes(s.get()))
     return fail(CUBLOX_ERR_INVALID, "server_create: budget below the tick scratch");
   cudaGetDevice(&s->device);
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->fstream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
+    if (s->stream) cudaStreamDestroy(s->stream);
     return fail(CUBLOX_ERR_CUDA, "server_create: stream creation failed");
   }
   int rc = cublox_batch_create(s->stream, &s->batch);
   if (rc) {
     cudaStreamDestroy(s->stream);
+    cudaStreamDestroy(s->fstream);
     return rc;
   }
   cublox_batch_set_option(s->batch, CUBLOX_BATCH_OPT_GRAPHS, s->cfg.graphs ? 1 : 0);
+  rc = cublox_batch_reserve(s->batch, s->cfg.max_tick_points, 64);
+  if (rc) {
+    cublox_batch_destroy(s->batch);
+    cudaStreamDestroy(s->stream);
+    cudaStreamDestroy(s->fstream);
+    return rc;
+  }
   cublox_server *raw = s.release();
   raw->worker = std::thread(worker_loop, raw);
   raw->completer = std::thread(completer_loop, raw);
+  raw->fetcher = std::thread(fetcher_loop, raw);
   *out = raw;
   return CUBLOX_OK;
 }
@@ -421,7 +486,9 @@ int cublox_server_destroy(cublox_server *s) {
   }
   s->cv_work.notify_all();
   s->cv_inflight.notify_all();
+  s->cv_fetch.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  if (s->fetcher.joinable()) s->fetcher.join();
   cudaStreamSynchronize(s->stream);
   if (s->completer.joinable()) s->completer.join();
   for (Tick &t : s->inflight) s->free_events.push_back(t.done);
@@ -431,6 +498,7 @@ int cublox_server_destroy(cublox_server *s) {
     if (m->g) cublox_grid_destroy(m->g);
   cublox_batch_destroy(s->batch);
   cudaStreamDestroy(s->stream);
+  cudaStreamDestroy(s->fstream);
   delete s;
   return CUBLOX_OK;
 }

@@ -239,6 +239,10 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
  * NULL.                                                                      */
 int cublox_batch_recenter(cublox_batch *b, int n, cublox_grid *const *grids,
                           const float *positions, int *actions);
+/* Size the batch's buffers for updates of up to `points` points over `maps`
+ * grids now, so that later updates of that size allocate nothing (growing
+ * a buffer frees the old one, which waits for the whole device).           */
+int cublox_batch_reserve(cublox_batch *b, int64_t points, int maps);
 int cublox_batch_synchronize(cublox_batch *b);
 int cublox_batch_last_timing(cublox_batch *b, float *walk_ms, float *fold_ms);
 int cublox_batch_stream(const cublox_batch *b, void **stream);
