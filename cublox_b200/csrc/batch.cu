@@ -322,36 +322,39 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
   }
 }
 
-// Walk and fold in one persistent launch.  Items come from one queue: every
-// walk item (ordered by map), then every fold item (ordered by map).  A fold
-// item of map m starts once all of m's walk items have finished, so later
-// maps' walks overlap earlier maps' folds.  A CTA waits only on walk items
-// that running CTAs have already taken, so the wait always ends; it is
-// bounded all the same, and once one wait gives up the launch skips the
-// remaining waits and folds (the map's error word says so).
+// Walk and fold in one persistent launch.  Items come from one queue, in
+// the order the host wrote them: map 0's walk items, map 1's walk items,
+// map 0's fold items, map 2's walk items, map 1's fold items, ... (a fold
+// item is a WalkItem with map = ~map and its FoldItem fields in place).  A
+// fold item of map m starts once all of m's walk items have finished, so
+// CTAs fold map m while others walk map m + 2 and later: the DRAM-bound
+// sweep overlaps the atomic-bound walk.  A CTA waits only on walk items
+// that running CTAs have already taken (they come earlier in the queue), so
+// the wait always ends; it is bounded all the same, and once one wait gives
+// up the launch skips the remaining waits and folds (the map's error word
+// says so).
 template <int S>
 __global__ void __launch_bounds__(1024) batch_fused_kernel(const MapDesc *maps,
-                                                           const WalkItem *witems,
-                                                           const FoldItem *fitems,
+                                                           const WalkItem *items,
+                                                           const FoldItem *unused,
                                                            int *counters, int *done) {
   extern __shared__ uint32_t cube[];
   __shared__ int s_item, s_ok;
-  const int n_w = counters[1];
-  const int n_all = n_w + counters[3];
+  const int n_all = counters[1];
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1);
     __syncthreads();
     const int it = s_item;
     if (it >= n_all) break;
-    if (it < n_w) {
-      const WalkItem item = witems[it];
-      walk_item<S>(maps[item.map], item, cube);  // ends with a barrier
+    const WalkItem raw = items[it];
+    if (raw.map >= 0) {
+      walk_item<S>(maps[raw.map], raw, cube);  // ends with a barrier
       if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(done + item.map, 1);
+        atomicAdd(done + raw.map, 1);
       }
     } else {
-      const FoldItem item = fitems[it - n_w];
+      const FoldItem item{~raw.map, raw.start, raw.count, raw.pad};
       const MapDesc &m = maps[item.map];
       if (threadIdx.x == 0) {
         volatile int *vd = done + item.map;
@@ -764,7 +767,8 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     const int64_t g4 = grids[i]->voxel_num >> 2;
     n_f += static_cast<int>((g4 + kFoldItemGroups - 1) / kFoldItemGroups) + 1;
   }
-  int rc = ensure_capacity(b, n, std::max(n_w, 1), std::max(n_f, 1));
+  // a fused shape queues walk and fold items in one list
+  int rc = ensure_capacity(b, n, std::max(sh.fused ? n_w + n_f : n_w, 1), std::max(n_f, 1));
   if (rc) return rc;
   // points: one concatenated x0 y0 z0 ... buffer, host or device
   cudaPointerAttributes pa;
@@ -795,6 +799,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   // descriptors and items; an empty scan leaves its grid untouched, as
   // cublox_grid_update does (OccupancyGrid.cpp:183-190)
   int w = 0, f = 0, d = 0;
+  std::vector<int> w_end, f_end;  // per map: end of its walk / fold items
   for (int i = 0; i < n; ++i) {
     cublox_grid *g = grids[i];
     const int64_t off = offsets[i] - offsets[0];
@@ -821,7 +826,36 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
       b->h_fitems[f++] = FoldItem{d, s0, std::min(kFoldItemGroups, g4 - s0), s0 == 0 ? 1 : 0};
       if (g4 == 0) break;
     }
+    w_end.push_back(w);
+    f_end.push_back(f);
     ++d;
+  }
+  if (sh.fused) {
+    // walk(0) walk(1) fold(0) walk(2) fold(1) ... fold(d-1), written after
+    // the walk items, then moved to the front
+    const int n_walk = w;
+    auto put_fold = [&](int map) {
+      for (int i = map ? f_end[map - 1] : 0; i < f_end[map]; ++i) {
+        const FoldItem &fi = b->h_fitems[i];
+        b->h_witems[w++] = WalkItem{~fi.map, fi.g4_start, fi.g4_count, fi.tail};
+      }
+    };
+    std::vector<WalkItem> order;
+    order.reserve(static_cast<size_t>(n_walk + f));
+    for (int map = 0; map < d; ++map) {
+      for (int i = map ? w_end[map - 1] : 0; i < w_end[map]; ++i) order.push_back(b->h_witems[i]);
+      if (map >= 1) {
+        w = n_walk;
+        put_fold(map - 1);
+        order.insert(order.end(), b->h_witems + n_walk, b->h_witems + w);
+      }
+    }
+    w = n_walk;
+    put_fold(d - 1);
+    order.insert(order.end(), b->h_witems + n_walk, b->h_witems + w);
+    std::copy(order.begin(), order.end(), b->h_witems);
+    w = static_cast<int>(order.size());
+    f = 0;
   }
   b->h_counters[0] = b->h_counters[2] = b->h_counters[4] = 0;
   b->h_counters[1] = w;
