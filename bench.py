@@ -167,6 +167,20 @@ def cpu_baseline(w, scans, origins, steps, budget_s=12.0):
                       f"{threads} threads, {dt:.1f} s"}
 
 
+def profiled_traffic(n_maps: int):
+    """DRAM bytes of one batched step (walk + fold) from the committed ncu
+    launch list of 8 README-scale maps, scaled to n_maps (traffic grows with
+    the maps: each map's fold sweeps its own counters)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "batch_walk_fold_batch8_readme.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_step:"):
+                    return float(line.split(":")[1]) * n_maps / 8.0
+    except OSError:
+        pass
+    return None
+
+
 def pct(a, q):
     return float(np.percentile(np.asarray(a, dtype=np.float64), q)) if len(a) else None
 
@@ -192,6 +206,8 @@ def run_headline(args, rank, world, dist):
     def new_batch(graphs=True):
         b = C.Batch(stream=stream.cuda_stream)
         b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
+        if args.shape >= 0:
+            b.set_option(C.BATCH_OPT_SHAPE, args.shape)
         gs = []
         for _ in range(K):
             g = b.add_grid(w.half, w.resolution, False, w.threshold)
@@ -537,6 +553,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20, help=">= 3; the launch-shape tuner "
                     "uses the first 16 updates")
     ap.add_argument("--maps", type=int, default=8)
+    ap.add_argument("--shape", type=int, default=-1, help="fix the batch launch shape "
+                    "(default: tuned online during warm-up)")
     ap.add_argument("--impl", choices=["cublox", "reference"], default="cublox")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
@@ -589,7 +607,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "update = batch walk + batch fold",
                      "achieved": h["achieved"], "peak": h["peak"], "unit": "GB/s",
                      "frac": h["achieved"] / h["peak"], "peak_source": h["peak_kind"],
-                     "traffic": None,
+                     "traffic": profiled_traffic(h["K"]),
+                     "traffic_source": "profiles/batch_walk_fold_batch8_readme.md (ncu, 8 maps, "
+                                       "scaled by maps), bytes per step",
                      "algorithmic_bytes": "12 B per point + 8 B per touched voxel (occ read+write); "
                                           "the fold's 4 B/voxel counter sweep is not algorithmic",
                      "atomics_per_s": float(np.mean(h["incs"]) / (np.mean(h["walk_ms"]) / 1e3))},
