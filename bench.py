@@ -191,6 +191,7 @@ def pct(a, q):
 def run_headline(args, rank, world, dist):
     import torch
     import cublox_b200 as C
+    from cublox_b200 import replicas
 
     K = args.maps
     n_steps = args.warmup + args.steps
@@ -245,12 +246,9 @@ def run_headline(args, rank, world, dist):
         dist.barrier()
     step_ms = np.asarray([ev[k][0].elapsed_time(ev[k][1]) for k in range(args.warmup, n_steps)])
     timed_vs = int(steps[args.warmup:].sum())
-    tot_ms = float(step_ms.sum())
-    if dist:
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = world * timed_vs / (tot_ms / 1e3)
+    own_ms = float(step_ms.sum())
+    value = replicas.job_rate(timed_vs, own_ms / 1e3, dist, device="cuda")
+    tot_ms = replicas.max_over_ranks(own_ms, dist, device="cuda")
     shape = b.get_option(C.BATCH_OPT_SHAPE)
     for g in gs:
         assert g.check() == 0, "device error word set"
@@ -293,12 +291,7 @@ def run_headline(args, rank, world, dist):
         if k >= args.warmup:
             wall.append(t1 - t0)
     b.close()
-    e2e_s = float(np.sum(wall))
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * timed_vs / e2e_s
+    e2e = replicas.job_rate(timed_vs, float(np.sum(wall)), dist, device="cuda")
     n_points = int(offsets[0][-1])
 
     peak, peak_kind = _peaks()
