@@ -539,6 +539,246 @@ def run_reference(args):
     }
 
 
+# ---------------------------------------------------------------------------
+# per-config suite (configs 1, 3, 4, 5 beside the headline), both arms
+# ---------------------------------------------------------------------------
+def _time_dev(fn, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _fetch_centres(w, g_origin_f, n, seed):
+    """n centres uniform inside the window (x, y) at z in [0, 3] m."""
+    rng = np.random.default_rng(seed)
+    half = np.asarray(w.half, dtype=np.float64) * w.resolution
+    c = np.empty((n, 3), dtype=np.float32)
+    c[:, 0] = g_origin_f[0] + rng.uniform(-half[0], half[0], n)
+    c[:, 1] = g_origin_f[1] + rng.uniform(-half[1], half[1], n)
+    c[:, 2] = rng.uniform(0.0, 3.0, n)
+    return c
+
+
+def suite_cublox(args):
+    import torch
+    import cublox_b200 as C
+    from cublox_b200 import synth
+    stream = torch.cuda.current_stream()
+    lo = C.yaml_log_odds()
+    out = {}
+    # config 1: plain small
+    w = synth.plain_small(threshold=1.0)
+    pts, s0 = w.scan(0), w.sensor_origin(0)
+    g = C.OccupancyGrid(w.half, w.resolution, False, 1.0, stream=stream.cuda_stream)
+    g.setLogOddsParams(*lo)
+    g.setMaxRaycastRange(w.sensor.max_range)
+    g.enable_timing(True)
+    dev = torch.from_numpy(np.ascontiguousarray(pts.T)).cuda()
+    g.update(dev, s0)
+    ms = [_time_dev(lambda: g.update(dev, s0), stream) for _ in range(30)]
+    cnt = C.OccupancyGrid(w.half, w.resolution, False, None, origin=tuple(float(v) for v in s0))
+    cnt.setMaxRaycastRange(w.sensor.max_range)
+    vs = cnt.reference_steps(pts, s0)
+    cnt.close()
+    oi, of = g.getOriginIndex(), g.getOriginPosition()
+    pos = (np.float32(of) + np.float32(w.extra["recenter_shift"]) * np.float32(w.resolution))
+    g.last_timing()
+    g.recenter(pos)
+    clear_ms = g.last_timing()[2]
+    cleared = g.last_clear()
+    cen = _fetch_centres(w, g.getOriginPosition(), 1000, 0)
+    g.fetch_batch(cen, 1.0)
+    t0 = time.perf_counter()
+    off, fp_, fs = g.fetch_batch(cen, 1.0)
+    fetch_s = time.perf_counter() - t0
+    g.close()
+    out["config1_plain_small"] = {
+        "update_ms_median": float(np.median(ms)), "rays_per_s": pts.shape[0] / (np.median(ms) / 1e3),
+        "voxel_steps_per_s": vs / (np.median(ms) / 1e3),
+        "recenter": {"shift_vox": list(w.extra["recenter_shift"]), "threshold_m": 1.0,
+                     "cleared_voxels": cleared, "clear_ms": clear_ms,
+                     "gb_per_s": 4.0 * cleared / (clear_ms / 1e3) / 1e9},
+        "fetch_1000_centres_r1m": {"us": fetch_s * 1e6, "samples": int(off[-1]),
+                                   "mode": "cublox_grid_fetch_batch (one call, samples to host)"}}
+    # config 5: stress
+    n_scans = args.stress_scans
+    sw = synth.stress(n_scans)
+    scans = [sw.scan(k) for k in range(n_scans)]
+    origins = [sw.sensor_origin(k) for k in range(n_scans)]
+    steps = count_steps(sw.half, sw.resolution, sw.sensor.max_range, sw.threshold, scans, origins)
+    g = C.OccupancyGrid(sw.half, sw.resolution, False, sw.threshold, stream=stream.cuda_stream)
+    g.setLogOddsParams(*lo)
+    g.setMaxRaycastRange(sw.sensor.max_range)
+    g.enable_timing(True)
+    devs = [torch.from_numpy(np.ascontiguousarray(p.T)).cuda() for p in scans]
+    upd, clr, cleared, fetch_occ, fetch_cnt, samples = [], [], [], [], [], []
+    for k in range(n_scans):
+        def step():
+            g.update(devs[k], origins[k])
+            g.recenter(origins[k])
+        t = _time_dev(step, stream)
+        tm = g.last_timing()
+        if k >= 1:
+            upd.append(t)
+            if tm[2] >= 0:
+                clr.append(tm[2])
+                cleared.append(g.last_clear())
+        if k >= n_scans - 3:
+            cen = _fetch_centres(sw, g.getOriginPosition(), sw.fetch_centres, k)
+            t0 = time.perf_counter()
+            cts = g.fetch_counts(cen, sw.fetch_radius)
+            fetch_cnt.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            off, _, _ = g.fetch_batch(cen, sw.fetch_radius, C.VoxelState.OCCUPIED)
+            fetch_occ.append(time.perf_counter() - t0)
+            samples.append((int(cts.sum()), int(off[-1])))
+    g.close()
+    out["config5_stress"] = {
+        "scans": n_scans - 1, "voxel_steps_per_s": float(steps[1:].sum() / (np.sum(upd) / 1e3)),
+        "update_recenter_ms_p50": pct(upd, 50), "update_recenter_ms_p99": pct(upd, 99),
+        "recenter_gb_per_s": float(4.0 * np.sum(cleared) / (np.sum(clr) / 1e3) / 1e9) if clr else None,
+        "recenters": len(clr),
+        "fetch_10000_centres_r2m": {"all_states_counts_only_ms": float(np.mean(fetch_cnt) * 1e3),
+                                    "occupied_samples_to_host_ms": float(np.mean(fetch_occ) * 1e3),
+                                    "samples_all_states": samples[-1][0],
+                                    "samples_occupied": samples[-1][1]}}
+    return out
+
+
+def suite_reference(args):
+    import oracle as O
+    import cublox_b200 as C
+    from cublox_b200 import synth
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref was not built"}
+    lo = C.yaml_log_odds()
+
+    def ref(half, res, thr, mr):
+        r = O.RefGrid(half, res, False, thr)
+        r.set_log_odds(*lo)
+        r.set_max_range(mr)
+        return r
+
+    def soa(p):
+        return tuple(np.ascontiguousarray(p[:, a]) for a in range(3))
+
+    out = {}
+    w = synth.plain_small(threshold=1.0)
+    pts, s0 = w.scan(0), w.sensor_origin(0)
+    r = ref(w.half, w.resolution, 1.0, w.sensor.max_range)
+    x = soa(pts)
+    r.update(None, s0, xyz=x)
+    ms = []
+    for _ in range(30):
+        t0 = time.perf_counter()
+        r.update(None, s0, xyz=x)
+        ms.append((time.perf_counter() - t0) * 1e3)
+    cnt = C.OccupancyGrid(w.half, w.resolution, False, None, origin=tuple(float(v) for v in s0))
+    cnt.setMaxRaycastRange(w.sensor.max_range)
+    vs = cnt.reference_steps(pts, s0)
+    cnt.close()
+    oi, of = r.origin()
+    pos = (np.float32(of) + np.float32(w.extra["recenter_shift"]) * np.float32(w.resolution))
+    t0 = time.perf_counter()
+    r.recenter(pos)
+    rec_ms = (time.perf_counter() - t0) * 1e3
+    cen = _fetch_centres(w, r.origin()[1], 1000, 0)
+    t0 = time.perf_counter()
+    ns = sum(r.fetch(c, 1.0)[0].shape[0] for c in cen)
+    fetch_s = time.perf_counter() - t0
+    r.close()
+    out["config1_plain_small"] = {
+        "update_ms_median": float(np.median(ms)), "rays_per_s": pts.shape[0] / (np.median(ms) / 1e3),
+        "voxel_steps_per_s": vs / (np.median(ms) / 1e3), "recenter_wall_ms": rec_ms,
+        "fetch_1000_centres_r1m": {"us": fetch_s * 1e6, "samples": ns,
+                                   "mode": "fetchOccupancyAround once per centre"}}
+    # config 3: 32 maps, one update call per map per step
+    bw = synth.batching(n_steps=args.batch_steps + 3)
+    refs = [ref(bw.halves[m], bw.resolution, bw.threshold, bw.max_range) for m in range(bw.n_maps)]
+    data = [bw.step(k) for k in range(args.batch_steps + 3)]
+    steps = np.zeros((len(data), bw.n_maps), np.int64)
+    for m in range(bw.n_maps):
+        steps[:, m] = count_steps(bw.halves[m], bw.resolution, bw.max_range, bw.threshold,
+                                  [d[0][m] for d in data], [d[1][m] for d in data])
+    wall = []
+    for k, (clouds, sensors) in enumerate(data):
+        xs = [soa(c) for c in clouds]
+        t0 = time.perf_counter()
+        for m in range(bw.n_maps):
+            refs[m].update(None, sensors[m], xyz=xs[m])
+            refs[m].recenter(sensors[m])
+        if k >= 3:
+            wall.append(time.perf_counter() - t0)
+    for rr in refs:
+        rr.close()
+    out["config3_batching"] = {"maps": bw.n_maps, "steps": len(wall),
+                               "voxel_steps_per_s": float(steps[3:].sum() / np.sum(wall)),
+                               "step_ms_p50": pct(wall, 50) * 1e3, "mode": "32 sequential update calls"}
+    # config 4: the same request stream served one scan at a time
+    sw = synth.serving(seconds=args.serve_seconds)
+    refs = [ref(sw.halves[rb], sw.resolution, sw.threshold, sw.max_range) for rb in range(sw.n_robots)]
+    svc = {0: [], 1: [], 2: []}
+    busy = 0.0
+    n_done = 0
+    t_start = time.perf_counter()
+    for t, kind, rb, c, j in sw.events:
+        if kind != "scan":
+            continue
+        p, o = sw.pool[rb][c][j]
+        xs = soa(p)
+        t0 = time.perf_counter()
+        refs[rb].update(None, o, xyz=xs)
+        refs[rb].recenter(o)
+        dt = time.perf_counter() - t0
+        busy += dt
+        svc[c].append(dt * 1e3)
+        n_done += 1
+        if time.perf_counter() - t_start > args.serve_seconds:
+            break
+    for rr in refs:
+        rr.close()
+    out["config4_serving"] = {
+        "mode": "each scan's update + recenter alone, back to back (no batching, no overlap)",
+        "scans": n_done, "max_scans_per_s": n_done / busy,
+        "offered_scans_per_s": 400.0,
+        **{f"service_ms_{k}": {"p50": pct(v, 50), "p99": pct(v, 99)}
+           for k, v in zip(("16384", "65536", "262144"), (svc[0], svc[1], svc[2]))}}
+    # config 5: stress
+    n_scans = args.stress_scans
+    sw5 = synth.stress(n_scans)
+    scans = [sw5.scan(k) for k in range(n_scans)]
+    origins = [sw5.sensor_origin(k) for k in range(n_scans)]
+    steps5 = count_steps(sw5.half, sw5.resolution, sw5.sensor.max_range, sw5.threshold, scans, origins)
+    r = ref(sw5.half, sw5.resolution, sw5.threshold, sw5.sensor.max_range)
+    upd, rec = [], []
+    for k in range(n_scans):
+        xs = soa(scans[k])
+        t0 = time.perf_counter()
+        r.update(None, origins[k], xyz=xs)
+        t1 = time.perf_counter()
+        r.recenter(origins[k])
+        t2 = time.perf_counter()
+        if k >= 1:
+            upd.append(t2 - t0)
+            rec.append(t2 - t1)
+    cen = _fetch_centres(sw5, r.origin()[1], 100, n_scans)
+    t0 = time.perf_counter()
+    for c in cen:
+        r.fetch(c, sw5.fetch_radius, state_filter=2)
+    f_occ = (time.perf_counter() - t0) / len(cen)
+    r.close()
+    out["config5_stress"] = {
+        "scans": n_scans - 1, "voxel_steps_per_s": float(steps5[1:].sum() / np.sum(upd)),
+        "update_recenter_ms_p50": pct(upd, 50) * 1e3, "recenter_wall_ms_p50": pct(rec, 50) * 1e3,
+        "fetch_10000_centres_r2m_occupied_ms": f_occ * 1e4 * 1e3,
+        "fetch_note": "100 centres timed one call each, scaled to 10,000"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -553,6 +793,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--only-headline", action="store_true")
+    ap.add_argument("--suite", choices=["headline", "configs"], default="headline",
+                    help="configs: the per-config numbers (1, 3, 4, 5) instead of the headline")
+    ap.add_argument("--stress-scans", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -562,6 +805,11 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
     torch.cuda.set_device(local)
+    if args.suite == "configs":
+        if rank == 0:
+            fn = suite_reference if args.impl == "reference" else suite_cublox
+            print(json.dumps({"impl": args.impl, "suite": "configs", **fn(args)}), flush=True)
+        return 0
     if args.impl == "reference":
         if rank != 0:
             return 0

@@ -115,6 +115,7 @@ def lib():
             "cublox_grid_last_stats": ([G, ctypes.POINTER(ScanStats)], ctypes.c_int),
             "cublox_grid_check": ([G, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
             "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
+            "cublox_grid_last_clear": ([G, i64], ctypes.c_int),
             "cublox_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
             "cublox_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
             "cublox_batch_add_grid": ([ctypes.c_void_p, i, ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -462,6 +463,12 @@ class OccupancyGrid:
         ms = (ctypes.c_float * 3)()
         _check(lib().cublox_grid_last_timing(self._h, ms), "last_timing")
         return tuple(ms)
+
+    def last_clear(self) -> int:
+        """Voxels the last recenter cleared."""
+        v = ctypes.c_int64()
+        _check(lib().cublox_grid_last_clear(self._h, ctypes.byref(v)), "last_clear")
+        return v.value
 
     def reference_steps(self, cloud, sensor_origin) -> int:
         """The reference's work units for one scan (DDA iterations + endpoint)."""

@@ -554,14 +554,23 @@ int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
     e = cudaMemcpy(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->voxel_num),
                    cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "release_device", __LINE__);
-  void **bufs[] = {reinterpret_cast<void **>(&g->d_occ),   reinterpret_cast<void **>(&g->d_cnt),
-                   reinterpret_cast<void **>(&g->d_hit),   reinterpret_cast<void **>(&g->d_cloud),
-                   reinterpret_cast<void **>(&g->d_bins),  reinterpret_cast<void **>(&g->d_work),
-                   reinterpret_cast<void **>(&g->d_segs),  reinterpret_cast<void **>(&g->d_rays),
-                   reinterpret_cast<void **>(&g->d_hist),  reinterpret_cast<void **>(&g->d_sorted),
-                   reinterpret_cast<void **>(&g->d_fq),    reinterpret_cast<void **>(&g->d_fpos),
-                   reinterpret_cast<void **>(&g->d_fstate), reinterpret_cast<void **>(&g->d_qout),
-                   reinterpret_cast<void **>(&g->d_qin)};
+  cudaFree(g->d_occ);
+  cudaFree(g->d_cnt);
+  cudaFree(g->d_hit);
+  g->d_occ = nullptr;
+  g->d_cnt = g->d_hit = nullptr;
+  return release_scratch(g);
+}
+
+int cublox_b200::detail::release_scratch(cublox_grid *g) {
+  const cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "release_scratch", __LINE__);
+  void **bufs[] = {reinterpret_cast<void **>(&g->d_cloud), reinterpret_cast<void **>(&g->d_bins),
+                   reinterpret_cast<void **>(&g->d_work),  reinterpret_cast<void **>(&g->d_segs),
+                   reinterpret_cast<void **>(&g->d_rays),  reinterpret_cast<void **>(&g->d_hist),
+                   reinterpret_cast<void **>(&g->d_sorted), reinterpret_cast<void **>(&g->d_fq),
+                   reinterpret_cast<void **>(&g->d_fpos),  reinterpret_cast<void **>(&g->d_fstate),
+                   reinterpret_cast<void **>(&g->d_qout),  reinterpret_cast<void **>(&g->d_qin)};
   for (void **b : bufs) {
     cudaFree(*b);
     *b = nullptr;
@@ -693,6 +702,7 @@ static int normalize_slice(int x, int half) {
 int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
   if (action) *action = 0;
   if (!g || !pos) return fail(CUBLOX_ERR_INVALID, "cublox_grid_recenter: null argument");
+  g->last_cleared = 0;
   if (!g->has_thr || g->voxel_num <= 0) return CUBLOX_OK;  // OccupancyGrid.cpp:142-145
   const float dx = pos[0] - g->origin_f[0];
   const float dy = pos[1] - g->origin_f[1];
@@ -712,6 +722,7 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
   if (max_shift >= max_map) {  // kernels.cu:338-347, :652-662
     CK(cudaMemsetAsync(g->d_occ, 0, sizeof(float) * static_cast<size_t>(g->voxel_num),
                        g->stream));
+    g->last_cleared = g->voxel_num;
     set_origin(g, no);
     if (action) *action = 2;
     return CUBLOX_OK;
@@ -742,6 +753,15 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
         for (int k = 0; k < n; ++k) mark(a, normalize_slice(-half + k, half));
     }
     if (a == 2) any_z = true;
+  }
+  {
+    int64_t keep = 1;  // voxels on no marked slab
+    for (int a = 0; a < 3; ++a) {
+      int marked = 0;
+      for (int w = 0; w < g->mask_words[a]; ++w) marked += __builtin_popcount(m[a][w]);
+      keep *= g->map[a] - marked;
+    }
+    g->last_cleared = g->voxel_num - keep;
   }
   const size_t mb = masks.size() * sizeof(uint32_t);
   // Pinned staging, reused once the previous recenter's copy has run, so the
@@ -831,7 +851,7 @@ QueryBox plan_query(const cublox_grid *g, const float c[3], float radius) {
 // waits for the whole device.
 static int ensure_fq(cublox_grid *g, cudaStream_t st, size_t bytes) {
   if (bytes <= g->fq_bytes) return CUBLOX_OK;
-  bytes = std::max({bytes, 2 * g->fq_bytes, static_cast<size_t>(64) << 10});
+  bytes = std::max({bytes, 2 * g->fq_bytes, static_cast<size_t>(4) << 10});
   CK(cudaStreamSynchronize(st));
   cudaFree(g->d_fq);
   g->d_fq = nullptr;
@@ -846,7 +866,7 @@ static int ensure_fq(cublox_grid *g, cudaStream_t st, size_t bytes) {
 
 static int ensure_fout(cublox_grid *g, cudaStream_t st, int64_t n) {
   if (n <= g->fcap) return CUBLOX_OK;
-  n = std::max({n, 2 * g->fcap, static_cast<int64_t>(1) << 16});
+  n = std::max({n, 2 * g->fcap, static_cast<int64_t>(1) << 12});
   CK(cudaStreamSynchronize(st));
   cudaFree(g->d_fpos);
   cudaFree(g->d_fstate);
@@ -1190,6 +1210,12 @@ int cublox_grid_enable_timing(cublox_grid *g, int enable) {
       if (!g->tev[i]) CK(cudaEventCreate(&g->tev[i]));
   g->timing_on = enable != 0;
   for (int i = 0; i < 3; ++i) g->tev_used[i] = false;
+  return CUBLOX_OK;
+}
+
+int cublox_grid_last_clear(const cublox_grid *g, int64_t *voxels) {
+  if (!g || !voxels) return fail(CUBLOX_ERR_INVALID, "null argument");
+  *voxels = g->last_cleared;
   return CUBLOX_OK;
 }
 

@@ -47,6 +47,7 @@ struct cublox_grid {
   float *d_sorted = nullptr;
   int bin_cap = 0;
   bool timing_on = false;
+  int64_t last_cleared = 0;  // voxels the last recenter cleared
   cudaEvent_t tev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool tev_used[3] = {false, false, false};
 
@@ -100,6 +101,10 @@ size_t device_bytes(const cublox_grid *g);
 // keeps its host state (window origin, parameters) and must not be used
 // until acquire_device.
 int release_device(cublox_grid *g, float *occ_host);
+// Free the per-call scratch a grid has grown (cloud staging, walk plans,
+// fetch and query buffers); the voxel buffers stay.  Syncs the grid's
+// stream.
+int release_scratch(cublox_grid *g);
 // Allocate the voxel buffers again, stored log-odds from occ_host (all
 // unknown if null), counters zero.
 int acquire_device(cublox_grid *g, const float *occ_host);

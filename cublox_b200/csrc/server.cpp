@@ -166,6 +166,13 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
   if (need + scratch_bytes(s) > s->cfg.hbm_budget_bytes)
     return fail(CUBLOX_ERR_NOMEM, "server: map needs " + std::to_string(need) +
                                       " bytes, more than the budget allows");
+  // First give back the per-call scratch (fetch outputs) of idle maps.
+  if (used_bytes(s) + need > s->cfg.hbm_budget_bytes)
+    for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
+      MapState &o = *s->maps[j];
+      if (j != mi && o.resident && !busy[j] && !o.fetching.load())
+        cublox_b200::detail::release_scratch(o.g);
+    }
   while (used_bytes(s) + need > s->cfg.hbm_budget_bytes) {
     int victim = -1;
     for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
@@ -250,6 +257,10 @@ void fetcher_loop(cublox_server *s) {
                                            static_cast<int>(r->centers.size() / 3), r->radius,
                                            r->filter, r->max_results, r->offsets, r->fpos,
                                            r->fstate);
+    // Outputs stay on the host: give the device scratch back when the
+    // budget is exceeded.
+    if (!rc && used_bytes(s) > s->cfg.hbm_budget_bytes)
+      rc = cublox_b200::detail::release_scratch(m.g);
     const std::string msg = rc ? cublox_last_error() : "";
     std::lock_guard<std::mutex> lk(s->mu);
     ++s->stats.fetches;

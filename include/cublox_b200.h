@@ -186,6 +186,10 @@ int cublox_grid_count_scan(cublox_grid *g, const float *xyz, int n,
  * (-1 where none ran since the last read); timing is opt-in.               */
 int cublox_grid_enable_timing(cublox_grid *g, int enable);
 int cublox_grid_last_timing(cublox_grid *g, float ms[3]);
+/* Voxels the last recenter cleared (its slab union, or every voxel on a
+ * full reset; 0 when it did nothing).  Accounting only, no reference
+ * counterpart.                                                              */
+int cublox_grid_last_clear(const cublox_grid *g, int64_t *voxels);
 
 /* Work units of one scan as the reference counts them: per ray, the DDA
  * iterations of rayCastUpdateKernel's loop that did not break, plus one for
@@ -255,7 +259,9 @@ int cublox_batch_stream(const cublox_batch *b, void **stream);
  * integrates the oldest pending scan of every map that has one (up to
  * max_tick_points) in one batched launch sequence, the next tick being
  * queued while the previous one still runs.  Maps are admitted to device
- * memory against hbm_budget_bytes (12 B a voxel plus scratch): when a map's
+ * memory against hbm_budget_bytes (12 B a voxel, the tick's point buffers
+ * and the fetch buffers maps keep between requests; a fetch in flight may
+ * exceed it by its own output buffers until it ends): when a map's
  * buffers do not fit, least recently used idle maps are evicted to host
  * memory and restored bit for bit when next used.  Per map, requests take
  * effect in submission order, and every result equals that of the same

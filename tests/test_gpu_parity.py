@@ -122,6 +122,10 @@ def test_recenter_plain_small(small, thr, expect_action):
     assert a == ro["action"] == expect_action
     assert g.getOriginIndex() == o.origin()[0]
     assert same_bits(g.export(), o.occ())
+    # cleared-voxel accounting: the union of the oracle's slabs
+    maps = [2 * h + 1 for h in w.half]
+    keep = np.prod([maps[k] - len(set(ro["slabs"][k].tolist())) for k in range(3)])
+    assert g.last_clear() == (int(np.prod(maps)) - keep if a == 1 else 0)
     r = ref_grid(w.half, w.resolution, thr=thr, max_range=w.sensor.max_range)
     if r is not None:
         r.update(pts, s)
@@ -143,6 +147,7 @@ def test_recenter_full_reset_and_mode1(small):
     far = np.float32([500.0, 0.0, 1.8])  # shift >= largest map side
     assert g.recenter(far) == 2 == o.recenter(far)["action"]
     assert not g.export().any()
+    assert g.last_clear() == g.voxel_num
     assert g.getOriginIndex() == o.origin()[0]
     # exiting-slabs-only mode clears a subset of compat mode's slabs
     g2, o2 = pair(w.half, w.resolution, thr=0.5, max_range=w.sensor.max_range)

@@ -115,7 +115,9 @@ def test_tight_budget_evicts_and_restores_bit_for_bit():
     check_alone(w, s, ids, out)
     st = s.stats()
     assert st["evictions"] > 0 and st["admissions"] > w.n_robots
-    assert st["peak_resident_bytes"] <= scratch + big + 12 * voxels(DIMS[0]) + (64 << 10)
+    # maps and tick scratch stay within the budget; a fetch in flight may add
+    # its own output buffers until it ends
+    assert st["peak_resident_bytes"] <= scratch + big + 12 * voxels(DIMS[0]) + (1 << 20)
     s.close()
 
 
