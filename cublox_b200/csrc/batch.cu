@@ -302,6 +302,92 @@ __global__ void __launch_bounds__(1024, kMinCtas) batch_walk_kernel(const MapDes
   }
 }
 
+// Persistent walk without per-item barriers.  A CTA adopts one map at a
+// time (starting at blockIdx % maps, then the next map with rays left): it
+// zeroes its cube around that map's sensor, and its warps take 32-ray items
+// of the map from the map's own counter until none is left; only then does
+// the CTA synchronise, flush the cube and move on.  A warp waits only for
+// its own longest ray, never for the rest of the CTA.  counters[1] holds the
+// number of maps; next[m] is map m's item counter (zero at launch).
+template <int S>
+__global__ void __launch_bounds__(1024) batch_walk_wq_kernel(const MapDesc *maps,
+                                                             const WalkItem *unused,
+                                                             int *counters, int *next) {
+  extern __shared__ uint32_t cube[];
+  constexpr int kCube = S * S * S;
+  __shared__ int s_map;
+  const int n_maps = counters[1];
+  const unsigned lane = threadIdx.x & 31u;
+  int m = n_maps > 0 ? static_cast<int>(blockIdx.x) % n_maps : 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int found = -1;
+      for (int k = 0; k < n_maps; ++k) {
+        const int mm = (m + k) % n_maps;
+        if (*reinterpret_cast<volatile int *>(next + mm) * 32 < maps[mm].ray.n) {
+          found = mm;
+          break;
+        }
+      }
+      s_map = found;
+    }
+    __syncthreads();
+    m = s_map;
+    if (m < 0) break;
+    const MapDesc &md = maps[m];
+    const RayParams p = md.ray;
+    const int clo[3] = {md.clo[0], md.clo[1], md.clo[2]};
+    for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
+      reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    uint32_t rays = 0, incs = 0, hits = 0;
+    for (;;) {
+      int it = 0;
+      if (lane == 0) it = atomicAdd(next + m, 1);
+      it = __shfl_sync(0xffffffffu, it, 0);
+      if (it * 32 >= p.n) break;
+      const int i = it * 32 + static_cast<int>(lane);
+      if (i >= p.n) continue;
+      const size_t k = static_cast<size_t>(i) * p.stride;
+      RayWalk w;
+      if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;
+      ++rays;
+      const RayEnd re = ray_end_of<S>(p, w, clo);
+      FarWalk f;
+      if (!walk_near<S>(p, cube, clo, w, f, incs)) walk_far(p, f, incs);
+      apply_end<S>(p, cube, re, incs, hits);
+    }
+    __syncthreads();
+    if constexpr (S > 0) {
+      for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
+        const uint32_t v = cube[q];
+        if (!v) continue;
+        const int g[3] = {clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S};
+        const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
+                       (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
+                          p.map[2] +
+                      (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+        atomicAdd(p.cnt + h, v);
+      }
+    }
+    if (p.stats) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        rays += __shfl_down_sync(0xffffffffu, rays, off);
+        incs += __shfl_down_sync(0xffffffffu, incs, off);
+        hits += __shfl_down_sync(0xffffffffu, hits, off);
+      }
+      if (lane == 0) {
+        atomicAdd(p.stats + 0, static_cast<unsigned long long>(rays));
+        atomicAdd(p.stats + 1, static_cast<unsigned long long>(incs));
+        atomicAdd(p.stats + 2, static_cast<unsigned long long>(hits));
+      }
+    }
+    __syncthreads();
+    m = (m + 1) % n_maps;
+  }
+}
+
 // Persistent fold: CTAs take fold items from counters[2].  U: counter
 // groups in flight per thread (fewer registers, more resident warps).
 template <int U>
@@ -320,6 +406,151 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
     const MapDesc &m = maps[item.map];
     add_touched(m, fold_item<U, false>(m, item));
   }
+}
+
+// ---- fold with the counter sweep on the bulk-copy engine ------------------
+// The counters of a fold item stream into shared memory in 16 KB chunks by
+// cp.async.bulk (no registers, no per-thread latency), kBulkStages chunks in
+// flight, each completing an mbarrier; the threads only look at the chunk in
+// shared memory and spend their loads on the stored values of the groups that
+// have a set counter (all of a thread's such loads of a chunk are issued
+// together).  Every wait is bounded: one that gives up flags
+// kErrWaitTimeout, skips the rest of the launch's folds and still waits
+// (bounded) for the copies it issued before the CTA exits.
+constexpr int kBulkGroups = 1024;  // 16-byte counter groups per chunk (16 KB)
+constexpr int kBulkStages = 4;
+constexpr size_t kBulkSmem = sizeof(uint4) * kBulkGroups * kBulkStages;
+constexpr int kBulkSpin = 1 << 24;  // try_wait polls before a wait gives up
+constexpr int kBulkItemGroups = 1 << 16;  // groups per fold item of this kernel
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Issue one chunk: arm the barrier with its byte count, start the copy.
+__device__ __forceinline__ void bulk_chunk(void *dst, const void *src, uint32_t bytes,
+                                           uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (int i = 0; i < kBulkSpin; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(256) batch_fold_bulk_kernel(const MapDesc *maps,
+                                                              const FoldItem *items,
+                                                              int *counters) {
+  extern __shared__ __align__(128) uint4 stage[];  // kBulkStages x kBulkGroups
+  __shared__ __align__(8) uint64_t bar[kBulkStages];
+  __shared__ int s_item, s_ok;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kBulkStages; ++i) mbar_init(&bar[i]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t parity = 0;   // bit i: phase parity of stage i's next completion
+  uint32_t pending = 0;  // bit i: a copy into stage i is in flight
+  const int n_items = counters[3];
+  for (;;) {
+    if (threadIdx.x == 0)
+      s_item = *reinterpret_cast<volatile int *>(counters + 4) ? n_items
+                                                               : atomicAdd(&counters[2], 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const FoldItem item = items[it];
+    const MapDesc &m = maps[item.map];
+    const FoldView v = fold_view(m);
+    const uint4 *src = reinterpret_cast<const uint4 *>(v.cnt) + item.g4_start;
+    uint4 *c4 = reinterpret_cast<uint4 *>(v.cnt) + item.g4_start;
+    float4 *o4 = reinterpret_cast<float4 *>(v.occ) + item.g4_start;
+    const int n_chunks = (item.g4_count + kBulkGroups - 1) / kBulkGroups;
+    auto chunk_groups = [&](int c) { return min(kBulkGroups, item.g4_count - c * kBulkGroups); };
+    if (threadIdx.x == 0)
+      for (int c = 0; c < min(kBulkStages, n_chunks); ++c) {
+        bulk_chunk(stage + c * kBulkGroups, src + c * kBulkGroups, 16u * chunk_groups(c), &bar[c]);
+        pending |= 1u << c;
+      }
+    uint32_t touched = 0;
+    bool ok = true;
+    for (int c = 0; c < n_chunks; ++c) {
+      const int st = c % kBulkStages;
+      // every thread waits for the chunk; the vote keeps the decision uniform
+      const bool got = __syncthreads_and(mbar_wait(&bar[st], (parity >> st) & 1u));
+      if (!got) {
+        ok = false;
+        break;
+      }
+      parity ^= 1u << st;
+      if (threadIdx.x == 0) pending &= ~(1u << st);
+      const uint4 *sc = stage + st * kBulkGroups;
+      const int ng = chunk_groups(c);
+      const int base = c * kBulkGroups;
+      uint4 cv[4];
+      float4 ov[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = threadIdx.x + u * 256;
+        cv[u] = q < ng ? sc[q] : make_uint4(0u, 0u, 0u, 0u);
+        ov[u] = any_set(cv[u]) ? o4[base + q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (!any_set(cv[u])) continue;
+        const int g = base + threadIdx.x + u * 256;
+        const int h = (item.g4_start + g) << 2;
+        if (cv[u].x) { ov[u].x = fold_counter(v, h + 0, cv[u].x, ov[u].x); ++touched; }
+        if (cv[u].y) { ov[u].y = fold_counter(v, h + 1, cv[u].y, ov[u].y); ++touched; }
+        if (cv[u].z) { ov[u].z = fold_counter(v, h + 2, cv[u].z, ov[u].z); ++touched; }
+        if (cv[u].w) { ov[u].w = fold_counter(v, h + 3, cv[u].w, ov[u].w); ++touched; }
+        o4[g] = ov[u];
+        c4[g] = make_uint4(0u, 0u, 0u, 0u);
+      }
+      __syncthreads();  // stage st is free again
+      if (threadIdx.x == 0 && c + kBulkStages < n_chunks) {
+        const int nc = c + kBulkStages;
+        bulk_chunk(stage + st * kBulkGroups, src + nc * kBulkGroups, 16u * chunk_groups(nc),
+                   &bar[st]);
+        pending |= 1u << st;
+      }
+    }
+    if (threadIdx.x == 0) s_ok = ok;
+    __syncthreads();
+    if (!s_ok) {
+      if (threadIdx.x == 0) {
+        atomicOr(m.ray.err, kErrWaitTimeout);
+        atomicExch(counters + 4, 1);
+      }
+      break;
+    }
+    if (item.tail) touched += fold_tail(v);
+    add_touched(m, touched);
+  }
+  // copies still in flight (only after a wait gave up): bounded wait
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kBulkStages; ++i)
+      if (pending & (1u << i)) mbar_wait(&bar[i], (parity >> i) & 1u);
 }
 
 // Walk and fold in one persistent launch.  Items come from one queue, in
@@ -387,11 +618,13 @@ struct Shape {
   int block;     // walk (or fused) CTA size
   int fused;     // 1: one launch, folds overlap later maps' walks
   int min_ctas;  // 2: registers capped for two CTAs per SM (cube <= 16)
+  int wq;        // 1: warps take 32-ray items of a CTA's current map (no item barriers)
 };
 
-const Shape kShapes[] = {{32, 512, 512, 0, 1},    {32, 1024, 1024, 0, 1}, {16, 512, 256, 0, 1},
-                         {16, 1024, 1024, 0, 2},  {16, 2048, 1024, 0, 2}, {0, 1024, 1024, 0, 2},
-                         {32, 1024, 1024, 1, 1},  {16, 512, 512, 1, 1}};
+const Shape kShapes[] = {{32, 512, 512, 0, 1, 0},  {32, 1024, 1024, 0, 1, 0},
+                         {32, 0, 512, 0, 1, 1},    {32, 0, 1024, 0, 1, 1},
+                         {16, 0, 512, 0, 1, 1},    {16, 1024, 1024, 0, 2, 0},
+                         {32, 1024, 1024, 1, 1, 0}, {16, 512, 512, 1, 1, 0}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 int sm_count_batch() {
@@ -408,6 +641,7 @@ int sm_count_batch() {
 template <int S>
 const void *shape_kernel_s(const Shape &sh) {
   if (sh.fused) return reinterpret_cast<const void *>(batch_fused_kernel<S>);
+  if (sh.wq) return reinterpret_cast<const void *>(batch_walk_wq_kernel<S>);
   if constexpr (S < 32) {
     if (sh.min_ctas >= 2) return reinterpret_cast<const void *>(batch_walk_kernel<S, 2>);
   }
@@ -462,8 +696,28 @@ cudaError_t launch_walk(const MapDesc *maps, const WalkItem *witems, const FoldI
   const Shape &sh = kShapes[shape];
   void *walk_args[] = {&maps, &witems, &counters};
   void *fused_args[] = {&maps, &witems, &fitems, &counters, &done};
+  void *wq_args[] = {&maps, &witems, &counters, &done};
   return cudaLaunchKernel(shape_kernel(sh), dim3(shape_grid(shape)), dim3(sh.block),
-                          sh.fused ? fused_args : walk_args, shape_smem(sh), s);
+                          sh.fused ? fused_args : (sh.wq ? wq_args : walk_args), shape_smem(sh),
+                          s);
+}
+
+int bulk_fold_ctas() {
+  static int grid = 0;
+  if (grid == 0) {
+    const int smem = static_cast<int>(kBulkSmem);
+    if (cudaFuncSetAttribute(batch_fold_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess)
+      cudaGetLastError();
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_fold_bulk_kernel, 256,
+                                                      kBulkSmem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    grid = sm_count_batch() * (per_sm < 1 ? 1 : per_sm);
+  }
+  return grid;
 }
 
 cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counters,
@@ -472,6 +726,9 @@ cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counte
   switch (variant) {
     case 1: batch_fold_kernel<4><<<grid, block, 0, s>>>(maps, fitems, counters); break;
     case 2: batch_fold_kernel<1><<<grid, block, 0, s>>>(maps, fitems, counters); break;
+    case 3:
+      batch_fold_bulk_kernel<<<bulk_fold_ctas(), block, kBulkSmem, s>>>(maps, fitems, counters);
+      break;
     default: batch_fold_kernel<2><<<grid, block, 0, s>>>(maps, fitems, counters); break;
   }
   return cudaGetLastError();
@@ -600,7 +857,7 @@ cudaError_t enqueue_step(cublox_batch *b, int shape, const char **what) {
       (e = cudaMemsetAsync(b->d_counters + 2, 0, sizeof(int), b->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->d_counters + 4, 0, sizeof(int), b->stream)) != cudaSuccess)
     return e;
-  if (sh.fused &&
+  if ((sh.fused || sh.wq) &&
       (e = cudaMemsetAsync(b->d_done, 0, sizeof(int) * b->maps_cap, b->stream)) != cudaSuccess)
     return e;
   *what = "timing event";
@@ -655,6 +912,7 @@ int cublox_batch_create(void *stream, cublox_batch **out) {
   }
   for (int i = 0; i < 4; ++i) cudaEventCreate(&b->ev[i]);
   for (int i = 0; i < kNumShapes; ++i) shape_grid(i);
+  bulk_fold_ctas();
   *out = b;
   return CUBLOX_OK;
 }
@@ -714,7 +972,7 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
       b->timed = value != 0;
       return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD:
-      if (value < 0 || value > 2) break;
+      if (value < 0 || value > 3) break;
       b->fold_variant = value;
       drop_graph(b);
       return CUBLOX_OK;
@@ -759,13 +1017,15 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   const int active_shape = tuning ? shape : b->shape;
   const Shape &sh = kShapes[active_shape];
   const int rays_per_item = shape_rays(active_shape, total);
+  const int fold_groups_per_item =
+      (!sh.fused && b->fold_variant == 3) ? kBulkItemGroups : kFoldItemGroups;
   // work items
   int n_w = 0, n_f = 0;
   for (int i = 0; i < n; ++i) {
     const int64_t c = offsets[i + 1] - offsets[i];
     n_w += static_cast<int>((c + rays_per_item - 1) / rays_per_item);
     const int64_t g4 = grids[i]->voxel_num >> 2;
-    n_f += static_cast<int>((g4 + kFoldItemGroups - 1) / kFoldItemGroups) + 1;
+    n_f += static_cast<int>((g4 + fold_groups_per_item - 1) / fold_groups_per_item) + 1;
   }
   // a fused shape queues walk and fold items in one list
   int rc = ensure_capacity(b, n, std::max(sh.fused ? n_w + n_f : n_w, 1), std::max(n_f, 1));
@@ -822,8 +1082,8 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     for (int s0 = 0; s0 < c; s0 += rays_per_item, ++md.n_walk)
       b->h_witems[w++] = WalkItem{d, s0, std::min(rays_per_item, c - s0), 0};
     const int g4 = g->voxel_num >> 2;
-    for (int s0 = 0; s0 < g4 || (s0 == 0 && g4 == 0); s0 += kFoldItemGroups) {
-      b->h_fitems[f++] = FoldItem{d, s0, std::min(kFoldItemGroups, g4 - s0), s0 == 0 ? 1 : 0};
+    for (int s0 = 0; s0 < g4 || (s0 == 0 && g4 == 0); s0 += fold_groups_per_item) {
+      b->h_fitems[f++] = FoldItem{d, s0, std::min(fold_groups_per_item, g4 - s0), s0 == 0 ? 1 : 0};
       if (g4 == 0) break;
     }
     w_end.push_back(w);
@@ -858,7 +1118,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     f = 0;
   }
   b->h_counters[0] = b->h_counters[2] = b->h_counters[4] = 0;
-  b->h_counters[1] = w;
+  b->h_counters[1] = sh.wq ? d : w;  // the warp-queue walk reads maps, not items
   b->h_counters[3] = f;
   cudaError_t e;
   if ((e = cudaMemcpyAsync(b->d_maps, b->h_maps, sizeof(MapDesc) * d, cudaMemcpyHostToDevice,

@@ -223,7 +223,9 @@ typedef struct cublox_batch cublox_batch;
 #define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
 #define CUBLOX_BATCH_OPT_FOLD 6       /* fold sweep: counter groups in flight
                                          per thread, 0: two (default),
-                                         1: four, 2: one                    */
+                                         1: four, 2: one; 3: counters
+                                         streamed to shared memory by the
+                                         bulk-copy engine                   */
 
 int cublox_batch_create(void *stream, cublox_batch **out);
 int cublox_batch_destroy(cublox_batch *b);
