@@ -190,21 +190,42 @@ __device__ __forceinline__ bool far_step(FarWalk &f, int map_a) {
   return f.out[A]-- == 0;
 }
 
-// Far phase to the end of the ray's loop.
+// Far phase to the end of the ray's loop.  The endpoint test costs nothing
+// per step: every step lowers one e counter by one, so the walk can stand on
+// the endpoint only after exactly e0 + e1 + e2 steps (an axis it never steps
+// on must already match), and not at all once a counter went negative.
+// Until then only the step limit and the window exit end the loop.
 __device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, uint32_t &incs) {
-  for (;;) {
-    if (f.left <= 0 || (f.e[0] | f.e[1] | f.e[2]) == 0) return;
-    atomicAdd(p.cnt + f.h, 1u);
-    ++incs;
-    --f.left;
-    bool gone;
-    if (f.tM[0] < f.tM[1]) {
-      gone = f.tM[0] < f.tM[2] ? far_step<0>(f, p.map[0]) : far_step<2>(f, p.map[2]);
-    } else {
-      gone = f.tM[1] < f.tM[2] ? far_step<1>(f, p.map[1]) : far_step<2>(f, p.map[2]);
-    }
-    if (gone) return;
+  const int left0 = f.left;
+  bool reachable = true;
+  int to_end = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (f.dh[a] == 0 ? f.e[a] != 0 : f.e[a] < 0) reachable = false;
+    to_end += f.e[a];
   }
+  int n = reachable ? min(f.left, to_end) : f.left;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (; n > 0; --n) {
+      atomicAdd(p.cnt + f.h, 1u);
+      --f.left;
+      bool gone;
+      if (f.tM[0] < f.tM[1]) {
+        gone = f.tM[0] < f.tM[2] ? far_step<0>(f, p.map[0]) : far_step<2>(f, p.map[2]);
+      } else {
+        gone = f.tM[1] < f.tM[2] ? far_step<1>(f, p.map[1]) : far_step<2>(f, p.map[2]);
+      }
+      if (gone) {
+        incs += static_cast<uint32_t>(left0 - f.left);
+        return;
+      }
+    }
+    // At the step limit, or where the endpoint could be: stop if on it,
+    // else (a counter overshot) only the step limit and the window remain.
+    if (f.left <= 0 || (f.e[0] | f.e[1] | f.e[2]) == 0) break;
+    n = f.left;
+  }
+  incs += static_cast<uint32_t>(left0 - f.left);
 }
 
 // One walk item: zero the cube, walk the item's rays (one thread per ray),
