@@ -316,6 +316,7 @@ def run_plain(args, hw):
     import torch
     import cublox_b200 as C
     w = hw["w"]
+    assert torch.cuda.current_stream().cuda_stream != 0, "run_headline sets a dedicated stream"
     scans = [hw["scans"][k][0] for k in range(len(hw["scans"]))]
     origins = [hw["origins"][k][0] for k in range(len(hw["origins"]))]
     steps = hw["steps"][:, 0]
@@ -375,6 +376,7 @@ def run_batching(args):
                                   [data[k][0][m] for k in range(n_steps)],
                                   [data[k][1][m] for k in range(n_steps)])
     stream = torch.cuda.current_stream()
+    assert stream.cuda_stream != 0, "run_headline sets a dedicated stream"
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     b = C.Batch(stream=stream.cuda_stream)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
@@ -567,7 +569,10 @@ def suite_cublox(args):
     import torch
     import cublox_b200 as C
     from cublox_b200 import synth
-    stream = torch.cuda.current_stream()
+    # a dedicated stream shared by the grids and the timing events (handle 0
+    # would make every grid create its own stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     lo = C.yaml_log_odds()
     out = {}
     # config 1: plain small
@@ -637,11 +642,34 @@ def suite_cublox(args):
             fetch_occ.append(time.perf_counter() - t0)
             samples.append((int(cts.sum()), int(off[-1])))
     g.close()
+    # the batched/graph form of the same drive: a batch of one map
+    b = C.Batch(stream=stream.cuda_stream)
+    b.set_option(C.BATCH_OPT_GRAPHS, 1)
+    gb = b.add_grid(sw.half, sw.resolution, False, sw.threshold)
+    gb.setLogOddsParams(*lo)
+    gb.setMaxRaycastRange(sw.sensor.max_range)
+    aos = [torch.from_numpy(p).cuda() for p in scans]
+    bt = []
+    for k in range(n_scans):
+        so = origins[k].reshape(1, 3)
+        off = np.array([0, scans[k].shape[0]], np.int64)
+
+        def bstep():
+            b.update([gb], aos[k], so, offsets=off)
+            b.recenter([gb], so)
+        t = _time_dev(bstep, stream)
+        if k >= 1:
+            bt.append(t)
+    b.close()
     out["config5_stress"] = {
         "scans": n_scans - 1, "voxel_steps_per_s": float(steps[1:].sum() / (np.sum(upd) / 1e3)),
         "update_recenter_ms_p50": pct(upd, 50), "update_recenter_ms_p99": pct(upd, 99),
         "recenter_gb_per_s": float(4.0 * np.sum(cleared) / (np.sum(clr) / 1e3) / 1e9) if clr else None,
         "recenters": len(clr),
+        "batched_graph_form": {"voxel_steps_per_s": float(steps[1:].sum() / (np.sum(bt) / 1e3)),
+                               "update_recenter_ms_p50": pct(bt, 50),
+                               "note": "same drive through a one-map Batch with CUDA-graph "
+                                       "replay (the first updates tune the launch shape)"},
         "fetch_10000_centres_r2m": {"all_states_counts_only_ms": float(np.mean(fetch_cnt) * 1e3),
                                     "occupied_samples_to_host_ms": float(np.mean(fetch_occ) * 1e3),
                                     "samples_all_states": samples[-1][0],

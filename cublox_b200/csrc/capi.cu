@@ -783,8 +783,28 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
   for (int a = 0; a < 3; ++a) cp.map[a] = g->map[a];
   cp.any_z = any_z ? 1 : 0;
   tmark(g, 2, 0);
-  launch_clear(cp, g->stream);
-  CK_LAUNCH();
+  // A marked x slab is one contiguous run of ny*nz values, and neighbouring
+  // marked slabs are neighbouring runs: clear each maximal run with one
+  // memset at copy bandwidth; the kernel then clears only y and z slabs.
+  const size_t slab = static_cast<size_t>(g->map[1]) * g->map[2];
+  for (int x = 0; x < g->map[0];) {
+    if (!((m[0][x >> 5] >> (x & 31)) & 1u)) {
+      ++x;
+      continue;
+    }
+    int e = x;
+    while (e < g->map[0] && ((m[0][e >> 5] >> (e & 31)) & 1u)) ++e;
+    CK(cudaMemsetAsync(g->d_occ + static_cast<size_t>(x) * slab, 0,
+                       sizeof(float) * slab * static_cast<size_t>(e - x), g->stream));
+    x = e;
+  }
+  cp.x_done = 1;
+  bool any_y = false;
+  for (int w = 0; w < g->mask_words[1]; ++w) any_y = any_y || m[1][w] != 0u;
+  if (any_y || any_z) {
+    launch_clear(cp, g->stream);
+    CK_LAUNCH();
+  }
   tmark(g, 2, 1);
   set_origin(g, no);
   if (action) *action = 1;

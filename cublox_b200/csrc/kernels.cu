@@ -182,6 +182,7 @@ __global__ void __launch_bounds__(256) clear_kernel(const ClearParams p) {
   for (int lx = blockIdx.x; lx < nx; lx += gridDim.x) {
     float *base = p.occ + static_cast<size_t>(lx) * ny * nz;
     if ((p.xmask[lx >> 5] >> (lx & 31)) & 1u) {
+      if (p.x_done) continue;
       const int n = ny * nz;
       for (int i = threadIdx.x; i < n; i += blockDim.x) base[i] = 0.0f;
       continue;

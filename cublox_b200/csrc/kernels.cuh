@@ -56,6 +56,7 @@ struct ClearParams {
   const uint32_t *xmask, *ymask, *zmask;  // bit per local slab slot
   int map[3];
   int any_z;
+  int x_done;  // marked x slabs are already cleared (contiguous memsets)
 };
 
 struct FetchParams {
