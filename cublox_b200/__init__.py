@@ -116,6 +116,7 @@ def lib():
             "cublox_grid_check": ([G, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
             "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
             "cublox_grid_last_clear": ([G, i64], ctypes.c_int),
+            "cublox_grid_update_pose": ([G, f, ctypes.c_int, ctypes.c_int, f, f], ctypes.c_int),
             "cublox_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
             "cublox_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
             "cublox_batch_add_grid": ([ctypes.c_void_p, i, ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -477,6 +478,21 @@ class OccupancyGrid:
         _check(lib().cublox_grid_reference_steps(self._h, _fp(p), p.shape[0], _f3(sensor_origin),
                                                  ctypes.byref(v)), "reference_steps")
         return v.value
+
+    def update_pose(self, cloud_sensor, rotation, translation):
+        """update() from a sensor-frame (N, 3) cloud (host array or CUDA
+        tensor) and the sensor pose (3x3 rotation, translation): the
+        reference driver's range filter and transform run on the device."""
+        R = np.ascontiguousarray(np.asarray(rotation, dtype=np.float32).reshape(9))
+        t = np.ascontiguousarray(np.asarray(translation, dtype=np.float32).reshape(3))
+        dp = _dev_ptr(cloud_sensor)
+        if dp is not None:
+            n = int(cloud_sensor.shape[0])
+            ptr = ctypes.cast(dp, ctypes.POINTER(ctypes.c_float))
+        else:
+            p = np.ascontiguousarray(np.asarray(cloud_sensor, dtype=np.float32).reshape(-1, 3))
+            n, ptr = p.shape[0], _fp(p)
+        _check(lib().cublox_grid_update_pose(self._h, ptr, LAYOUT_AOS, n, _fp(R), _fp(t)), "update_pose")
 
     def update_ptr(self, ptr: int, n: int, sensor_origin, layout: int = LAYOUT_SOA):
         """update() from a raw pointer (device, pinned or pageable host)."""

@@ -110,6 +110,8 @@ static void free_all(cublox_grid *g) {
   if (g->h_masks) cudaFreeHost(g->h_masks);
   if (g->mask_ev) cudaEventDestroy(g->mask_ev);
   cudaFree(g->d_cloud);
+  cudaFree(g->d_world);
+  cudaFree(g->d_kept);
   cudaFree(g->d_bins);
   cudaFree(g->d_work);
   cudaFree(g->d_segs);
@@ -541,7 +543,7 @@ RayParams cublox_b200::detail::ray_params(const cublox_grid *g, const float *x,
 
 size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
   size_t b = 12 * static_cast<size_t>(g->d_occ ? g->voxel_num : 0);
-  b += sizeof(float) * 3 * static_cast<size_t>(g->cloud_cap);
+  b += sizeof(float) * 3 * (static_cast<size_t>(g->cloud_cap) + static_cast<size_t>(g->world_cap));
   b += g->fq_bytes + 13 * static_cast<size_t>(g->fcap) + 13 * static_cast<size_t>(g->qcap);
   b += static_cast<size_t>(g->split_cap) * (16 * split_seg_bytes() + 64);  // 16 segments a ray
   b += static_cast<size_t>(g->bin_cap) * 16;
@@ -565,6 +567,9 @@ int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
 int cublox_b200::detail::release_scratch(cublox_grid *g) {
   const cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "release_scratch", __LINE__);
+  cudaFree(g->d_world);
+  g->d_world = nullptr;
+  g->world_cap = 0;
   void **bufs[] = {reinterpret_cast<void **>(&g->d_cloud), reinterpret_cast<void **>(&g->d_bins),
                    reinterpret_cast<void **>(&g->d_work),  reinterpret_cast<void **>(&g->d_segs),
                    reinterpret_cast<void **>(&g->d_rays),  reinterpret_cast<void **>(&g->d_hist),
@@ -683,6 +688,83 @@ int cublox_grid_update_xyz(cublox_grid *g, const float *xyz, int layout,
   if (layout != CUBLOX_LAYOUT_SOA && layout != CUBLOX_LAYOUT_AOS)
     return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_xyz: unknown layout");
   return update_impl(g, nullptr, nullptr, nullptr, xyz, layout, n, sensor_origin);
+}
+
+// update() from a sensor-frame cloud and the sensor pose: the reference
+// driver's buildCloudInOdomFrame (src/main.cpp:640-693) on the device, then
+// update(world_cloud, t) (OccupancyGrid.cpp:181-238).
+int cublox_grid_update_pose(cublox_grid *g, const float *xyz, int layout, int n,
+                            const float rotation[9], const float translation[3]) {
+  if (!g || !rotation || !translation || (n > 0 && !xyz))
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_pose: null argument");
+  if (layout != CUBLOX_LAYOUT_SOA && layout != CUBLOX_LAYOUT_AOS)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_pose: unknown layout");
+  if (g->voxel_num <= 0 || n <= 0) return CUBLOX_OK;  // the driver skips empty clouds
+  int rc;
+  // the raw cloud on the device, in its own layout
+  const float *src = xyz;
+  if (mem_kind(xyz) != 2) {
+    if ((rc = ensure_cloud(g, n))) return rc;
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(n);
+    if (mem_kind(xyz) == 1) {
+      CK(cudaMemcpyAsync(g->d_cloud, xyz, bytes, cudaMemcpyHostToDevice, g->stream));
+      if (!g->stage_ev[0]) CK(cudaEventCreateWithFlags(&g->stage_ev[0], cudaEventDisableTiming));
+      CK(cudaEventRecord(g->stage_ev[0], g->stream));
+      CK(cudaEventSynchronize(g->stage_ev[0]));  // the caller may reuse its buffer
+    } else {
+      if ((rc = ensure_stage(g, n))) return rc;
+      const int s = g->stage_idx;
+      g->stage_idx ^= 1;
+      CK(cudaEventSynchronize(g->stage_ev[s]));
+      std::memcpy(g->h_stage[s], xyz, bytes);
+      CK(cudaMemcpyAsync(g->d_cloud, g->h_stage[s], bytes, cudaMemcpyHostToDevice, g->stream));
+      CK(cudaEventRecord(g->stage_ev[s], g->stream));
+    }
+    src = g->d_cloud;
+  }
+  if (n > g->world_cap) {
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(g->d_world);
+    g->d_world = nullptr;
+    g->world_cap = 0;
+    if (cudaMalloc(&g->d_world, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update_pose: world buffer allocation failed");
+    }
+    g->world_cap = n;
+  }
+  IngestParams ip{};
+  ip.xyz = src;
+  ip.layout = layout;
+  ip.n = n;
+  for (int i = 0; i < 9; ++i) ip.R[i] = rotation[i];
+  for (int a = 0; a < 3; ++a) ip.t[a] = translation[a];
+  ip.max_r2 = fmul(g->max_range, g->max_range);  // main.cpp:451
+  ip.dst = g->d_world;
+  ip.count = nullptr;
+  if (g->first_run) {
+    // The driver calls update() only if a point survives its filters; the
+    // first call snaps the window, so the first run needs the count.
+    if (!g->d_kept) {
+      if (cudaMalloc(&g->d_kept, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update_pose: allocation failed");
+      }
+    }
+    CK(cudaMemsetAsync(g->d_kept, 0, sizeof(int), g->stream));
+    ip.count = g->d_kept;
+  }
+  launch_ingest(ip, g->stream);
+  CK_LAUNCH();
+  if (g->first_run) {
+    int kept = 0;
+    CK(cudaMemcpyAsync(&kept, g->d_kept, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    if (kept == 0) return CUBLOX_OK;
+  }
+  snap_first_run(g, translation);
+  return integrate(g, g->d_world, g->d_world + n, g->d_world + 2 * static_cast<size_t>(n), n, 1,
+                   translation);
 }
 
 // ---- recenter ---------------------------------------------------------------

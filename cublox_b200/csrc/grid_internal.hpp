@@ -67,6 +67,9 @@ struct cublox_grid {
 
   float *d_cloud = nullptr;  // SoA [x|y|z]
   int cloud_cap = 0;
+  float *d_world = nullptr;  // update_pose: world-frame SoA points
+  int world_cap = 0;
+  int *d_kept = nullptr;     // update_pose: points kept by the range filter
   float *h_stage[2] = {nullptr, nullptr};
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   int stage_cap = 0;

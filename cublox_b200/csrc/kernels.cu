@@ -329,6 +329,38 @@ __global__ void gather_soa_kernel(const float *xyz, int layout, int n,
   }
 }
 
+// One point of buildCloudInOdomFrame (main.cpp:666-684), in its FP32 order
+// on x86-64 without FMA: squaredNorm as (x*x + y*y) + z*z, the isometry as
+// ((r0*x + r1*y) + r2*z) + t per row.
+__global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
+       i += gridDim.x * blockDim.x) {
+    float x, y, z;
+    if (p.layout == 1) {
+      x = p.xyz[3 * static_cast<size_t>(i)];
+      y = p.xyz[3 * static_cast<size_t>(i) + 1];
+      z = p.xyz[3 * static_cast<size_t>(i) + 2];
+    } else {
+      x = p.xyz[i];
+      y = p.xyz[p.n + i];
+      z = p.xyz[2 * static_cast<size_t>(p.n) + i];
+    }
+    float w[3];
+    bool keep = isfinite(x) && isfinite(y) && isfinite(z);
+    if (keep) keep = !(fadd(fadd(fmul(x, x), fmul(y, y)), fmul(z, z)) > p.max_r2);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float *r = p.R + 3 * a;
+      w[a] = keep ? fadd(fadd(fadd(fmul(r[0], x), fmul(r[1], y)), fmul(r[2], z)), p.t[a])
+                  : __int_as_float(0x7fc00000);
+    }
+    p.dst[i] = w[0];
+    p.dst[p.n + i] = w[1];
+    p.dst[2 * static_cast<size_t>(p.n) + i] = w[2];
+    if (p.count && keep) atomicAdd(p.count, 1);
+  }
+}
+
 int sm_count() {
   static int n = 0;
   if (n == 0) {
@@ -406,6 +438,11 @@ void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
   if (n <= 0) return;
   int grid = (n + 255) / 256;
   gather_soa_kernel<<<grid, 256, 0, s>>>(xyz, layout, n, dst);
+}
+
+void launch_ingest(const IngestParams &p, cudaStream_t s) {
+  if (p.n <= 0) return;
+  ingest_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(p);
 }
 
 }  // namespace cublox_b200

@@ -127,6 +127,21 @@ void launch_apply(const ApplyParams &p, cudaStream_t s);
 void launch_clear(const ClearParams &p, cudaStream_t s);
 void launch_fetch(const FetchParams &p, int pass, cudaStream_t s);
 void launch_query(const QueryParams &p, cudaStream_t s);
+// Sensor-frame cloud -> world-frame SoA (the reference driver's
+// buildCloudInOdomFrame, src/main.cpp:640-693): non-finite points and points
+// farther than sqrt(max_r2) from the sensor are dropped (written as NaN, which
+// the walk drops), the rest become R p + t.
+struct IngestParams {
+  const float *xyz;  // n points, layout 0 SoA / 1 AoS
+  int layout, n;
+  float R[9];        // row-major rotation, sensor -> world
+  float t[3];        // sensor origin in the world
+  float max_r2;      // squared range filter
+  float *dst;        // SoA world points
+  int *count;        // if not null: += points kept
+};
+void launch_ingest(const IngestParams &p, cudaStream_t s);
+
 void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
                        cudaStream_t s);
 

@@ -193,6 +193,22 @@ class OccupancyGrid : public Grid {
     refreshOrigin();
   }
 
+  // update() from a sensor-frame cloud and the sensor pose (rotation
+  // row-major, translation = sensor origin): the range filter and transform
+  // the reference's driver applies before update() (src/main.cpp:640-693),
+  // done on the device.  Not in the reference class.
+  void updateFromSensor(const PointCloud &cloud_sensor, const float rotation_row_major[9],
+                        const Eigen::Vector3f &translation) {
+    if (!g_ || cloud_sensor.rows() <= 0) return;
+    const float t[3] = {translation.x(), translation.y(), translation.z()};
+    detail::ok(cublox_grid_update_pose(g_, cloud_sensor.col(0).data(), CUBLOX_LAYOUT_SOA,
+                                       static_cast<int>(cloud_sensor.rows()), rotation_row_major,
+                                       t),
+               "updateFromSensor");
+    if (!async_) detail::ok(cublox_grid_synchronize(g_), "updateFromSensor");
+    refreshOrigin();
+  }
+
   // Sliding-window recenter (OccupancyGrid.cpp:141-179).
   void recenter(const Eigen::Vector3f &pos) {
     if (!g_) return;

@@ -108,6 +108,15 @@ int cublox_grid_update(cublox_grid *g, const float *x, const float *y,
 /* Same, with the cloud in one buffer of the given layout.                   */
 int cublox_grid_update_xyz(cublox_grid *g, const float *xyz, int layout,
                            int n, const float sensor_origin[3]);
+/* update() from a sensor-frame cloud and the sensor's pose: what the
+ * reference's driver does before calling update() (buildCloudInOdomFrame,
+ * src/main.cpp:640-693, called at :450-452) — drop non-finite points and
+ * points farther than the max raycast range, map the rest to the world as
+ * rotation * p + translation (rotation row-major) — done on the device,
+ * followed by update(world_cloud, translation).  A cloud with no point left
+ * leaves the grid untouched, as the driver then skips update().             */
+int cublox_grid_update_pose(cublox_grid *g, const float *xyz, int layout, int n,
+                            const float rotation[9], const float translation[3]);
 
 /* recenter(pos) — OccupancyGrid.hpp:57, OccupancyGrid.cpp:141-179.
  * *action (may be NULL): 0 nothing, 1 slabs cleared, 2 full reset.

@@ -121,6 +121,8 @@ def oracle_lib():
         L.orc_global_to_pos.restype = ctypes.c_float
         L.orc_logit.argtypes = [ctypes.c_float]
         L.orc_logit.restype = ctypes.c_float
+        L.orc_ingest.argtypes = [f3, ctypes.c_int, f3, f3, ctypes.c_float, f3]
+        L.orc_ingest.restype = ctypes.c_int
         st = ctypes.POINTER(OrcStats)
         L.orc_raycast.argtypes = [G, f3, f3, f3, ctypes.c_int, f3, st, ctypes.c_int]
         L.orc_apply.argtypes = [G, st, ctypes.c_int]
@@ -430,3 +432,16 @@ class RefGrid:
                 for a, d in ((occ, np.float32), (op, np.int32), (hit, np.int32))]
         ptrs = [f(a) if a is not None else None for a, f in zip(keep, (_fp, _ip, _ip))]
         self._call(self._L.ref_upload(self._h, *ptrs), "ref_upload")
+
+
+def ingest(points_sensor, rotation, translation, max_range):
+    """World-frame cloud the reference driver builds from a sensor-frame one
+    (src/main.cpp:640-693): filtered, transformed, in input order."""
+    L = oracle_lib()
+    p = np.ascontiguousarray(np.asarray(points_sensor, dtype=np.float32).reshape(-1, 3))
+    R = np.ascontiguousarray(np.asarray(rotation, dtype=np.float32).reshape(9))
+    t = np.ascontiguousarray(np.asarray(translation, dtype=np.float32).reshape(3))
+    out = np.empty_like(p)
+    r = np.float32(max_range)
+    k = L.orc_ingest(_fp(p), p.shape[0], _fp(R), _fp(t), float(r * r), _fp(out))
+    return out[:k].copy()

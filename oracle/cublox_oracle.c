@@ -835,3 +835,19 @@ float orc_fetch_sos(const float c[3], const int gi[3], float res, int ctr,
   }
   return sos(d[0], d[1], d[2], ORC_FP_FETCH_SOS(mode));
 }
+
+/* main.cpp:666-684, one point at a time. */
+int orc_ingest(const float *xyz_aos, int n, const float R[9], const float t[3],
+               float max_r2, float *out_aos) {
+  int kept = 0;
+  for (int i = 0; i < n; ++i) {
+    const float x = xyz_aos[3 * i], y = xyz_aos[3 * i + 1], z = xyz_aos[3 * i + 2];
+    if (!isfinite(x) || !isfinite(y) || !isfinite(z)) continue;
+    const float r2 = (x * x + y * y) + z * z;  /* squaredNorm */
+    if (r2 > max_r2) continue;
+    for (int a = 0; a < 3; ++a)
+      out_aos[3 * kept + a] = ((R[3 * a] * x + R[3 * a + 1] * y) + R[3 * a + 2] * z) + t[a];
+    ++kept;
+  }
+  return kept;
+}

@@ -110,6 +110,14 @@ void orc_hash_to_local(int h, const int map[3], const int half[3], int l[3]);
 float orc_global_to_pos(int g, float res, int origin_at_center);
 float orc_logit(float p);
 
+/* The reference driver's buildCloudInOdomFrame (src/main.cpp:640-693): keep
+ * finite points with (x*x + y*y) + z*z <= max_r2, write ((r0*x + r1*y) +
+ * r2*z) + t per row (Eigen's order for Isometry3f * Vector3f on x86-64
+ * without FMA; R row-major), in input order.  Returns the points kept.
+ * Eigen itself is absent here, so that order is restated, not pinned.     */
+int orc_ingest(const float *xyz_aos, int n, const float R[9], const float t[3],
+               float max_r2, float *out_aos);
+
 /* Raycast of one scan into op/hit (kernels.cu:33-152).  Does not snap the
  * first-run origin and does not apply.  `nthreads` > 1 splits the rays over
  * POSIX threads with relaxed atomic increments.                            */

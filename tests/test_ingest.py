@@ -1,0 +1,98 @@
+"""Sensor-frame ingest (cublox_grid_update_pose): the reference driver's
+buildCloudInOdomFrame (src/main.cpp:640-693) — finite and range filter, then
+the sensor-to-world isometry — followed by update().
+
+CPU: the oracle's restatement against the same arithmetic written out in
+numpy float32 (IEEE, no fused multiply-add).  GPU: update_pose equals
+update() of the oracle-built world cloud, bit for bit, for host and device
+inputs, and a cloud with no point left leaves the grid untouched.
+"""
+import numpy as np
+import pytest
+
+import cublox_b200 as C
+import oracle as O
+from cublox_b200 import synth
+
+
+def pose(yaw=0.7, roll=0.05):
+    cy, sy, cr, sr = np.cos(yaw), np.sin(yaw), np.cos(roll), np.sin(roll)
+    Rz = np.array([[cy, -sy, 0], [sy, cy, 0], [0, 0, 1]])
+    Rx = np.array([[1, 0, 0], [0, cr, -sr], [0, sr, cr]])
+    return (Rz @ Rx).astype(np.float32)
+
+
+def sensor_cloud(w, R, t, n_bad=64, seed=0):
+    world = w.scan(0).astype(np.float64)
+    local = ((world - t.astype(np.float64)) @ R.astype(np.float64)).astype(np.float32)
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(local.shape[0], n_bad, replace=False)
+    local[idx[: n_bad // 2], rng.integers(0, 3)] = np.nan
+    local[idx[n_bad // 2:]] *= np.float32(40.0)  # beyond the range filter
+    return local
+
+
+def numpy_ingest(p, R, t, max_range):
+    f = np.float32
+    x, y, z = p[:, 0], p[:, 1], p[:, 2]
+    keep = np.isfinite(p).all(axis=1)
+    r2 = (x * x + y * y) + z * z
+    keep &= ~(r2 > f(max_range) * f(max_range))
+    out = np.stack([((R[a, 0] * x + R[a, 1] * y) + R[a, 2] * z) + t[a] for a in range(3)], axis=1)
+    return out[keep].astype(np.float32)
+
+
+def test_oracle_ingest_matches_explicit_float32():
+    O.build()
+    w = synth.plain_small()
+    R, t = pose(), np.float32([0.4, -1.1, 1.8])
+    p = sensor_cloud(w, R, t)
+    got = O.ingest(p, R, t, w.sensor.max_range)
+    want = numpy_ingest(p, R, t, w.sensor.max_range)
+    assert got.shape == want.shape and got.shape[0] < p.shape[0]
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    # the filter keeps r^2 == max^2 and drops anything beyond
+    edge = np.float32([[20.0, 0.0, 0.0], [20.000002, 0.0, 0.0]])
+    assert O.ingest(edge, np.eye(3, dtype=np.float32), np.zeros(3, np.float32), 20.0).shape[0] == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_update_pose_equals_update_of_driver_cloud(where):
+    import torch
+    w = synth.plain_small()
+    lo = C.yaml_log_odds()
+    R, t = pose(), np.float32([0.4, -1.1, 1.8])
+    p = sensor_cloud(w, R, t)
+    world = O.ingest(p, R, t, w.sensor.max_range)
+    a = C.OccupancyGrid(w.half, w.resolution, False, 4.0)
+    b = C.OccupancyGrid(w.half, w.resolution, False, 4.0)
+    o = O.OracleGrid(w.half, w.resolution, False, 4.0)
+    for g in (a, b):
+        g.setLogOddsParams(*lo)
+        g.setMaxRaycastRange(w.sensor.max_range)
+    o.set_log_odds(*lo)
+    o.set_max_range(w.sensor.max_range)
+    src = torch.from_numpy(p).cuda() if where == "device" else p
+    for k in range(2):  # first run (snap) and a second scan from a moved pose
+        tk = t + np.float32([0.3 * k, 0.1 * k, 0.0])
+        wk = O.ingest(p, R, tk, w.sensor.max_range)
+        a.update_pose(src, R, tk)
+        b.update(wk, tk)
+        o.update(wk, tk)
+        assert a.getOriginIndex() == b.getOriginIndex()
+        assert np.array_equal(a.export().view(np.uint32), b.export().view(np.uint32)), k
+        assert np.array_equal(a.export().view(np.uint32), o.occ().view(np.uint32)), k
+    assert world.shape[0] < p.shape[0]
+
+
+@pytest.mark.gpu
+def test_update_pose_with_nothing_left_is_a_no_op():
+    w = synth.plain_small()
+    g = C.OccupancyGrid(w.half, w.resolution, False, 4.0, origin=(5.0, 5.0, 0.0))
+    g.setMaxRaycastRange(w.sensor.max_range)
+    before = g.getOriginIndex()
+    far = np.full((100, 3), 1000.0, np.float32)  # all beyond the range filter
+    g.update_pose(far, np.eye(3, dtype=np.float32), np.float32([0.0, 0.0, 1.8]))
+    assert g.getOriginIndex() == before  # no first-run snap: update() was never due
+    assert not g.export().any()
