@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libcublox_b200.so")
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_RANGE, ERR_DEVICE = -1, -2, -3, -4, -5
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
+DEPTH_U16_MM, DEPTH_F32_M = 0, 1
 OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT, OPT_SEGMENT, OPT_FOLD, OPT_BLOCK, OPT_CONTIGUOUS = (
     1, 2, 3, 4, 5, 6, 7, 8)
 
@@ -117,6 +118,8 @@ def lib():
             "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
             "cublox_grid_last_clear": ([G, i64], ctypes.c_int),
             "cublox_grid_update_pose": ([G, f, ctypes.c_int, ctypes.c_int, f, f], ctypes.c_int),
+            "cublox_grid_update_depth": ([G, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int64, f, f, f], ctypes.c_int),
             "cublox_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
             "cublox_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
             "cublox_batch_add_grid": ([ctypes.c_void_p, i, ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -493,6 +496,33 @@ class OccupancyGrid:
             p = np.ascontiguousarray(np.asarray(cloud_sensor, dtype=np.float32).reshape(-1, 3))
             n, ptr = p.shape[0], _fp(p)
         _check(lib().cublox_grid_update_pose(self._h, ptr, LAYOUT_AOS, n, _fp(R), _fp(t)), "update_pose")
+
+    def update_depth(self, image, intrinsics, rotation, translation):
+        """update() from an (H, W) depth image — uint16 millimetres
+        (16UC1) or float32 metres (32FC1), host array or CUDA tensor — with
+        intrinsics (fx, fy, cx, cy) and the camera pose, as the reference
+        driver's depthCallback + buildCloudInOdomFrame do."""
+        K = np.ascontiguousarray(np.asarray(intrinsics, dtype=np.float32).reshape(4))
+        R = np.ascontiguousarray(np.asarray(rotation, dtype=np.float32).reshape(9))
+        t = np.ascontiguousarray(np.asarray(translation, dtype=np.float32).reshape(3))
+        dp = _dev_ptr(image)
+        if dp is not None:
+            h, w = int(image.shape[0]), int(image.shape[1])
+            es = image.element_size()
+            enc = DEPTH_U16_MM if es == 2 else DEPTH_F32_M
+            step, ptr, keep = int(image.stride(0)) * es, dp, None
+        else:
+            keep = np.asarray(image)
+            if keep.dtype not in (np.uint16, np.float32):
+                keep = keep.astype(np.float32)
+            if keep.strides[1] != keep.itemsize:
+                keep = np.ascontiguousarray(keep)
+            h, w = keep.shape
+            enc = DEPTH_U16_MM if keep.dtype == np.uint16 else DEPTH_F32_M
+            step, ptr = keep.strides[0], keep.ctypes.data
+        _check(lib().cublox_grid_update_depth(self._h, ctypes.c_void_p(ptr), enc, w, h, step, _fp(K),
+                                              _fp(R), _fp(t)), "update_depth")
+        del keep
 
     def update_ptr(self, ptr: int, n: int, sensor_origin, layout: int = LAYOUT_SOA):
         """update() from a raw pointer (device, pinned or pageable host)."""

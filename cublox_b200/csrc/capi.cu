@@ -112,6 +112,7 @@ static void free_all(cublox_grid *g) {
   cudaFree(g->d_cloud);
   cudaFree(g->d_world);
   cudaFree(g->d_kept);
+  cudaFree(g->d_image);
   cudaFree(g->d_bins);
   cudaFree(g->d_work);
   cudaFree(g->d_segs);
@@ -544,6 +545,7 @@ RayParams cublox_b200::detail::ray_params(const cublox_grid *g, const float *x,
 size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
   size_t b = 12 * static_cast<size_t>(g->d_occ ? g->voxel_num : 0);
   b += sizeof(float) * 3 * (static_cast<size_t>(g->cloud_cap) + static_cast<size_t>(g->world_cap));
+  b += g->image_cap;
   b += g->fq_bytes + 13 * static_cast<size_t>(g->fcap) + 13 * static_cast<size_t>(g->qcap);
   b += static_cast<size_t>(g->split_cap) * (16 * split_seg_bytes() + 64);  // 16 segments a ray
   b += static_cast<size_t>(g->bin_cap) * 16;
@@ -570,6 +572,9 @@ int cublox_b200::detail::release_scratch(cublox_grid *g) {
   cudaFree(g->d_world);
   g->d_world = nullptr;
   g->world_cap = 0;
+  cudaFree(g->d_image);
+  g->d_image = nullptr;
+  g->image_cap = 0;
   void **bufs[] = {reinterpret_cast<void **>(&g->d_cloud), reinterpret_cast<void **>(&g->d_bins),
                    reinterpret_cast<void **>(&g->d_work),  reinterpret_cast<void **>(&g->d_segs),
                    reinterpret_cast<void **>(&g->d_rays),  reinterpret_cast<void **>(&g->d_hist),
@@ -690,6 +695,64 @@ int cublox_grid_update_xyz(cublox_grid *g, const float *xyz, int layout,
   return update_impl(g, nullptr, nullptr, nullptr, xyz, layout, n, sensor_origin);
 }
 
+// buildCloudInOdomFrame uses at most the first kMaxCloudPoints points of a
+// cloud (src/main.cpp:54, :655-661).
+constexpr int kDriverCloudCap = 1000000;
+
+static int ensure_world(cublox_grid *g, int n) {
+  if (n <= g->world_cap) return CUBLOX_OK;
+  CK(cudaStreamSynchronize(g->stream));
+  cudaFree(g->d_world);
+  g->d_world = nullptr;
+  g->world_cap = 0;
+  if (cudaMalloc(&g->d_world, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUBLOX_ERR_NOMEM, "sensor-frame update: world buffer allocation failed");
+  }
+  g->world_cap = n;
+  return CUBLOX_OK;
+}
+
+// Ingest parameters of a sensor-frame update; on the first run the kept
+// points are counted (the driver calls update() only if one survives, and
+// the first call snaps the window).
+static int world_params(cublox_grid *g, int n, const float rotation[9],
+                        const float translation[3], IngestParams *ip) {
+  int rc = ensure_world(g, n);
+  if (rc) return rc;
+  *ip = IngestParams{};
+  ip->n = n;
+  for (int i = 0; i < 9; ++i) ip->R[i] = rotation[i];
+  for (int a = 0; a < 3; ++a) ip->t[a] = translation[a];
+  ip->max_r2 = fmul(g->max_range, g->max_range);  // main.cpp:451
+  ip->dst = g->d_world;
+  ip->count = nullptr;
+  if (g->first_run) {
+    if (!g->d_kept && cudaMalloc(&g->d_kept, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "sensor-frame update: allocation failed");
+    }
+    CK(cudaMemsetAsync(g->d_kept, 0, sizeof(int), g->stream));
+    ip->count = g->d_kept;
+  }
+  return CUBLOX_OK;
+}
+
+// After the ingest launch: update(world_cloud, translation), unless nothing
+// survived the driver's filters on the first run.
+static int world_update(cublox_grid *g, const IngestParams &ip, const float translation[3]) {
+  if (ip.count) {
+    int kept = 0;
+    CK(cudaMemcpyAsync(&kept, ip.count, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    if (kept == 0) return CUBLOX_OK;
+  }
+  snap_first_run(g, translation);
+  const int n = ip.n;
+  return integrate(g, g->d_world, g->d_world + n, g->d_world + 2 * static_cast<size_t>(n), n, 1,
+                   translation);
+}
+
 // update() from a sensor-frame cloud and the sensor pose: the reference
 // driver's buildCloudInOdomFrame (src/main.cpp:640-693) on the device, then
 // update(world_cloud, t) (OccupancyGrid.cpp:181-238).
@@ -722,49 +785,67 @@ int cublox_grid_update_pose(cublox_grid *g, const float *xyz, int layout, int n,
     }
     src = g->d_cloud;
   }
-  if (n > g->world_cap) {
-    CK(cudaStreamSynchronize(g->stream));
-    cudaFree(g->d_world);
-    g->d_world = nullptr;
-    g->world_cap = 0;
-    if (cudaMalloc(&g->d_world, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update_pose: world buffer allocation failed");
-    }
-    g->world_cap = n;
-  }
-  IngestParams ip{};
+  IngestParams ip;
+  if ((rc = world_params(g, std::min(n, kDriverCloudCap), rotation, translation, &ip))) return rc;
   ip.xyz = src;
   ip.layout = layout;
-  ip.n = n;
-  for (int i = 0; i < 9; ++i) ip.R[i] = rotation[i];
-  for (int a = 0; a < 3; ++a) ip.t[a] = translation[a];
-  ip.max_r2 = fmul(g->max_range, g->max_range);  // main.cpp:451
-  ip.dst = g->d_world;
-  ip.count = nullptr;
-  if (g->first_run) {
-    // The driver calls update() only if a point survives its filters; the
-    // first call snaps the window, so the first run needs the count.
-    if (!g->d_kept) {
-      if (cudaMalloc(&g->d_kept, sizeof(int)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update_pose: allocation failed");
-      }
-    }
-    CK(cudaMemsetAsync(g->d_kept, 0, sizeof(int), g->stream));
-    ip.count = g->d_kept;
-  }
+  ip.col = n;
   launch_ingest(ip, g->stream);
   CK_LAUNCH();
-  if (g->first_run) {
-    int kept = 0;
-    CK(cudaMemcpyAsync(&kept, g->d_kept, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
-    CK(cudaStreamSynchronize(g->stream));
-    if (kept == 0) return CUBLOX_OK;
+  return world_update(g, ip, translation);
+}
+
+// update() from a depth image, as the reference driver's depthCallback
+// (src/main.cpp:558-638) turns it into a cloud before the same steps.
+int cublox_grid_update_depth(cublox_grid *g, const void *image, int encoding, int width,
+                             int height, int64_t step, const float intrinsics[4],
+                             const float rotation[9], const float translation[3]) {
+  if (!g || !intrinsics || !rotation || !translation)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_depth: null argument");
+  if (encoding != CUBLOX_DEPTH_U16_MM && encoding != CUBLOX_DEPTH_F32_M)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_depth: unknown encoding");
+  const int64_t px = encoding == CUBLOX_DEPTH_U16_MM ? 2 : 4;
+  if (width < 0 || height < 0 || step < px * width ||
+      static_cast<int64_t>(width) * height > 0x7fffffff)
+    return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_depth: bad image size or step");
+  const int n = width * height;
+  if (g->voxel_num <= 0 || n == 0) return CUBLOX_OK;  // depthCallback returns on 0 x 0
+  if (!image) return fail(CUBLOX_ERR_INVALID, "cublox_grid_update_depth: null image");
+  const size_t bytes = static_cast<size_t>(step) * static_cast<size_t>(height);
+  const unsigned char *dimg = static_cast<const unsigned char *>(image);
+  if (mem_kind(image) != 2) {
+    if (bytes > g->image_cap) {
+      CK(cudaStreamSynchronize(g->stream));
+      cudaFree(g->d_image);
+      g->d_image = nullptr;
+      g->image_cap = 0;
+      if (cudaMalloc(&g->d_image, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update_depth: image buffer allocation failed");
+      }
+      g->image_cap = bytes;
+    }
+    CK(cudaMemcpyAsync(g->d_image, image, bytes, cudaMemcpyHostToDevice, g->stream));
+    if (!g->stage_ev[0]) CK(cudaEventCreateWithFlags(&g->stage_ev[0], cudaEventDisableTiming));
+    CK(cudaEventRecord(g->stage_ev[0], g->stream));
+    CK(cudaEventSynchronize(g->stage_ev[0]));  // the caller may reuse its image
+    dimg = g->d_image;
   }
-  snap_first_run(g, translation);
-  return integrate(g, g->d_world, g->d_world + n, g->d_world + 2 * static_cast<size_t>(n), n, 1,
-                   translation);
+  DepthParams dp{};
+  int rc = world_params(g, std::min(n, kDriverCloudCap), rotation, translation, &dp.ingest);
+  if (rc) return rc;
+  dp.image = dimg;
+  dp.encoding = encoding;
+  dp.width = width;
+  dp.height = height;
+  dp.step = step;
+  dp.fx = intrinsics[0];
+  dp.fy = intrinsics[1];
+  dp.cx = intrinsics[2];
+  dp.cy = intrinsics[3];
+  launch_depth(dp, g->stream);
+  CK_LAUNCH();
+  return world_update(g, dp.ingest, translation);
 }
 
 // ---- recenter ---------------------------------------------------------------

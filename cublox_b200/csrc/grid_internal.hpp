@@ -70,6 +70,8 @@ struct cublox_grid {
   float *d_world = nullptr;  // update_pose: world-frame SoA points
   int world_cap = 0;
   int *d_kept = nullptr;     // update_pose: points kept by the range filter
+  unsigned char *d_image = nullptr;  // update_depth: the image on the device
+  size_t image_cap = 0;
   float *h_stage[2] = {nullptr, nullptr};
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   int stage_cap = 0;

@@ -331,33 +331,61 @@ __global__ void gather_soa_kernel(const float *xyz, int layout, int n,
 
 // One point of buildCloudInOdomFrame (main.cpp:666-684), in its FP32 order
 // on x86-64 without FMA: squaredNorm as (x*x + y*y) + z*z, the isometry as
-// ((r0*x + r1*y) + r2*z) + t per row.
+// ((r0*x + r1*y) + r2*z) + t per row; a dropped point is written as NaN.
+__device__ __forceinline__ void ingest_point(const IngestParams &p, int i, float x, float y,
+                                             float z) {
+  float w[3];
+  bool keep = isfinite(x) && isfinite(y) && isfinite(z);
+  if (keep) keep = !(fadd(fadd(fmul(x, x), fmul(y, y)), fmul(z, z)) > p.max_r2);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float *r = p.R + 3 * a;
+    w[a] = keep ? fadd(fadd(fadd(fmul(r[0], x), fmul(r[1], y)), fmul(r[2], z)), p.t[a])
+                : __int_as_float(0x7fc00000);
+  }
+  p.dst[i] = w[0];
+  p.dst[p.n + i] = w[1];
+  p.dst[2 * static_cast<size_t>(p.n) + i] = w[2];
+  if (p.count && keep) atomicAdd(p.count, 1);
+}
+
 __global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n;
        i += gridDim.x * blockDim.x) {
-    float x, y, z;
-    if (p.layout == 1) {
-      x = p.xyz[3 * static_cast<size_t>(i)];
-      y = p.xyz[3 * static_cast<size_t>(i) + 1];
-      z = p.xyz[3 * static_cast<size_t>(i) + 2];
+    if (p.layout == 1)
+      ingest_point(p, i, p.xyz[3 * static_cast<size_t>(i)], p.xyz[3 * static_cast<size_t>(i) + 1],
+                   p.xyz[3 * static_cast<size_t>(i) + 2]);
+    else
+      ingest_point(p, i, p.xyz[i], p.xyz[p.col + i], p.xyz[2 * static_cast<size_t>(p.col) + i]);
+  }
+}
+
+// One pixel of depthCallback (main.cpp:596-631): invalid depth (16-bit 0;
+// float non-finite or <= 0) gives NaN; else z in metres, x = ((u - cx) * z)
+// / fx, y = ((v - cy) * z) / fy, then ingest_point.
+__global__ void __launch_bounds__(256) depth_kernel(const DepthParams p) {
+  const int n = p.ingest.n;  // pixels used (the driver's cloud cap)
+  const float nan = __int_as_float(0x7fc00000);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = i / p.width, u = i - v * p.width;
+    const unsigned char *row = p.image + static_cast<long long>(v) * p.step;
+    float z;
+    bool valid;
+    if (p.encoding == 0) {
+      const uint16_t raw = reinterpret_cast<const uint16_t *>(row)[u];
+      valid = raw != 0;
+      z = fmul(static_cast<float>(raw), 0.001f);
     } else {
-      x = p.xyz[i];
-      y = p.xyz[p.n + i];
-      z = p.xyz[2 * static_cast<size_t>(p.n) + i];
+      z = reinterpret_cast<const float *>(row)[u];
+      valid = isfinite(z) && z > 0.0f;
     }
-    float w[3];
-    bool keep = isfinite(x) && isfinite(y) && isfinite(z);
-    if (keep) keep = !(fadd(fadd(fmul(x, x), fmul(y, y)), fmul(z, z)) > p.max_r2);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float *r = p.R + 3 * a;
-      w[a] = keep ? fadd(fadd(fadd(fmul(r[0], x), fmul(r[1], y)), fmul(r[2], z)), p.t[a])
-                  : __int_as_float(0x7fc00000);
+    if (!valid) {
+      ingest_point(p.ingest, i, nan, nan, nan);
+      continue;
     }
-    p.dst[i] = w[0];
-    p.dst[p.n + i] = w[1];
-    p.dst[2 * static_cast<size_t>(p.n) + i] = w[2];
-    if (p.count && keep) atomicAdd(p.count, 1);
+    const float x = fdiv(fmul(fsub(static_cast<float>(u), p.cx), z), p.fx);
+    const float y = fdiv(fmul(fsub(static_cast<float>(v), p.cy), z), p.fy);
+    ingest_point(p.ingest, i, x, y, z);
   }
 }
 
@@ -443,6 +471,12 @@ void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
 void launch_ingest(const IngestParams &p, cudaStream_t s) {
   if (p.n <= 0) return;
   ingest_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(p);
+}
+
+void launch_depth(const DepthParams &p, cudaStream_t s) {
+  const int n = p.ingest.n;
+  if (n <= 0) return;
+  depth_kernel<<<(n + 255) / 256, 256, 0, s>>>(p);
 }
 
 }  // namespace cublox_b200

@@ -132,8 +132,9 @@ void launch_query(const QueryParams &p, cudaStream_t s);
 // farther than sqrt(max_r2) from the sensor are dropped (written as NaN, which
 // the walk drops), the rest become R p + t.
 struct IngestParams {
-  const float *xyz;  // n points, layout 0 SoA / 1 AoS
-  int layout, n;
+  const float *xyz;  // points, layout 0 SoA (columns `col` floats apart) / 1 AoS
+  int layout, n;     // the first n points are used
+  int col;
   float R[9];        // row-major rotation, sensor -> world
   float t[3];        // sensor origin in the world
   float max_r2;      // squared range filter
@@ -141,6 +142,19 @@ struct IngestParams {
   int *count;        // if not null: += points kept
 };
 void launch_ingest(const IngestParams &p, cudaStream_t s);
+
+// Depth image -> sensor-frame points (the reference driver's depthCallback,
+// src/main.cpp:558-632), then the same filter and transform as IngestParams,
+// one pixel per point (row-major), written as world-frame SoA.
+struct DepthParams {
+  const unsigned char *image;  // height rows of `step` bytes
+  int encoding;                // 0: 16-bit millimetres (16UC1, mono16), 1: 32-bit float metres
+  int width, height;
+  long long step;
+  float fx, fy, cx, cy;
+  IngestParams ingest;         // xyz, layout unused; n = width * height
+};
+void launch_depth(const DepthParams &p, cudaStream_t s);
 
 void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
                        cudaStream_t s);

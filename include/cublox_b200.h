@@ -118,6 +118,19 @@ int cublox_grid_update_xyz(cublox_grid *g, const float *xyz, int layout,
 int cublox_grid_update_pose(cublox_grid *g, const float *xyz, int layout, int n,
                             const float rotation[9], const float translation[3]);
 
+/* Depth image encodings of cublox_grid_update_depth (depthCallback,
+ * src/main.cpp:572-573).                                                    */
+#define CUBLOX_DEPTH_U16_MM 0 /* 16UC1 / mono16: millimetres, 0 = no return  */
+#define CUBLOX_DEPTH_F32_M 1  /* 32FC1: metres, non-finite or <= 0 = none    */
+/* update() from a depth image (height rows of `step` bytes, host or device):
+ * the reference driver's depthCallback (src/main.cpp:558-638) makes one
+ * camera-frame point per pixel, x = ((u - cx) * z) / fx, y = ((v - cy) * z)
+ * / fy, then the cloud goes through cublox_grid_update_pose.  intrinsics =
+ * {fx, fy, cx, cy} (K(0,0), K(1,1), K(0,2), K(1,2)).                        */
+int cublox_grid_update_depth(cublox_grid *g, const void *image, int encoding, int width,
+                             int height, int64_t step, const float intrinsics[4],
+                             const float rotation[9], const float translation[3]);
+
 /* recenter(pos) — OccupancyGrid.hpp:57, OccupancyGrid.cpp:141-179.
  * *action (may be NULL): 0 nothing, 1 slabs cleared, 2 full reset.
  * mode 0 reproduces the reference's slab set exactly (its extra band of

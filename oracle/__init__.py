@@ -123,6 +123,9 @@ def oracle_lib():
         L.orc_logit.restype = ctypes.c_float
         L.orc_ingest.argtypes = [f3, ctypes.c_int, f3, f3, ctypes.c_float, f3]
         L.orc_ingest.restype = ctypes.c_int
+        L.orc_depth_cloud.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_longlong, f3, f3]
+        L.orc_depth_cloud.restype = None
         st = ctypes.POINTER(OrcStats)
         L.orc_raycast.argtypes = [G, f3, f3, f3, ctypes.c_int, f3, st, ctypes.c_int]
         L.orc_apply.argtypes = [G, st, ctypes.c_int]
@@ -445,3 +448,19 @@ def ingest(points_sensor, rotation, translation, max_range):
     r = np.float32(max_range)
     k = L.orc_ingest(_fp(p), p.shape[0], _fp(R), _fp(t), float(r * r), _fp(out))
     return out[:k].copy()
+
+
+def depth_cloud(image, intrinsics):
+    """Camera-frame cloud the reference driver makes from a depth image
+    (src/main.cpp:558-632): (H*W, 3) float32, NaN rows for invalid pixels.
+    `image`: (H, W) uint16 millimetres or float32 metres."""
+    L = oracle_lib()
+    img = np.ascontiguousarray(image)
+    enc = 0 if img.dtype == np.uint16 else 1
+    if enc == 1:
+        img = img.astype(np.float32, copy=False)
+    h, w = img.shape
+    K = np.ascontiguousarray(np.asarray(intrinsics, dtype=np.float32).reshape(4))
+    out = np.empty((h * w, 3), dtype=np.float32)
+    L.orc_depth_cloud(img.ctypes.data, enc, w, h, img.strides[0], _fp(K), _fp(out))
+    return out

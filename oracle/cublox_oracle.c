@@ -840,6 +840,7 @@ float orc_fetch_sos(const float c[3], const int gi[3], float res, int ctr,
 int orc_ingest(const float *xyz_aos, int n, const float R[9], const float t[3],
                float max_r2, float *out_aos) {
   int kept = 0;
+  if (n > 1000000) n = 1000000; /* kMaxCloudPoints, main.cpp:54, :655-661 */
   for (int i = 0; i < n; ++i) {
     const float x = xyz_aos[3 * i], y = xyz_aos[3 * i + 1], z = xyz_aos[3 * i + 2];
     if (!isfinite(x) || !isfinite(y) || !isfinite(z)) continue;
@@ -850,4 +851,35 @@ int orc_ingest(const float *xyz_aos, int n, const float R[9], const float t[3],
     ++kept;
   }
   return kept;
+}
+
+/* depthCallback (main.cpp:596-631): one camera-frame point per pixel,
+ * row-major, NaN where the depth is invalid. */
+void orc_depth_cloud(const unsigned char *image, int encoding, int width, int height,
+                     long long step, const float K[4], float *out_aos) {
+  const float nan = NAN;
+  for (int v = 0; v < height; ++v) {
+    const unsigned char *row = image + (long long)v * step;
+    for (int u = 0; u < width; ++u) {
+      float *o = out_aos + 3 * ((long long)v * width + u);
+      float z;
+      int valid;
+      if (encoding == 0) {
+        unsigned short raw;
+        memcpy(&raw, row + 2 * u, 2);
+        valid = raw != 0;
+        z = (float)raw * 0.001f;
+      } else {
+        memcpy(&z, row + 4 * u, 4);
+        valid = isfinite(z) && z > 0.f;
+      }
+      if (!valid) {
+        o[0] = o[1] = o[2] = nan;
+        continue;
+      }
+      o[0] = ((float)u - K[2]) * z / K[0];
+      o[1] = ((float)v - K[3]) * z / K[1];
+      o[2] = z;
+    }
+  }
 }

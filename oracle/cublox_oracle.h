@@ -118,6 +118,13 @@ float orc_logit(float p);
 int orc_ingest(const float *xyz_aos, int n, const float R[9], const float t[3],
                float max_r2, float *out_aos);
 
+/* The reference driver's depthCallback (src/main.cpp:558-632): one
+ * camera-frame point per pixel (row-major) of a 16-bit millimetre
+ * (encoding 0) or float metre (1) image, NaN where the depth is invalid.
+ * K = {fx, fy, cx, cy}.                                                   */
+void orc_depth_cloud(const unsigned char *image, int encoding, int width, int height,
+                     long long step, const float K[4], float *out_aos);
+
 /* Raycast of one scan into op/hit (kernels.cu:33-152).  Does not snap the
  * first-run origin and does not apply.  `nthreads` > 1 splits the rays over
  * POSIX threads with relaxed atomic increments.                            */

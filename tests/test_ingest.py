@@ -96,3 +96,70 @@ def test_update_pose_with_nothing_left_is_a_no_op():
     g.update_pose(far, np.eye(3, dtype=np.float32), np.float32([0.0, 0.0, 1.8]))
     assert g.getOriginIndex() == before  # no first-run snap: update() was never due
     assert not g.export().any()
+
+
+# ---------------------------------------------------------------------------
+# depth images (depthCallback, src/main.cpp:558-638)
+# ---------------------------------------------------------------------------
+K = np.float32([240.0, 238.5, 159.5, 119.25])
+
+
+def depth_images(seed=3, h=120, w=160):
+    rng = np.random.default_rng(seed)
+    mm = rng.integers(300, 9000, size=(h, w)).astype(np.uint16)
+    mm[rng.random((h, w)) < 0.05] = 0
+    m = (mm.astype(np.float32) * np.float32(0.001)) + rng.normal(0, 0.01, (h, w)).astype(np.float32)
+    m[rng.random((h, w)) < 0.03] = np.nan
+    m[rng.random((h, w)) < 0.03] = -1.0
+    return mm, m.astype(np.float32)
+
+
+def numpy_depth(img):
+    h, w = img.shape
+    v, u = np.mgrid[0:h, 0:w]
+    u = u.astype(np.float32)
+    v = v.astype(np.float32)
+    if img.dtype == np.uint16:
+        valid = img != 0
+        z = img.astype(np.float32) * np.float32(0.001)
+    else:
+        z = img
+        valid = np.isfinite(z) & (z > 0)
+    x = ((u - K[2]) * z) / K[0]
+    y = ((v - K[3]) * z) / K[1]
+    out = np.stack([x, y, z], axis=-1).reshape(-1, 3).astype(np.float32)
+    out[~valid.reshape(-1)] = np.nan
+    return out
+
+
+def test_oracle_depth_cloud_matches_explicit_float32():
+    O.build()
+    for img in depth_images():
+        got, want = O.depth_cloud(img, K), numpy_depth(img)
+        same = (got.view(np.uint32) == want.view(np.uint32)) | (np.isnan(got) & np.isnan(want))
+        assert same.all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("enc", [0, 1], ids=["16UC1", "32FC1"])
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_update_depth_equals_driver_cloud(enc, where):
+    import torch
+    img = depth_images()[enc]
+    R, t = pose(yaw=0.3, roll=-0.4), np.float32([1.0, 0.5, 1.2])
+    lo = C.yaml_log_odds()
+    a = C.OccupancyGrid((60, 60, 20), 0.05, False, 4.0)
+    b = C.OccupancyGrid((60, 60, 20), 0.05, False, 4.0)
+    for g in (a, b):
+        g.setLogOddsParams(*lo)
+        g.setMaxRaycastRange(6.0)
+    cloud = O.ingest(O.depth_cloud(img, K), R, t, 6.0)
+    if where == "device":
+        src = torch.from_numpy(img.view(np.int16) if enc == 0 else img).cuda()
+    else:
+        src = img
+    a.update_depth(src, K, R, t)
+    b.update(cloud, t)
+    assert a.getOriginIndex() == b.getOriginIndex()
+    assert np.array_equal(a.export().view(np.uint32), b.export().view(np.uint32))
+    assert a.export().any()
