@@ -118,6 +118,9 @@ def lib():
             "cublox_grid_count_scan": ([G, f, ctypes.c_int, f, i, i], ctypes.c_int),
             "cublox_grid_last_clear": ([G, i64], ctypes.c_int),
             "cublox_grid_update_pose": ([G, f, ctypes.c_int, ctypes.c_int, f, f], ctypes.c_int),
+            "cublox_grid_fetch_viz": ([G, f, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_float, ctypes.c_int64, f, f, ctypes.c_int64, i64],
+                                      ctypes.c_int),
             "cublox_grid_update_depth": ([G, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int64, f, f, f], ctypes.c_int),
             "cublox_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
@@ -350,6 +353,21 @@ class OccupancyGrid:
                                              st.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), total),
                "fetch_batch")
         return off, pos[:total], st[:total]
+
+    def fetch_viz(self, center, radius: float, state_filter=None, max_results: int = 0,
+                  subsample_step: int = 1, max_viz_radius: float = 25.0, max_points: int = 200000,
+                  robot_pos=None) -> np.ndarray:
+        """The driver's visualisation cloud of one fetch: (n, 4) float32
+        rows x, y, z, rgb (rgb's bits are 0x00RRGGBB)."""
+        flt = -1 if state_filter is None else int(state_filter)
+        rp = center if robot_pos is None else robot_pos
+        out = np.empty((max(int(max_points), 1), 4), dtype=np.float32)
+        n = ctypes.c_int64()
+        _check(lib().cublox_grid_fetch_viz(self._h, _f3(center), float(radius), flt, int(max_results),
+                                           int(subsample_step), float(max_viz_radius), int(max_points),
+                                           _f3(rp), _fp(out), out.shape[0], ctypes.byref(n)),
+               "fetch_viz")
+        return out[: n.value]
 
     def fetch_counts(self, centers, radius: float, state_filter=None, max_results: int = 0):
         flt = -1 if state_filter is None else int(state_filter)

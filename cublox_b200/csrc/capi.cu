@@ -1178,6 +1178,69 @@ int cublox_b200::detail::fetch_into(cublox_grid *g, cudaStream_t st, const float
 
 extern "C" {
 
+// The visualisation cloud the reference's driver publishes after its
+// OCCUPIED fetch (src/main.cpp:487-491 -> :740-790), built on the device
+// from the fetch samples (ascending global index order here).
+int cublox_grid_fetch_viz(cublox_grid *g, const float center[3], float radius, int filter,
+                          int max_results, int subsample_step, float max_viz_radius,
+                          int64_t max_points, const float robot_pos[3], float *out_xyzrgb,
+                          int64_t capacity, int64_t *n_out) {
+  if (n_out) *n_out = 0;
+  if (!g || !center || !robot_pos || !n_out || (capacity > 0 && !out_xyzrgb))
+    return fail(CUBLOX_ERR_INVALID, "fetch_viz: null argument");
+  if (max_points < 0) return fail(CUBLOX_ERR_INVALID, "fetch_viz: negative max_points");
+  int64_t off[2] = {0, 0};
+  int rc = fetch_impl(g, g->stream, center, 1, radius, filter, max_results, nullptr, off,
+                      nullptr, nullptr, std::numeric_limits<int64_t>::max(), true);
+  if (rc) return rc;
+  const int64_t total = off[1];
+  if (total == 0 || max_points == 0) return CUBLOX_OK;
+  const int64_t cap = std::min<int64_t>(max_points, total);
+  if (capacity < cap)
+    return fail(CUBLOX_ERR_INVALID, "fetch_viz: capacity " + std::to_string(capacity) + " < " +
+                                        std::to_string(cap) + " points");
+  // output on the device in the query buffers: d_qin (12 B per query slot)
+  // takes the 16 B per point, d_qout (1 B per slot) the 8 B count
+  const size_t need = sizeof(float) * 4 * static_cast<size_t>(cap);
+  if (static_cast<size_t>(g->qcap) * 12 < need || g->qcap < 8) {
+    CK(cudaStreamSynchronize(g->stream));
+    cudaFree(g->d_qin);
+    cudaFree(g->d_qout);
+    g->d_qin = nullptr;
+    g->d_qout = nullptr;
+    g->qcap = 0;
+    const int q = static_cast<int>(std::max<size_t>((need + 11) / 12, 8));
+    if (cudaMalloc(&g->d_qin, sizeof(float) * 3 * static_cast<size_t>(q)) != cudaSuccess ||
+        cudaMalloc(&g->d_qout, static_cast<size_t>(q)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "fetch_viz: allocation failed");
+    }
+    g->qcap = q;
+  }
+  VizParams vp{};
+  vp.pos = g->d_fpos;
+  vp.n = total;
+  vp.inv = g->res_inv;
+  vp.ctr = g->ctr ? 1 : 0;
+  vp.step = subsample_step;
+  vp.d_max = max_viz_radius;
+  for (int a = 0; a < 3; ++a) vp.o[a] = robot_pos[a];
+  vp.max_points = cap;
+  vp.out = g->d_qin;
+  vp.written = reinterpret_cast<long long *>(g->d_qout);
+  launch_viz(vp, g->stream);
+  CK_LAUNCH();
+  long long written = 0;
+  CK(cudaMemcpyAsync(&written, vp.written, sizeof(written), cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  if (written > 0)
+    CK(cudaMemcpyAsync(out_xyzrgb, g->d_qin, sizeof(float) * 4 * static_cast<size_t>(written),
+                       cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaStreamSynchronize(g->stream));
+  *n_out = written;
+  return CUBLOX_OK;
+}
+
 int cublox_grid_fetch(cublox_grid *g, const float center[3], float radius,
                       int filter, int max_results, float *out_pos,
                       uint8_t *out_state, int64_t capacity, int64_t *n_out) {

@@ -389,6 +389,86 @@ __global__ void __launch_bounds__(256) depth_kernel(const DepthParams p) {
   }
 }
 
+// occupancyVizDropBySubsample (main.cpp:71-84): the host's binning (no FMA)
+// of the sample position, x ^ y ^ z of the global index, modulo step.
+__device__ __forceinline__ bool viz_drop(const VizParams &p, const float *q) {
+  if (p.step <= 1) return false;
+  const unsigned mix = static_cast<unsigned>(pos_to_global_dev(q[0], p.inv, p.ctr != 0, 0u)) ^
+                       static_cast<unsigned>(pos_to_global_dev(q[1], p.inv, p.ctr != 0, 0u)) ^
+                       static_cast<unsigned>(pos_to_global_dev(q[2], p.inv, p.ctr != 0, 0u));
+  return (mix % static_cast<unsigned>(p.step)) != 0u;
+}
+
+// distanceToOccupancyColor + packRGBFloat (main.cpp:275-304): distance by
+// Eigen's norm, sqrt((dx*dx + dy*dy) + dz*dz).
+__device__ __forceinline__ float viz_rgb(const VizParams &p, const float *q) {
+  const float dx = fsub(q[0], p.o[0]), dy = fsub(q[1], p.o[1]), dz = fsub(q[2], p.o[2]);
+  const float d = fsqrt(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+  const float dm = fmaxf(p.d_max, 1.0f);
+  const float t = fminf(fmaxf(fdiv(d, dm), 0.0f), 1.0f);
+  float r, g, b;
+  if (t <= 0.5f) {
+    const float k = fmul(t, 2.0f);
+    r = 0.0f;
+    g = fsub(1.0f, k);
+    b = k;
+  } else {
+    const float k = fmul(fsub(t, 0.5f), 2.0f);
+    r = k;
+    g = 0.0f;
+    b = fsub(1.0f, k);
+  }
+  auto c8 = [](float c) {
+    return static_cast<uint32_t>(fmul(fminf(fmaxf(c, 0.0f), 1.0f), 255.0f));
+  };
+  return __uint_as_float((c8(r) << 16) | (c8(g) << 8) | c8(b));
+}
+
+// One block walks the samples in order, 1024 at a time, and compacts the
+// kept ones with a block-wide prefix sum, so the output keeps the sample
+// order; it stops at max_points.
+__global__ void __launch_bounds__(1024) viz_kernel(const VizParams p) {
+  __shared__ int warp_sum[32];
+  __shared__ long long s_base;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long c0 = 0; c0 < p.n; c0 += blockDim.x) {
+    const long long i = c0 + threadIdx.x;
+    const bool keep = i < p.n && !viz_drop(p, p.pos + 3 * i);
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_sum[warp] = __popc(m);
+    __syncthreads();
+    if (warp == 0) {
+      const int nw = blockDim.x >> 5;
+      int v = lane < nw ? warp_sum[lane] : 0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += y;
+      }
+      if (lane < nw) warp_sum[lane] = v;  // inclusive
+    }
+    __syncthreads();
+    const long long base = s_base;
+    const long long at = base + (warp ? warp_sum[warp - 1] : 0) + __popc(m & ((1u << lane) - 1u));
+    if (keep && at < p.max_points) {
+      const float *q = p.pos + 3 * i;
+      float4 v;
+      v.x = q[0];
+      v.y = q[1];
+      v.z = q[2];
+      v.w = viz_rgb(p, q);
+      reinterpret_cast<float4 *>(p.out)[at] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_base = base + warp_sum[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    if (s_base >= p.max_points) break;
+  }
+  if (threadIdx.x == 0) *p.written = s_base < p.max_points ? s_base : p.max_points;
+}
+
 int sm_count() {
   static int n = 0;
   if (n == 0) {
@@ -472,6 +552,8 @@ void launch_ingest(const IngestParams &p, cudaStream_t s) {
   if (p.n <= 0) return;
   ingest_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(p);
 }
+
+void launch_viz(const VizParams &p, cudaStream_t s) { viz_kernel<<<1, 1024, 0, s>>>(p); }
 
 void launch_depth(const DepthParams &p, cudaStream_t s) {
   const int n = p.ingest.n;

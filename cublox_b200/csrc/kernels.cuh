@@ -156,6 +156,24 @@ struct DepthParams {
 };
 void launch_depth(const DepthParams &p, cudaStream_t s);
 
+// Visualisation cloud of fetch samples (the reference driver's
+// publishOccupancyCloudAsync, src/main.cpp:740-790): samples in order,
+// dropped by the global-index subsample hash, coloured by distance to the
+// robot, packed as x, y, z, rgb floats, at most max_points written.
+struct VizParams {
+  const float *pos;  // n samples, x0 y0 z0 x1 ...
+  long long n;
+  float inv;
+  int ctr;
+  int step;          // subsample: keep 1 of `step` (<= 1: all)
+  float d_max;       // colour scale (max_viz_radius)
+  float o[3];        // robot position
+  long long max_points;
+  float *out;        // 4 floats per written point
+  long long *written;
+};
+void launch_viz(const VizParams &p, cudaStream_t s);
+
 void launch_gather_soa(const float *xyz, int layout, int n, float *dst,
                        cudaStream_t s);
 

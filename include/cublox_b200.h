@@ -146,6 +146,17 @@ int cublox_grid_set_recenter_mode(cublox_grid *g, int mode);
 int cublox_grid_fetch(cublox_grid *g, const float center[3], float radius,
                       int filter, int max_results, float *out_pos,
                       uint8_t *out_state, int64_t capacity, int64_t *n_out);
+/* The driver's visualisation cloud (src/main.cpp:740-790) of one fetch:
+ * the samples in fetch order, dropped unless (gx ^ gy ^ gz) % subsample_step
+ * == 0 for their global index (:71-84), coloured by distance to robot_pos
+ * over max_viz_radius (:275-289) and packed as x, y, z, rgb floats (the rgb
+ * float carries 0x00RRGGBB, :291-302); at most max_points.  Built on the
+ * device from the fetch's samples; *n_out gets the points written.       */
+int cublox_grid_fetch_viz(cublox_grid *g, const float center[3], float radius, int filter,
+                          int max_results, int subsample_step, float max_viz_radius,
+                          int64_t max_points, const float robot_pos[3], float *out_xyzrgb,
+                          int64_t capacity, int64_t *n_out);
+
 /* Many fetches in one launch (no reference counterpart beyond calling
  * fetchOccupancyAround once per centre).  out_offsets gets n_centers+1
  * entries; query q's samples are [out_offsets[q], out_offsets[q+1]).

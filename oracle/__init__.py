@@ -126,6 +126,9 @@ def oracle_lib():
         L.orc_depth_cloud.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_longlong, f3, f3]
         L.orc_depth_cloud.restype = None
+        L.orc_viz.argtypes = [f3, ctypes.c_longlong, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_float, ctypes.c_longlong, f3, f3]
+        L.orc_viz.restype = ctypes.c_longlong
         st = ctypes.POINTER(OrcStats)
         L.orc_raycast.argtypes = [G, f3, f3, f3, ctypes.c_int, f3, st, ctypes.c_int]
         L.orc_apply.argtypes = [G, st, ctypes.c_int]
@@ -464,3 +467,15 @@ def depth_cloud(image, intrinsics):
     out = np.empty((h * w, 3), dtype=np.float32)
     L.orc_depth_cloud(img.ctypes.data, enc, w, h, img.strides[0], _fp(K), _fp(out))
     return out
+
+
+def viz(samples_pos, resolution, origin_at_center, step, max_viz_radius, max_points, robot):
+    """(n, 4) float32 x, y, z, rgb of the driver's visualisation cloud."""
+    L = oracle_lib()
+    p = np.ascontiguousarray(np.asarray(samples_pos, dtype=np.float32).reshape(-1, 3))
+    out = np.empty((max(min(p.shape[0], int(max_points)), 1), 4), dtype=np.float32)
+    inv = np.float32(1.0) / np.float32(resolution)
+    k = L.orc_viz(_fp(p), p.shape[0], float(inv), int(bool(origin_at_center)), int(step),
+                  float(max_viz_radius), int(max_points),
+                  (ctypes.c_float * 3)(*[float(v) for v in robot]), _fp(out))
+    return out[:k].copy()

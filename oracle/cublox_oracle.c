@@ -883,3 +883,50 @@ void orc_depth_cloud(const unsigned char *image, int encoding, int width, int he
     }
   }
 }
+
+/* publishOccupancyCloudAsync's loop (main.cpp:763-790) with
+ * occupancyVizDropBySubsample (:71-84), distanceToOccupancyColor (:275-289)
+ * and packRGBFloat (:291-302), on the host's FP32 order. */
+static int orc_host_bin(float p, float inv, int ctr) {
+  if (ctr) {
+    const float s = p < 0.0f ? -1.0f : 1.0f;
+    return (int)(p * inv + s * 0.5f);
+  }
+  return (int)floorf(p * inv);
+}
+
+static float orc_clamp01(float v) { return v < 0.f ? 0.f : (1.f < v ? 1.f : v); }
+
+long long orc_viz(const float *pos, long long n, float inv, int ctr, int step, float d_max,
+                  long long max_points, const float robot[3], float *out) {
+  long long written = 0;
+  for (long long i = 0; i < n && written < max_points; ++i) {
+    const float *q = pos + 3 * i;
+    if (step > 1) {
+      const unsigned mix = (unsigned)orc_host_bin(q[0], inv, ctr) ^
+                           (unsigned)orc_host_bin(q[1], inv, ctr) ^
+                           (unsigned)orc_host_bin(q[2], inv, ctr);
+      if (mix % (unsigned)step != 0u) continue;
+    }
+    const float dx = q[0] - robot[0], dy = q[1] - robot[1], dz = q[2] - robot[2];
+    const float d = sqrtf((dx * dx + dy * dy) + dz * dz);
+    const float dm = d_max < 1.0f ? 1.0f : d_max;
+    const float t = orc_clamp01(d / dm);
+    float r, g, b;
+    if (t <= 0.5f) {
+      const float k = t * 2.0f;
+      r = 0.0f; g = 1.0f - k; b = k;
+    } else {
+      const float k = (t - 0.5f) * 2.0f;
+      r = k; g = 0.0f; b = 1.0f - k;
+    }
+    const unsigned packed = ((unsigned)(orc_clamp01(r) * 255.f) << 16) |
+                            ((unsigned)(orc_clamp01(g) * 255.f) << 8) |
+                            (unsigned)(orc_clamp01(b) * 255.f);
+    float *o = out + 4 * written;
+    o[0] = q[0]; o[1] = q[1]; o[2] = q[2];
+    memcpy(&o[3], &packed, 4);
+    ++written;
+  }
+  return written;
+}

@@ -125,6 +125,11 @@ int orc_ingest(const float *xyz_aos, int n, const float R[9], const float t[3],
 void orc_depth_cloud(const unsigned char *image, int encoding, int width, int height,
                      long long step, const float K[4], float *out_aos);
 
+/* The driver's visualisation cloud of fetch samples (src/main.cpp:740-790):
+ * x, y, z, rgb per kept sample, in sample order.  Returns the count.      */
+long long orc_viz(const float *pos, long long n, float inv, int ctr, int step, float d_max,
+                  long long max_points, const float robot[3], float *out);
+
 /* Raycast of one scan into op/hit (kernels.cu:33-152).  Does not snap the
  * first-run origin and does not apply.  `nthreads` > 1 splits the rays over
  * POSIX threads with relaxed atomic increments.                            */

@@ -163,3 +163,52 @@ def test_update_depth_equals_driver_cloud(enc, where):
     assert a.getOriginIndex() == b.getOriginIndex()
     assert np.array_equal(a.export().view(np.uint32), b.export().view(np.uint32))
     assert a.export().any()
+
+
+# ---------------------------------------------------------------------------
+# visualisation cloud (publishOccupancyCloudAsync, src/main.cpp:740-790)
+# ---------------------------------------------------------------------------
+def numpy_viz(pos, res, step, d_max, max_points, robot):
+    f = np.float32
+    inv = f(1.0) / f(res)
+    gi = np.floor(pos * inv).astype(np.int64).astype(np.uint32)
+    keep = np.ones(pos.shape[0], bool) if step <= 1 else ((gi[:, 0] ^ gi[:, 1] ^ gi[:, 2]) % step) == 0
+    q = pos[keep][:max_points]
+    d = q - np.float32(robot)
+    dist = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+    t = np.clip(dist / max(f(d_max), f(1.0)), f(0), f(1)).astype(np.float32)
+    lo = t <= f(0.5)
+    k = np.where(lo, t * f(2), (t - f(0.5)) * f(2)).astype(np.float32)
+    r = np.where(lo, f(0), k)
+    g = np.where(lo, f(1) - k, f(0))
+    b = np.where(lo, k, f(1) - k)
+    c8 = lambda c: (np.clip(c, 0, 1).astype(np.float32) * f(255)).astype(np.uint32)
+    rgb = ((c8(r) << 16) | (c8(g) << 8) | c8(b)).view(np.float32)
+    return np.concatenate([q, rgb[:, None]], axis=1)
+
+
+def test_oracle_viz_matches_explicit_float32():
+    O.build()
+    rng = np.random.default_rng(4)
+    pos = ((rng.integers(-200, 200, size=(5000, 3)) + np.float32(0.5)) * np.float32(0.1)).astype(np.float32)
+    for step, mp in ((1, 10**6), (3, 10**6), (2, 700)):
+        got = O.viz(pos, 0.1, False, step, 12.0, mp, (0.3, -0.2, 1.8))
+        want = numpy_viz(pos, 0.1, step, 12.0, mp, (0.3, -0.2, 1.8))
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), step
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("step,max_points,flt", [(1, 10**6, None), (3, 10**6, C.VoxelState.OCCUPIED),
+                                                 (2, 500, None)])
+def test_fetch_viz_equals_driver_loop(step, max_points, flt):
+    w = synth.plain_small()
+    g = C.OccupancyGrid(w.half, w.resolution, False, 4.0)
+    g.setLogOddsParams(*C.yaml_log_odds())
+    g.setMaxRaycastRange(w.sensor.max_range)
+    g.update(w.scan(0), w.sensor_origin(0))
+    robot = w.sensor_origin(0)
+    pos, _ = g.fetchOccupancyAround(robot, 3.0, flt)
+    want = O.viz(pos, w.resolution, False, step, 12.0, max_points, robot)
+    got = g.fetch_viz(robot, 3.0, flt, 0, step, 12.0, max_points)
+    assert got.shape[0] == want.shape[0] > 0
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
