@@ -661,6 +661,7 @@ def suite_cublox(args):
         if k >= 1:
             bt.append(t)
     b.close()
+    out["next_rows"] = _next_rows_cublox(stream)
     out["config5_stress"] = {
         "scans": n_scans - 1, "voxel_steps_per_s": float(steps[1:].sum() / (np.sum(upd) / 1e3)),
         "update_recenter_ms_p50": pct(upd, 50), "update_recenter_ms_p99": pct(upd, 99),
@@ -675,6 +676,87 @@ def suite_cublox(args):
                                     "samples_all_states": samples[-1][0],
                                     "samples_occupied": samples[-1][1]}}
     return out
+
+
+def _next_rows_inputs():
+    """A README-scale scan in its sensor frame (yawed pose), a 640x480
+    16-bit depth image and the robot's position, for the driver-side steps."""
+    from cublox_b200 import synth
+    w = synth.readme_scale(2)
+    world, t = w.scan(0), w.sensor_origin(0)
+    yaw = 0.4
+    R = np.array([[np.cos(yaw), -np.sin(yaw), 0], [np.sin(yaw), np.cos(yaw), 0], [0, 0, 1]],
+                 dtype=np.float32)
+    local = ((world.astype(np.float64) - t) @ R.astype(np.float64)).astype(np.float32)
+    rng = np.random.default_rng(5)
+    depth = rng.integers(400, 8000, size=(480, 640)).astype(np.uint16)
+    depth[rng.random((480, 640)) < 0.05] = 0
+    K = np.float32([525.0, 525.0, 319.5, 239.5])
+    return w, local, R, t, depth, K
+
+
+def _next_rows_cublox(stream):
+    import torch
+    import cublox_b200 as C
+    w, local, R, t, depth, K = _next_rows_inputs()
+    g = C.OccupancyGrid(w.half, w.resolution, False, None, stream=stream.cuda_stream)
+    g.setLogOddsParams(*C.yaml_log_odds())
+    g.setMaxRaycastRange(w.sensor.max_range)
+    dl = torch.from_numpy(local).cuda()
+    g.update_pose(dl, R, t)
+    pose_ms = [_time_dev(lambda: g.update_pose(dl, R, t), stream) for _ in range(10)]
+    world = torch.from_numpy(np.ascontiguousarray(
+        (local.astype(np.float64) @ R.T.astype(np.float64) + t).astype(np.float32).T)).cuda()
+    plain_ms = [_time_dev(lambda: g.update(world, t), stream) for _ in range(10)]
+    dd = torch.from_numpy(depth.view(np.int16)).cuda()
+    depth_ms = [_time_dev(lambda: g.update_depth(dd, K, np.eye(3, dtype=np.float32), t), stream)
+                for _ in range(10)]
+    g.fetch_viz(t, 25.0, C.VoxelState.OCCUPIED, 0, 1, 25.0, 200000)
+    t0 = time.perf_counter()
+    for _ in range(10):
+        v = g.fetch_viz(t, 25.0, C.VoxelState.OCCUPIED, 0, 1, 25.0, 200000)
+    viz_ms = (time.perf_counter() - t0) / 10 * 1e3
+    g.close()
+    return {"update_pose_65536_points_ms": float(np.median(pose_ms)),
+            "update_world_cloud_same_scan_ms": float(np.median(plain_ms)),
+            "update_depth_640x480_ms": float(np.median(depth_ms)),
+            "fetch_viz_occupied_r25m_ms": viz_ms, "viz_points": int(v.shape[0]),
+            "note": "device time of update from a sensor-frame cloud (filter + transform fused "
+                    "ahead of the walk) beside update of the same scan already in the world "
+                    "frame; fetch_viz wall time with samples to host"}
+
+
+def _next_rows_reference():
+    """The driver's own host loops for the same steps (restated in the oracle,
+    single thread): buildCloudInOdomFrame, depthCallback, the viz loop."""
+    import oracle as O
+    import cublox_b200 as C
+    w, local, R, t, depth, K = _next_rows_inputs()
+    O.build()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        O.ingest(local, R, t, w.sensor.max_range)
+    ingest_ms = (time.perf_counter() - t0) / 5 * 1e3
+    t0 = time.perf_counter()
+    for _ in range(5):
+        O.depth_cloud(depth, K)
+    depth_ms = (time.perf_counter() - t0) / 5 * 1e3
+    g = C.OccupancyGrid(w.half, w.resolution, False, None)
+    g.setMaxRaycastRange(w.sensor.max_range)
+    g.setLogOddsParams(*C.yaml_log_odds())
+    g.update_pose(local, R, t)
+    pos, _ = g.fetchOccupancyAround(t, 25.0, C.VoxelState.OCCUPIED, 200000)
+    g.close()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        O.viz(pos, w.resolution, False, 1, 25.0, 200000, t)
+    viz_ms = (time.perf_counter() - t0) / 5 * 1e3
+    return {"build_cloud_in_odom_frame_65536_points_ms": ingest_ms,
+            "depth_to_cloud_640x480_ms": depth_ms,
+            "viz_loop_ms": viz_ms, "viz_points_in": int(pos.shape[0]),
+            "kind": "port", "cores": 1,
+            "note": "the reference's driver does these on the host; timed here as their "
+                    "single-threaded CPU restatement (oracle)"}
 
 
 def suite_reference(args):
@@ -694,7 +776,7 @@ def suite_reference(args):
     def soa(p):
         return tuple(np.ascontiguousarray(p[:, a]) for a in range(3))
 
-    out = {}
+    out = {"next_rows": _next_rows_reference()}
     w = synth.plain_small(threshold=1.0)
     pts, s0 = w.scan(0), w.sensor_origin(0)
     r = ref(w.half, w.resolution, 1.0, w.sensor.max_range)

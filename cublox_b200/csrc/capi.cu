@@ -1082,28 +1082,60 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
   }
   std::vector<int> boxes(8 * static_cast<size_t>(nq));
   std::vector<float> r2(nq);
+  std::vector<long long> cand(nq);
+  long long all_cand = 0;
   for (int q = 0; q < nq; ++q) {
     const QueryBox b = plan_query(g, centers + 3 * static_cast<size_t>(q), radius);
     std::memcpy(&boxes[8 * static_cast<size_t>(q)], b.box, sizeof(b.box));
     r2[q] = b.r2;
+    const long long nx = b.box[1] - b.box[0] + 1, ny = b.box[3] - b.box[2] + 1,
+                    nz = b.box[5] - b.box[4] + 1;
+    cand[q] = (nx > 0 && ny > 0 && nz > 0) ? nx * ny * nz : 0;
+    all_cand += cand[q];
   }
+  // about 32 units per SM, never below kFetchMinUnit candidates
+  int sms = 148;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+  }
+  const long long unit = std::max<long long>(kFetchMinUnit, all_cand / (32LL * sms) + 1);
+  std::vector<int> uq;
+  std::vector<long long> ut0;
+  for (int q = 0; q < nq; ++q)
+    for (long long t = 0; t < cand[q]; t += unit) {
+      uq.push_back(q);
+      ut0.push_back(t);
+    }
+  const int nu = static_cast<int>(uq.size());
   const size_t b_cent = sizeof(float) * 3 * nq, b_box = sizeof(int) * 8 * nq,
-               b_r2 = sizeof(float) * nq, b_ll = sizeof(long long) * nq;
+               b_r2 = sizeof(float) * nq, b_uq = sizeof(int) * std::max(nu, 1),
+               b_ll = sizeof(long long) * std::max(nu, 1);
   auto al = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
-  const size_t o_box = al(b_cent), o_r2 = o_box + al(b_box), o_cnt = o_r2 + al(b_r2),
-               o_off = o_cnt + al(b_ll), o_lim = o_off + al(b_ll), total = o_lim + al(b_ll);
+  const size_t o_box = al(b_cent), o_r2 = o_box + al(b_box), o_uq = o_r2 + al(b_r2),
+               o_ut0 = o_uq + al(b_uq), o_cnt = o_ut0 + al(b_ll), o_off = o_cnt + al(b_ll),
+               o_lim = o_off + al(b_ll), total = o_lim + al(b_ll);
   int rc = ensure_fq(g, st, total);
   if (rc) return rc;
   char *base = static_cast<char *>(g->d_fq);
   CK(cudaMemcpyAsync(base, centers, b_cent, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_box, boxes.data(), b_box, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_r2, r2.data(), b_r2, cudaMemcpyHostToDevice, st));
+  if (nu > 0) {
+    CK(cudaMemcpyAsync(base + o_uq, uq.data(), sizeof(int) * nu, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(base + o_ut0, ut0.data(), sizeof(long long) * nu, cudaMemcpyHostToDevice,
+                       st));
+  }
   FetchParams p{};
   p.occ = g->d_occ;
   p.centers = reinterpret_cast<const float *>(base);
   p.qbox = reinterpret_cast<const int *>(base + o_box);
   p.qr2 = reinterpret_cast<const float *>(base + o_r2);
   p.nq = nq;
+  p.uq = reinterpret_cast<const int *>(base + o_uq);
+  p.ut0 = reinterpret_cast<const long long *>(base + o_ut0);
+  p.nu = nu;
+  p.unit = unit;
   for (int a = 0; a < 3; ++a) {
     p.win[a] = g->origin_i[a];
     p.half[a] = g->half[a];
@@ -1122,15 +1154,27 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
   p.err = g->d_err;
   launch_fetch(p, 1, st);
   CK_LAUNCH();
-  std::vector<long long> cnt(nq), off(nq + 1), lim(nq);
-  CK(cudaMemcpyAsync(cnt.data(), p.counts, b_ll, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  std::vector<long long> ucnt(std::max(nu, 1)), uoff(std::max(nu, 1)), ulim(std::max(nu, 1));
+  if (nu > 0) {
+    CK(cudaMemcpyAsync(ucnt.data(), p.counts, sizeof(long long) * nu, cudaMemcpyDeviceToHost,
+                       st));
+    CK(cudaStreamSynchronize(st));
+  }
+  // Per query, its units in order: each keeps what fits under the cap, and
+  // writes after everything its query kept before it.
   const long long cap_q = max_results > 0 ? max_results : 500000;  // OccupancyGrid.cpp:292
+  std::vector<long long> off(nq + 1);
   off[0] = 0;
-  for (int q = 0; q < nq; ++q) {
-    lim[q] = std::min<long long>(cnt[q], cap_q);
-    off[q + 1] = off[q] + lim[q];
-    if (kept) kept[q] = lim[q];
+  for (int u = 0, q = 0; q < nq; ++q) {
+    long long running = 0;
+    for (; u < nu && uq[u] == q; ++u) {
+      uoff[u] = off[q] + std::min(running, cap_q);
+      ulim[u] = std::max(0LL, std::min(ucnt[u], cap_q - running));
+      running += ucnt[u];
+    }
+    const long long lim = std::min(running, cap_q);
+    off[q + 1] = off[q] + lim;
+    if (kept) kept[q] = lim;
   }
   if (offsets)
     for (int q = 0; q <= nq; ++q) offsets[q] = off[q];
@@ -1149,8 +1193,10 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
   if (total_s == 0) return CUBLOX_OK;
   rc = ensure_fout(g, st, total_s);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(base + o_off, off.data(), b_ll, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(base + o_lim, lim.data(), b_ll, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_off, uoff.data(), sizeof(long long) * nu, cudaMemcpyHostToDevice,
+                     st));
+  CK(cudaMemcpyAsync(base + o_lim, ulim.data(), sizeof(long long) * nu, cudaMemcpyHostToDevice,
+                     st));
   p.out_pos = g->d_fpos;
   p.out_state = g->d_fstate;
   launch_fetch(p, 2, st);

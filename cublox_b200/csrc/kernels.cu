@@ -208,7 +208,8 @@ template <int kPass>
 __global__ void __launch_bounds__(256) fetch_kernel(const FetchParams p) {
   __shared__ int warp_tot[8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = blockIdx.x; q < p.nq; q += gridDim.x) {
+  for (int u = blockIdx.x; u < p.nu; u += gridDim.x) {
+    const int q = p.uq[u];
     const int *b = p.qbox + 8 * q;
     const int gx0 = b[0], gy0 = b[2], gz0 = b[4];
     const int nx = b[1] - b[0] + 1, nyy = b[3] - b[2] + 1, nzz = b[5] - b[4] + 1;
@@ -216,12 +217,14 @@ __global__ void __launch_bounds__(256) fetch_kernel(const FetchParams p) {
                         p.centers[3 * q + 2]};
     const float r2 = p.qr2[q];
     long long running = 0;
-    const long long limit = kPass == 2 ? p.limits[q] : 0;
-    const long long base_off = kPass == 2 ? p.offsets[q] : 0;
-    const long long total = (nx > 0 && nyy > 0 && nzz > 0)
-                                ? static_cast<long long>(nx) * nyy * nzz
-                                : 0;
-    for (long long t0 = 0; t0 < total; t0 += blockDim.x) {
+    const long long limit = kPass == 2 ? p.limits[u] : 0;
+    const long long base_off = kPass == 2 ? p.offsets[u] : 0;
+    const long long all = (nx > 0 && nyy > 0 && nzz > 0)
+                              ? static_cast<long long>(nx) * nyy * nzz
+                              : 0;
+    const long long t_begin = p.ut0[u];
+    const long long total = min(all, t_begin + p.unit);  // end of this unit
+    for (long long t0 = t_begin; t0 < total; t0 += blockDim.x) {
       if (kPass == 2 && running >= limit) break;
       const long long t = t0 + threadIdx.x;
       bool keep = false;
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(256) fetch_kernel(const FetchParams p) {
       running += blk;
       __syncthreads();
     }
-    if (kPass == 1 && threadIdx.x == 0) p.counts[q] = running;
+    if (kPass == 1 && threadIdx.x == 0) p.counts[u] = running;
   }
 }
 
@@ -525,8 +528,8 @@ void launch_clear(const ClearParams &p, cudaStream_t s) {
 }
 
 void launch_fetch(const FetchParams &p, int pass, cudaStream_t s) {
-  if (p.nq <= 0) return;
-  int grid = p.nq;
+  if (p.nu <= 0) return;
+  int grid = p.nu;
   const int cap = sm_count() * 8;
   if (grid > cap) grid = cap;
   if (pass == 1)

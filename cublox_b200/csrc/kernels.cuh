@@ -59,21 +59,30 @@ struct ClearParams {
   int x_done;  // marked x slabs are already cleared (contiguous memsets)
 };
 
+// A fetch's candidates are cut into work units of `unit` consecutive
+// candidates of one query (in the query's (x, y, z) order), so that one
+// large sphere spreads over the whole GPU while many small ones stay whole.
+constexpr int kFetchMinUnit = 8192;
+
 struct FetchParams {
   const float *occ;
   const float *centers;  // 3 per query
   const int *qbox;       // 8 ints per query: gx0 gx1 gy0 gy1 gz0 gz1 pad pad
   const float *qr2;      // radius_sq per query
   int nq;
+  const int *uq;             // per unit: its query
+  const long long *ut0;      // per unit: its first candidate
+  int nu;
+  long long unit;            // candidates per unit
   int win[3], half[3], map[3];
   float res;
   int ctr;
   unsigned fp;
   float l_free, l_occ, l_unknown;
   int filter;
-  long long *counts;         // pass 1 output: samples per query
-  const long long *offsets;  // pass 2 input: exclusive scan of kept counts
-  const long long *limits;   // pass 2: samples to keep per query
+  long long *counts;         // pass 1 output: samples per unit
+  const long long *offsets;  // pass 2 input: where each unit's samples go
+  const long long *limits;   // pass 2: samples each unit keeps (the cap)
   float *out_pos;
   uint8_t *out_state;
   uint32_t *err;
