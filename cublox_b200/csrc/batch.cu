@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(1024, kMinCtas) batch_walk_kernel(const MapDes
 // number of maps; next[m] is map m's item counter (zero at launch).
 template <int S>
 __global__ void __launch_bounds__(1024) batch_walk_wq_kernel(const MapDesc *maps,
-                                                             const WalkItem *unused,
+                                                             const WalkItem * /*items*/,
                                                              int *counters, int *next) {
   extern __shared__ uint32_t cube[];
   constexpr int kCube = S * S * S;
@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(256) batch_fold_bulk_kernel(const MapDesc *map
 template <int S>
 __global__ void __launch_bounds__(1024) batch_fused_kernel(const MapDesc *maps,
                                                            const WalkItem *items,
-                                                           const FoldItem *unused,
+                                                           const FoldItem * /*fold items*/,
                                                            int *counters, int *done) {
   extern __shared__ uint32_t cube[];
   __shared__ int s_item, s_ok;

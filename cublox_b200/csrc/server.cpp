@@ -117,7 +117,6 @@ struct cublox_server {
   int64_t next_id = 1;
   int64_t pending = 0;  // requests not yet done
   uint64_t clock = 0;   // use counter for LRU
-  size_t resident_bytes = 0;
   cublox_server_stats stats{};
   bool stop = false;
   std::thread worker, completer, fetcher;
@@ -197,7 +196,8 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
     rc = cublox_grid_create(m.half, m.res, m.ctr, m.has_thr, m.thr, m.origin, s->stream, &m.g);
     if (rc) return rc;
     cublox_grid_set_max_range(m.g, m.max_range);
-    if (m.has_lo) cublox_grid_set_log_odds(m.g, m.lo[0], m.lo[1], m.lo[2], m.lo[3], m.lo[4], m.lo[5]);
+    if (m.has_lo)
+      cublox_grid_set_log_odds(m.g, m.lo[0], m.lo[1], m.lo[2], m.lo[3], m.lo[4], m.lo[5]);
   } else {
     rc = cublox_b200::detail::acquire_device(m.g, m.snapshot.empty() ? nullptr : m.snapshot.data());
     if (rc) return rc;
