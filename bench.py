@@ -905,8 +905,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--only-headline", action="store_true")
-    ap.add_argument("--suite", choices=["headline", "configs"], default="headline",
-                    help="configs: the per-config numbers (1, 3, 4, 5) instead of the headline")
+    ap.add_argument("--suite", choices=["headline", "configs", "plain"], default="headline",
+                    help="configs: the per-config numbers (1, 3, 4, 5) instead of the headline; "
+                         "plain: only the one-map drop-in run")
     ap.add_argument("--stress-scans", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -917,6 +918,17 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
     torch.cuda.set_device(local)
+    if args.suite == "plain":
+        if rank == 0:
+            stream = torch.cuda.Stream()
+            torch.cuda.set_stream(stream)
+            n_steps = args.warmup + args.steps
+            w, scans, origins = readme_batch(1, n_steps)
+            steps = count_steps(w.half, w.resolution, w.sensor.max_range, w.threshold,
+                                [sc[0] for sc in scans], [o[0] for o in origins])
+            hw = {"w": w, "scans": scans, "origins": origins, "steps": steps[:, None]}
+            print(json.dumps({"suite": "plain", **run_plain(args, hw)}), flush=True)
+        return 0
     if args.suite == "configs":
         if rank == 0:
             fn = suite_reference if args.impl == "reference" else suite_cublox

@@ -31,13 +31,13 @@ struct cublox_grid {
   bool stats_on = false;
   // kernel options (cublox_grid_set_option)
   int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
-  int opt_seg = 48;     // split walk: target in-window steps per lane
+  int opt_seg = 64;     // split walk: target in-window steps per lane
   int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
   int opt_block = 512;  // split walk CTA size
   int opt_contig = 1;   // split walk: contiguous segment runs per CTA
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
   int opt_match = 0;    // merge duplicate voxels within a warp
-  int opt_sort = 1;     // walk rays in direction-bin order
+  int opt_sort = 0;     // walk rays in direction-bin order
   void *d_segs = nullptr;  // split walk: segment records
   void *d_rays = nullptr;  // split walk: ray records
   int *d_work = nullptr;   // split walk: 2 counters

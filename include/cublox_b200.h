@@ -91,8 +91,8 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
                                 sensor: 0, 8, 16 or 32 (default 32; 8 is
                                 split walk only)                           */
 #define CUBLOX_OPT_MATCH 3   /* merge duplicate voxels per warp (default 0) */
-#define CUBLOX_OPT_SORT 4    /* walk rays in direction order (default 1)    */
-#define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (48)   */
+#define CUBLOX_OPT_SORT 4    /* walk rays in direction order (default 0)    */
+#define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (64)   */
 #define CUBLOX_OPT_FOLD 6    /* fold sweep: 0 scalar, 1 16-byte (default)   */
 #define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
 #define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
