@@ -547,7 +547,7 @@ size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
   b += sizeof(float) * 3 * (static_cast<size_t>(g->cloud_cap) + static_cast<size_t>(g->world_cap));
   b += g->image_cap;
   b += g->fq_bytes + 13 * static_cast<size_t>(g->fcap) + 13 * static_cast<size_t>(g->qcap);
-  b += static_cast<size_t>(g->split_cap) * (16 * split_seg_bytes() + 64);  // 16 segments a ray
+  b += static_cast<size_t>(g->split_cap) * (16 * split_seg_bytes() + split_ray_bytes());
   b += static_cast<size_t>(g->bin_cap) * 16;
   return b;
 }

@@ -34,7 +34,7 @@ struct cublox_grid {
   int opt_seg = 64;     // split walk: target in-window steps per lane
   int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
   int opt_block = 512;  // split walk CTA size
-  int opt_contig = 1;   // split walk: contiguous segment runs per CTA
+  int opt_contig = 0;   // split walk: contiguous segment runs per CTA
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
   int opt_match = 0;    // merge duplicate voxels within a warp
   int opt_sort = 0;     // walk rays in direction-bin order

@@ -1,17 +1,16 @@
-// Warp-cooperative exact raycast: long rays are split between lanes.
+// Segmented exact raycast: long rays are split between lanes.
 //
 // The reference walks each ray sequentially in one thread (kernels.cu:106-
 // 137), so a scan's latency is set by its longest ray (~900 dependent steps
-// at README scale).  Here a warp takes 32 rays, estimates each one's
-// in-window length, and cuts it into K time segments; every lane then walks
-// one segment.  Bit-exactness:
+// at README scale).  Here each ray's in-window length is estimated and the
+// ray is cut into K time segments of about the same number of steps; every
+// lane then walks one segment.  Bit-exactness:
 //
 //  * The walk is a merge of three per-axis event sequences T_a(j) (the
 //    rounded running sums tM += tD), ordered by (T, axis rank z<y<x) — the
-//    reference's tie rule.  A segment [tau_k, tau_k+1) owns the states
-//    produced by the events with T in that range; its start state is the
-//    one after all events with T < tau_k, which first_at_or_above()
-//    (dda_jump.cuh) computes exactly per axis.
+//    reference's tie rule.  Segment k starts at the state after all events
+//    with T < tau_k, which first_at_or_above() (dda_jump.cuh) computes
+//    exactly per axis, and walks up to the next segment's start state.
 //  * The reference stops at the first state equal to the end voxel, which
 //    can only be state |dx|+|dy|+|dz| (= L1); whether it is reached follows
 //    from comparing the last needed event of every axis with the first
@@ -26,6 +25,7 @@
 #include <cstdint>
 
 #include "dda_jump.cuh"
+#include "far_walk.cuh"
 #include "kernels.cuh"
 #include "ray_walk.cuh"
 
@@ -146,49 +146,31 @@ __device__ bool reaches_end(const RayWalk &w0, const int64_t j0[3], const float 
   return ev_less(need_t, need_r, extra_t, extra_r);
 }
 
-__device__ __forceinline__ int pick_axis(const RayWalk &w) {
-  if (w.tM[0] < w.tM[1]) return w.tM[0] < w.tM[2] ? 0 : 2;
-  return w.tM[1] < w.tM[2] ? 1 : 2;
-}
-
-__device__ __forceinline__ float axis_time(const RayWalk &w, int a) {
-  return a == 0 ? w.tM[0] : (a == 1 ? w.tM[1] : w.tM[2]);
-}
-
-template <int S>
-struct Emitter {
-  const RayParams &p;
-  uint32_t *cube;
-  int clo0, clo1, clo2;
-  uint32_t incs;
-
-  __device__ __forceinline__ void voxel(const RayWalk &w) {
-    const int c0 = w.id[0] - clo0, c1 = w.id[1] - clo1, c2 = w.id[2] - clo2;
-    if (S > 0 && static_cast<unsigned>(c0) < static_cast<unsigned>(S) &&
-        static_cast<unsigned>(c1) < static_cast<unsigned>(S) &&
-        static_cast<unsigned>(c2) < static_cast<unsigned>(S)) {
-      atomicAdd(&cube[(c0 * S + c1) * S + c2], 1u);
-    } else {
-      atomicAdd(p.cnt + walk_hash(w, p), 1u);
-    }
-    ++incs;
-  }
-};
-
 // ---- planned split ------------------------------------------------------
-// Per ray (plan kernel, one thread per ray): the exact setup, the cuts, and
-// every segment's start state, computed by continuing each axis's jump from
-// the previous cut (so each axis's binades are walked once per ray).  Per
-// segment (walk kernel, one lane per segment from a global queue): load the
-// start state and walk until the next cut.
+// A ray's loop states 0, 1, 2, ... are cut at K times tau_1 < ... <
+// tau_{K-1}: segment k owns the states i_k .. i_{k+1} - 1, where i_k counts
+// the events with T < tau_k (i_0 = 0; the last segment runs to the ray's
+// end).  Two launches:
+//   seg_plan_kernel  32 rays per CTA, one warp per axis: the exact set-up
+//                    and the cuts (every warp computes them), then warp a
+//                    follows axis a's event sequence from cut to cut with
+//                    the exact jump of dda_jump.cuh, so each axis's binades
+//                    are walked once per ray, and writes that axis's part of
+//                    every segment record;
+//   seg_walk_kernel  one lane per segment from a queue: walk i_{k+1} - i_k
+//                    loop iterations from the start state, near phase then
+//                    far phase (far_walk.cuh).
+// Segment records: slot r holds ray r's first segment (the one that starts
+// at the sensor and crosses the shared-memory cube); the later segments of
+// all rays follow, so warps of the walk see segments of one kind.
 
-struct SegRec {     // 48 bytes
-  int ray;
-  int i;            // index of the start state
+struct SegRec {     // 64 bytes
+  int ray;          // -1: the ray was dropped (first-segment slots only)
+  int k;            // segment number within the ray
+  int j[3];         // per-axis events before the segment (start state index = sum)
+  int nj[3];        // per-axis events in the segment (-1: last segment)
   int id[3];        // start voxel
   float tM[3];      // per-axis next event times
-  float tau_next;   // the segment owns events with T < tau_next
-  int k;            // segment number within the ray
   int pad[2];
 };
 
@@ -201,97 +183,130 @@ struct RayRec {     // 48 bytes
   int flags;        // bit0 clipped, bit1 state L1 is the end voxel
 };
 
-__global__ void __launch_bounds__(256) seg_plan_kernel(const RayParams p, int seg_len,
-                                                       int max_segs, SegRec *segs,
-                                                       RayRec *rays, int *seg_count,
-                                                       int seg_cap) {
-  __shared__ int warp_tot[8];
-  __shared__ int block_base;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+constexpr int kFlagClipped = 1, kFlagEndsAtL1 = 2;
+constexpr int kPlanRays = 32;
+
+template <typename T>
+__device__ __forceinline__ T pick3(const T (&v)[3], int a) {
+  return a == 0 ? v[0] : (a == 1 ? v[1] : v[2]);
+}
+
+__global__ void __launch_bounds__(3 * kPlanRays) seg_plan_kernel(const RayParams p, int seg_len,
+                                                                 int max_segs, SegRec *segs,
+                                                                 RayRec *rays, int *seg_count,
+                                                                 int seg_cap) {
+  __shared__ int s_base;
+  __shared__ long long s_j[3][kPlanRays];
+  __shared__ float s_s[3][kPlanRays];
+  const int a = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kPlanRays + lane;
   RayWalk w;
   bool valid = false;
   Cuts cuts{0.0f, 0.0f, 0};
-  float ex = 0.0f, ey = 0.0f, ez = 0.0f;
   if (i < p.n) {
     const size_t k = static_cast<size_t>(i) * p.stride;
-    ex = p.x[k];
-    ey = p.y[k];
-    ez = p.z[k];
+    const float ex = p.x[k], ey = p.y[k], ez = p.z[k];
     valid = ray_begin(p, ex, ey, ez, w);
     if (valid) {
       cuts = plan_cuts(p, w, ex, ey, ez, seg_len);
       if (cuts.K > max_segs) cuts.K = max_segs;
     }
   }
-  int K = valid ? cuts.K : 0;
-  // block-wide exclusive scan of K, one global reservation per block
-  int incl = K;
+  // Later segments (k >= 1) of the CTA's rays: one reservation per CTA.
+  const int more = valid ? cuts.K - 1 : 0;
+  int incl = more;
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
     const int v = __shfl_up_sync(0xffffffffu, incl, off);
     if (lane >= off) incl += v;
   }
-  if (lane == 31) warp_tot[warp] = incl;
+  if (threadIdx.x == 31) s_base = atomicAdd(seg_count, incl);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int q = 0; q < static_cast<int>(blockDim.x >> 5); ++q) {
-      const int t = warp_tot[q];
-      warp_tot[q] = run;
-      run += t;
-    }
-    block_base = atomicAdd(seg_count, run);
-  }
-  __syncthreads();
-  int base = block_base + warp_tot[warp] + incl - K;
-  if (!valid) return;
-  if (base + K > seg_cap) {  // never expected: capacity is n * max_segs
+  const int base = p.n + s_base + incl - more;  // record of segment 1
+  if (valid && base + more > seg_cap) {         // never expected: capacity is n * max_segs
     atomicOr(p.err, kErrFetchOverflow);
-    return;
+    valid = false;
   }
+  if (!valid && a == 0 && i < p.n) segs[i].ray = -1;
+  long long jc = 0;
+  float sc = 0.0f;
+  if (valid) {
+    const int st = pick3(w.st, a), id0 = pick3(w.id, a);
+    const float tD = pick3(w.tD, a);
+    sc = pick3(w.tM, a);
+    const int K = cuts.K;
+    for (int k = 0; k < K; ++k) {
+      SegRec *r = segs + (k == 0 ? i : base + k - 1);
+      long long jn = jc;
+      float sn = sc;
+      if (k + 1 < K && st != 0) {
+        const JumpResult q = first_at_or_above(sc, tD, cut_time(cuts, k + 1),
+                                               static_cast<int64_t>(w.max_steps) - jc);
+        if (!q.ok) atomicOr(p.err, kErrJumpStall);  // excluded by plan_cuts
+        jn = jc + q.j;
+        sn = q.s;
+      }
+      if (a == 0) {
+        r->ray = i;
+        r->k = k;
+      }
+      r->j[a] = static_cast<int>(jc);
+      r->nj[a] = k + 1 < K ? static_cast<int>(jn - jc) : -1;
+      r->id[a] = id0 + st * static_cast<int>(jc);
+      r->tM[a] = sc;
+      if (k + 1 < K) {
+        jc = jn;
+        sc = sn;
+      }
+    }
+  }
+  // (jc, sc): axis a at the last cut
+  s_j[a][lane] = jc;
+  s_s[a][lane] = sc;
+  __syncthreads();
+  if (!valid || a != 0) return;
   RayRec rr;
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    rr.en[a] = w.en[a];
-    rr.st[a] = w.st[a];
-    rr.tD[a] = w.tD[a];
+  for (int b = 0; b < 3; ++b) {
+    rr.en[b] = w.en[b];
+    rr.st[b] = w.st[b];
+    rr.tD[b] = w.tD[b];
   }
   rr.max_steps = w.max_steps;
   rr.L1 = abs(w.en[0] - w.id[0]) + abs(w.en[1] - w.id[1]) + abs(w.en[2] - w.id[2]);
-  // segment start states, cut by cut
-  int64_t jc[3] = {0, 0, 0};
-  float sc[3] = {w.tM[0], w.tM[1], w.tM[2]};
-  for (int k = 0; k < K; ++k) {
-    SegRec sr;
-    sr.ray = i;
-    sr.k = k;
-    sr.tau_next = cut_time(cuts, k + 1);
-    int64_t idx = 0;
-    if (k > 0) {
-      const float tau = cut_time(cuts, k);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        if (w.st[a] == 0) continue;
-        const JumpResult r =
-            first_at_or_above(sc[a], w.tD[a], tau, static_cast<int64_t>(w.max_steps) - jc[a]);
-        if (!r.ok) atomicOr(p.err, kErrJumpStall);  // excluded by plan_cuts
-        jc[a] += r.j;
-        sc[a] = r.s;
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      idx += jc[a];
-      sr.id[a] = w.id[a] + w.st[a] * static_cast<int>(jc[a]);
-      sr.tM[a] = sc[a];
-    }
-    sr.i = idx > w.max_steps ? w.max_steps : static_cast<int>(idx);
-    sr.pad[0] = sr.pad[1] = 0;
-    segs[base + k] = sr;
+  bool ends = false;
+  if (cuts.K > 1) {
+    const int64_t j0[3] = {s_j[0][lane], s_j[1][lane], s_j[2][lane]};
+    const float s0[3] = {s_s[0][lane], s_s[1][lane], s_s[2][lane]};
+    ends = reaches_end(w, j0, s0);
   }
-  rr.flags = (w.clipped ? 1 : 0) | ((K > 1 && reaches_end(w, jc, sc)) ? 2 : 0);
+  rr.flags = (w.clipped ? kFlagClipped : 0) | (ends ? kFlagEndsAtL1 : 0);
   rays[i] = rr;
+}
+
+// Near phase of a segment: the exact loop while the voxel is in the cube or
+// outside the window, for at most `budget` iterations.  Returns true if the
+// segment ended in it; false once the walk is in the window and outside the
+// cube (f then holds it).
+template <int S>
+__device__ __forceinline__ bool seg_near(const RayParams &p, uint32_t *cube, const int clo[3],
+                                         RayWalk &w, int i, int &budget, FarWalk &f,
+                                         uint32_t &incs) {
+  for (;; ++i, --budget) {
+    if (budget <= 0 || i >= w.max_steps || at_end(w)) return true;
+    if (in_window(w, p)) {
+      const int c = cube_cell<S>(w.id[0], w.id[1], w.id[2], clo);
+      if (c < 0) {
+        to_far(p, w, i, f);
+        return false;
+      }
+      atomicAdd(&cube[c], 1u);
+      ++incs;
+    } else if (left_for_good(w, p)) {
+      return true;
+    }
+    ray_step(w, p);
+  }
 }
 
 template <int S>
@@ -308,13 +323,13 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
   if (threadIdx.x == 0) cta_next = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int total = *seg_count;
+  const int total = p.n + *seg_count;  // first-segment slots, then later segments
+  const int clo[3] = {cl0, cl1, cl2};
   // contiguous: CTA c owns segments [lo, hi); warps share them via cta_next.
   const int per = (total + gridDim.x - 1) / gridDim.x;
   const int lo = contiguous ? min(total, blockIdx.x * per) : 0;
   const int hi = contiguous ? min(total, lo + per) : total;
-  Emitter<S> em{p, cube, cl0, cl1, cl2, 0u};
-  uint32_t nrays = 0, hits = 0;
+  uint32_t nrays = 0, hits = 0, incs = 0;
   for (;;) {
     int b = 0;
     if (lane == 0) b = contiguous ? lo + atomicAdd(&cta_next, 32) : atomicAdd(work, 32);
@@ -323,7 +338,13 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
     const int g = b + lane;
     if (g >= hi) continue;
     const SegRec sr = segs[g];
+    if (sr.ray < 0) continue;
     const RayRec rr = rays[sr.ray];
+    const int j_sum = sr.j[0] + sr.j[1] + sr.j[2];
+    const int i0 = min(j_sum, rr.max_steps);
+    int budget = sr.nj[0] < 0
+                     ? 0x7fffffff
+                     : min(j_sum + sr.nj[0] + sr.nj[1] + sr.nj[2], rr.max_steps) - i0;
     RayWalk w;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -336,73 +357,17 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
       w.slot[a] = global_to_local(w.id[a], p.map[a], p.half[a]) + p.half[a];
     }
     w.max_steps = rr.max_steps;
-    w.clipped = rr.flags & 1;
-    const bool ends_at_l1 = (rr.flags & 2) != 0;
-    int i = sr.i;
-    bool go = i < w.max_steps;
-    if (sr.k == 0) {
-      ++nrays;
-      if (!go || at_end(w)) {
-        go = false;
-      } else if (in_window(w, p)) {
-        em.voxel(w);
-      } else if (left_for_good(w, p)) {
-        go = false;
-      }
-    }
-    while (go) {
-      const int a = pick_axis(w);
-      if (axis_time(w, a) >= sr.tau_next) break;
-      if (a == 0) {
-        w.id[0] += w.st[0];
-        w.rel[0] += w.st[0];
-        w.slot[0] = wrap_slot(w.slot[0] + w.st[0], p.map[0]);
-        w.tM[0] = fadd(w.tM[0], w.tD[0]);
-      } else if (a == 1) {
-        w.id[1] += w.st[1];
-        w.rel[1] += w.st[1];
-        w.slot[1] = wrap_slot(w.slot[1] + w.st[1], p.map[1]);
-        w.tM[1] = fadd(w.tM[1], w.tD[1]);
-      } else {
-        w.id[2] += w.st[2];
-        w.rel[2] += w.st[2];
-        w.slot[2] = wrap_slot(w.slot[2] + w.st[2], p.map[2]);
-        w.tM[2] = fadd(w.tM[2], w.tD[2]);
-      }
-      ++i;
-      if (i >= w.max_steps) break;
-      // Only state L1 can be the end voxel; past it the walk continues only
-      // if state L1 was not the end (a segment that started past L1 learns
-      // that from the plan).
-      if (i == rr.L1) {
-        if (at_end(w)) break;
-      } else if (i > rr.L1 && sr.i >= rr.L1 && ends_at_l1) {
-        break;
-      }
-      if (in_window(w, p)) {
-        em.voxel(w);
-      } else if (left_for_good(w, p)) {
-        break;
-      }
+    w.clipped = (rr.flags & kFlagClipped) != 0;
+    // A ray whose state L1 is the end voxel stops there: segments past it
+    // have nothing to walk.
+    if (!((rr.flags & kFlagEndsAtL1) && i0 > rr.L1)) {
+      FarWalk f;
+      if (!seg_near<S>(p, cube, clo, w, i0, budget, f, incs)) walk_far(p, f, budget, incs);
     }
     if (sr.k == 0) {
       // Endpoint (kernels.cu:139-151).
-      const int h = end_hash(w, p);
-      if (h >= 0) {
-        const int c0 = w.en[0] - cl0, c1 = w.en[1] - cl1, c2 = w.en[2] - cl2;
-        if (S > 0 && static_cast<unsigned>(c0) < static_cast<unsigned>(S) &&
-            static_cast<unsigned>(c1) < static_cast<unsigned>(S) &&
-            static_cast<unsigned>(c2) < static_cast<unsigned>(S))
-          atomicAdd(&cube[(c0 * S + c1) * S + c2], 1u);
-        else
-          atomicAdd(p.cnt + h, 1u);
-        ++em.incs;
-        if (!w.clipped) {
-          atomicOr(p.cnt + h, kHitFlag);
-          atomicAdd(p.hit + h, 1u);
-          ++hits;
-        }
-      }
+      ++nrays;
+      apply_end<S>(p, cube, ray_end_of<S>(p, w, clo), incs, hits);
     }
   }
   __syncthreads();
@@ -418,7 +383,6 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
     atomicAdd(p.cnt + h, v);
   }
   if (p.stats) {
-    uint32_t incs = em.incs;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       nrays += __shfl_down_sync(0xffffffffu, nrays, off);
@@ -473,7 +437,7 @@ void launch_raycast_split(const RayParams &p, int cube, int seg_len, const Split
                           cudaStream_t s) {
   if (p.n <= 0) return;
   cudaMemsetAsync(sc.counters, 0, 2 * sizeof(int), s);
-  seg_plan_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(
+  seg_plan_kernel<<<(p.n + kPlanRays - 1) / kPlanRays, 3 * kPlanRays, 0, s>>>(
       p, seg_len, sc.max_segs, reinterpret_cast<SegRec *>(sc.segs),
       reinterpret_cast<RayRec *>(sc.rays), sc.counters, sc.seg_cap);
   int clo[3];

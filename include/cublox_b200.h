@@ -96,7 +96,8 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 #define CUBLOX_OPT_FOLD 6    /* fold sweep: 0 scalar, 1 16-byte (default)   */
 #define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
 #define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
-                                   consecutive segments (default 1)         */
+                                   consecutive segments (default 0: all
+                                   CTAs share one segment queue)            */
 int cublox_grid_set_option(cublox_grid *g, int key, int value);
 int cublox_grid_get_option(const cublox_grid *g, int key, int *value);
 

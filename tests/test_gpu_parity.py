@@ -378,14 +378,20 @@ def test_split_walk_many_geometries():
     """The split walk on tiny segments over varied grids, resolutions and
     binnings: every ray is cut at many exact time points."""
     rng = np.random.default_rng(12)
-    for half, res, ctr in [((40, 40, 40), 0.1, False), ((30, 50, 20), 0.07, True),
-                           ((64, 64, 16), 0.05, False), ((25, 25, 25), 0.3, True)]:
+    # the last two put the sensor outside the window: rays enter it late,
+    # so early segments walk nothing in it
+    for half, res, ctr, org in [((40, 40, 40), 0.1, False, (1, -2, 0)),
+                                ((30, 50, 20), 0.07, True, (1, -2, 0)),
+                                ((64, 64, 16), 0.05, False, (1, -2, 0)),
+                                ((25, 25, 25), 0.3, True, (1, -2, 0)),
+                                ((25, 25, 25), 0.1, False, (40, 3, -2)),
+                                ((20, 30, 10), 0.1, True, (-30, -35, 12))]:
         g, o = pair(half, res, ctr=ctr, max_range=float(np.float32(res) * 60))
         g.set_option(C.OPT_RAYCAST, 2)
         g.set_option(C.OPT_SEGMENT, 4)
         s = rng.uniform(-1, 1, 3).astype(np.float32) * np.float32(res) * 3
-        g.set_origin_index((1, -2, 0))
-        o.set_origin_index((1, -2, 0))
+        g.set_origin_index(org)
+        o.set_origin_index(org)
         d = rng.normal(size=(20000, 3))
         d /= np.linalg.norm(d, axis=1, keepdims=True)
         r = rng.uniform(0.01, 1.0, (20000, 1)) * float(np.float32(res) * 90)
