@@ -82,7 +82,21 @@ CBX_HD float f32_scale(float v, int k) {  // v * 2^k, exact while normal
 //   v < 0:  V + F <= -2^23 - [d/u not an integer]   (magnitude >= 2^e)
 // so the number of on-grid steps and the first term >= tau are integer
 // divisions.
-CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax) {
+// The on-grid run of the sum inside one binade that a query ended in:
+// positions S + k*D (in ulps u = 2^(e-23)) for k = 0..m, the value at
+// position S being s at index j, each step adding delta = D*u exactly.  A
+// later query with a larger tau that lands in the same run needs one
+// integer division (stretch_query), not a walk.
+struct JumpStretch {
+  int64_t j;
+  float s, delta;
+  int32_t S, D, m;
+  int e;
+  bool valid;
+};
+
+CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax,
+                                    JumpStretch *stretch = nullptr) {
   JumpResult r{0, s0, true};
   for (int guard = 0; guard < 4096; ++guard) {
     if (r.s >= tau || r.j >= jmax) return r;
@@ -135,12 +149,65 @@ CBX_HD JumpResult first_at_or_above(float s0, float d, float tau, int64_t jmax) 
         kt = -floor_div_pos(-(T - S), D);  // ceil((T - S) / D)
       }
     }
+    if (stretch && kt <= m) *stretch = JumpStretch{r.j, r.s, delta, S, D, m, e, true};
     int64_t k = kt < m ? kt : m;
     if (jmax - r.j < k) k = jmax - r.j;
     r.s = fadd(r.s, fmul(static_cast<float>(k), delta));  // exact
     r.j += k;
   }
   r.ok = false;
+  return r;
+}
+
+// The first j >= the stretch's own index with s_j >= tau, capped at jmax,
+// if tau lies inside the stretch (the same arithmetic as the jump in
+// first_at_or_above); false if it lies beyond, or no stretch is known.
+// The caller has checked that its current s_j is still below tau.
+CBX_HD bool stretch_query(const JumpStretch &st, float tau, int64_t jmax, JumpResult &out) {
+  if (!st.valid || !(tau < 3.4028234e38f)) return false;
+  const float Tf = f32_scale(tau, 23 - st.e);
+  const float hi = static_cast<float>(st.S) + static_cast<float>(st.m) * static_cast<float>(st.D);
+  if (!(Tf <= hi)) return false;
+  int32_t kt = 0;
+  if (Tf > static_cast<float>(st.S)) {
+    const int32_t T = static_cast<int32_t>(ceilf(Tf));
+    kt = -floor_div_pos(-(T - st.S), st.D);  // ceil((T - S) / D)
+  }
+  if (kt > st.m) return false;  // hi rounded past the run's end
+  int64_t k = kt;
+  if (jmax - st.j < k) k = jmax - st.j;
+  out.j = st.j + k;
+  out.s = fadd(st.s, fmul(static_cast<float>(k), st.delta));  // exact
+  out.ok = true;
+  return true;
+}
+
+// Advance a position (j, s = s_j) of the sequence to the first index with
+// s_j >= tau, capped at jmax, for queries with growing tau: a query that
+// lands in the stretch the previous one ended in costs one division, any
+// other walks on with first_at_or_above and records its stretch in st.
+CBX_HD JumpResult advance_to(int64_t j, float s, float d, float tau, int64_t jmax,
+                             JumpStretch &st) {
+  JumpResult r{j, s, true};
+  if (s >= tau || j >= jmax) return r;
+  if (st.valid) {
+    if (stretch_query(st, tau, jmax, r)) return r;
+    // tau lies past the run (its end S + m*D is exact in FP32: |S + m*D| <=
+    // 2^24): continue from the run's last on-grid position.
+    int64_t k = st.m;
+    if (jmax - st.j < k) k = jmax - st.j;
+    if (st.j + k > j) {
+      r.j = st.j + k;
+      r.s = fadd(st.s, fmul(static_cast<float>(k), st.delta));  // exact
+      if (r.s >= tau || r.j >= jmax) return r;
+      j = r.j;
+      s = r.s;
+    }
+  }
+  st.valid = false;
+  r = first_at_or_above(s, d, tau, jmax - j, &st);
+  r.j += j;
+  if (st.valid) st.j += j;
   return r;
 }
 

@@ -114,32 +114,56 @@ __device__ __forceinline__ JumpResult value_from(float t0, float d, int64_t j0, 
 
 // Does the walk's state number L1 (= |dx|+|dy|+|dz|) equal the end voxel?
 // It does iff every event needed to reach the end voxel (the first |D_a|
-// of each axis) precedes, in (T, rank) order, every further event.  (j0,
-// s0) are known positions of each axis's sequence to continue from.
-__device__ bool reaches_end(const RayWalk &w0, const int64_t j0[3], const float s0[3]) {
+// of each axis) precedes, in (T, rank) order, every further event.  Each
+// axis contributes its last needed event and its first extra one
+// (end_events), computed from a known position (j0, s0) of its sequence
+// when that is not past the event, else from the start (tM0); end_combine
+// orders the contributions.
+struct EndEvents {
+  float need_t, extra_t;
+  bool ok;        // false: this axis alone rules the end voxel out
+  bool has_need;  // the axis must step to reach the end voxel
+  bool has_extra; // the axis steps at all
+};
+
+__device__ __forceinline__ EndEvents end_events(int D, int st, float tM0, float tD, int64_t j0,
+                                                float s0) {
+  EndEvents r{-inf_f(), inf_f(), true, false, false};
+  if (D != 0 && (st == 0 || (D > 0) != (st > 0))) {
+    r.ok = false;
+    return r;
+  }
+  if (st == 0) return r;  // never steps: extra events at +inf
+  r.has_extra = true;
+  const int n = abs(D);
+  if (n > 0) {
+    const JumpResult v = value_from(tM0, tD, j0, s0, n - 1);
+    if (!v.ok) {
+      r.ok = false;
+      return r;
+    }
+    r.has_need = true;
+    r.need_t = v.s;
+    r.extra_t = fadd(v.s, tD);
+  } else {
+    r.extra_t = tM0;
+  }
+  return r;
+}
+
+__device__ __forceinline__ bool end_combine(const EndEvents ev[3]) {
   float need_t = -inf_f(), extra_t = inf_f();
   int need_r = -1, extra_r = 3;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int D = w0.en[a] - w0.id[a];
     const int rank = 2 - a;
-    if (D != 0 && (w0.st[a] == 0 || (D > 0) != (w0.st[a] > 0))) return false;
-    const int n = abs(D);
-    if (w0.st[a] == 0) continue;  // never steps: extra events at +inf
-    float tn;
-    if (n > 0) {
-      const JumpResult v = value_from(w0.tM[a], w0.tD[a], j0[a], s0[a], n - 1);
-      if (!v.ok) return false;
-      if (ev_less(need_t, need_r, v.s, rank)) {
-        need_t = v.s;
-        need_r = rank;
-      }
-      tn = fadd(v.s, w0.tD[a]);
-    } else {
-      tn = w0.tM[a];
+    if (!ev[a].ok) return false;
+    if (ev[a].has_need && ev_less(need_t, need_r, ev[a].need_t, rank)) {
+      need_t = ev[a].need_t;
+      need_r = rank;
     }
-    if (ev_less(tn, rank, extra_t, extra_r)) {
-      extra_t = tn;
+    if (ev[a].has_extra && ev_less(ev[a].extra_t, rank, extra_t, extra_r)) {
+      extra_t = ev[a].extra_t;
       extra_r = rank;
     }
   }
@@ -154,9 +178,11 @@ __device__ bool reaches_end(const RayWalk &w0, const int64_t j0[3], const float 
 //   seg_plan_kernel  32 rays per CTA, one warp per axis: the exact set-up
 //                    and the cuts (every warp computes them), then warp a
 //                    follows axis a's event sequence from cut to cut with
-//                    the exact jump of dda_jump.cuh, so each axis's binades
-//                    are walked once per ray, and writes that axis's part of
-//                    every segment record;
+//                    the exact jump of dda_jump.cuh (advance_to: a cut in
+//                    the binade run the previous one ended in costs one
+//                    division), so each axis's binades are walked once per
+//                    ray, and writes that axis's part of every segment
+//                    record;
 //   seg_walk_kernel  one lane per segment from a queue: walk i_{k+1} - i_k
 //                    loop iterations from the start state, near phase then
 //                    far phase (far_walk.cuh).
@@ -164,14 +190,18 @@ __device__ bool reaches_end(const RayWalk &w0, const int64_t j0[3], const float 
 // at the sensor and crosses the shared-memory cube); the later segments of
 // all rays follow, so warps of the walk see segments of one kind.
 
-struct SegRec {     // 64 bytes
+struct SegAxis {    // 16 bytes: one axis of a segment's start, written in one store
+  int j;            // events before the segment (start state index = sum over axes)
+  int nj;           // events in the segment (-1: last segment)
+  int id;           // start voxel coordinate
+  float tM;         // next event time
+};
+
+struct __align__(16) SegRec {  // 64 bytes
   int ray;          // -1: the ray was dropped (first-segment slots only)
   int k;            // segment number within the ray
-  int j[3];         // per-axis events before the segment (start state index = sum)
-  int nj[3];        // per-axis events in the segment (-1: last segment)
-  int id[3];        // start voxel
-  float tM[3];      // per-axis next event times
   int pad[2];
+  SegAxis ax[3];
 };
 
 struct RayRec {     // 48 bytes
@@ -196,8 +226,7 @@ __global__ void __launch_bounds__(3 * kPlanRays) seg_plan_kernel(const RayParams
                                                                  RayRec *rays, int *seg_count,
                                                                  int seg_cap) {
   __shared__ int s_base;
-  __shared__ long long s_j[3][kPlanRays];
-  __shared__ float s_s[3][kPlanRays];
+  __shared__ EndEvents s_end[3][kPlanRays];
   const int a = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kPlanRays + lane;
   RayWalk w;
@@ -234,35 +263,33 @@ __global__ void __launch_bounds__(3 * kPlanRays) seg_plan_kernel(const RayParams
     const int st = pick3(w.st, a), id0 = pick3(w.id, a);
     const float tD = pick3(w.tD, a);
     sc = pick3(w.tM, a);
+    JumpStretch run{};
+    run.valid = false;
     const int K = cuts.K;
     for (int k = 0; k < K; ++k) {
       SegRec *r = segs + (k == 0 ? i : base + k - 1);
       long long jn = jc;
       float sn = sc;
       if (k + 1 < K && st != 0) {
-        const JumpResult q = first_at_or_above(sc, tD, cut_time(cuts, k + 1),
-                                               static_cast<int64_t>(w.max_steps) - jc);
+        const JumpResult q = advance_to(jc, sc, tD, cut_time(cuts, k + 1), w.max_steps, run);
         if (!q.ok) atomicOr(p.err, kErrJumpStall);  // excluded by plan_cuts
-        jn = jc + q.j;
+        jn = q.j;
         sn = q.s;
       }
-      if (a == 0) {
-        r->ray = i;
-        r->k = k;
-      }
-      r->j[a] = static_cast<int>(jc);
-      r->nj[a] = k + 1 < K ? static_cast<int>(jn - jc) : -1;
-      r->id[a] = id0 + st * static_cast<int>(jc);
-      r->tM[a] = sc;
+      if (a == 0) *reinterpret_cast<int2 *>(r) = make_int2(i, k);
+      *reinterpret_cast<int4 *>(&r->ax[a]) =
+          make_int4(static_cast<int>(jc), k + 1 < K ? static_cast<int>(jn - jc) : -1,
+                    id0 + st * static_cast<int>(jc), __float_as_int(sc));
       if (k + 1 < K) {
         jc = jn;
         sc = sn;
       }
     }
   }
-  // (jc, sc): axis a at the last cut
-  s_j[a][lane] = jc;
-  s_s[a][lane] = sc;
+  // (jc, sc): axis a at the last cut; its share of the end test
+  if (valid && cuts.K > 1)
+    s_end[a][lane] = end_events(pick3(w.en, a) - pick3(w.id, a), pick3(w.st, a),
+                                pick3(w.tM, a), pick3(w.tD, a), jc, sc);
   __syncthreads();
   if (!valid || a != 0) return;
   RayRec rr;
@@ -276,9 +303,8 @@ __global__ void __launch_bounds__(3 * kPlanRays) seg_plan_kernel(const RayParams
   rr.L1 = abs(w.en[0] - w.id[0]) + abs(w.en[1] - w.id[1]) + abs(w.en[2] - w.id[2]);
   bool ends = false;
   if (cuts.K > 1) {
-    const int64_t j0[3] = {s_j[0][lane], s_j[1][lane], s_j[2][lane]};
-    const float s0[3] = {s_s[0][lane], s_s[1][lane], s_s[2][lane]};
-    ends = reaches_end(w, j0, s0);
+    const EndEvents ev[3] = {s_end[0][lane], s_end[1][lane], s_end[2][lane]};
+    ends = end_combine(ev);
   }
   rr.flags = (w.clipped ? kFlagClipped : 0) | (ends ? kFlagEndsAtL1 : 0);
   rays[i] = rr;
@@ -340,19 +366,19 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
     const SegRec sr = segs[g];
     if (sr.ray < 0) continue;
     const RayRec rr = rays[sr.ray];
-    const int j_sum = sr.j[0] + sr.j[1] + sr.j[2];
+    const int j_sum = sr.ax[0].j + sr.ax[1].j + sr.ax[2].j;
     const int i0 = min(j_sum, rr.max_steps);
-    int budget = sr.nj[0] < 0
+    int budget = sr.ax[0].nj < 0
                      ? 0x7fffffff
-                     : min(j_sum + sr.nj[0] + sr.nj[1] + sr.nj[2], rr.max_steps) - i0;
+                     : min(j_sum + sr.ax[0].nj + sr.ax[1].nj + sr.ax[2].nj, rr.max_steps) - i0;
     RayWalk w;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      w.id[a] = sr.id[a];
+      w.id[a] = sr.ax[a].id;
       w.en[a] = rr.en[a];
       w.st[a] = rr.st[a];
       w.tD[a] = rr.tD[a];
-      w.tM[a] = sr.tM[a];
+      w.tM[a] = sr.ax[a].tM;
       w.rel[a] = w.id[a] - p.win[a];
       w.slot[a] = global_to_local(w.id[a], p.map[a], p.half[a]) + p.half[a];
     }

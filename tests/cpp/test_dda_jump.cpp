@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <random>
 
 #include "../../cublox_b200/csrc/dda_jump.cuh"
@@ -62,6 +63,38 @@ int main(int argc, char **argv) {
           std::printf("first_at_or_above s0=%a d=%a tau=%a got %lld want %d\n", s0, d, tau,
                       static_cast<long long>(t.j), want);
         ++fails;
+      }
+    }
+    // growing taus through one position, as the split-walk planner asks
+    // them (advance_to and its stretch cache)
+    {
+      float taus[16];
+      for (int q = 0; q < 16; ++q) {
+        const int j = static_cast<int>(U(rng) * n);
+        taus[q] = (q % 3 == 0) ? seq[j]
+                : (q % 3 == 1) ? std::nextafter(seq[j], -INFINITY)
+                               : static_cast<float>(seq[0] + U(rng) * (seq[n] - seq[0]));
+      }
+      std::sort(taus, taus + 16);
+      const int64_t jmax = (c % 5 == 0) ? n / 2 : n;
+      int64_t jc = 0;
+      float sc = s0;
+      JumpStretch st{};
+      st.valid = false;
+      for (int q = 0; q < 16; ++q) {
+        const JumpResult a = advance_to(jc, sc, d, taus[q], jmax, st);
+        if (!a.ok && (a.s + d) == a.s) break;  // stalled sum: left to the caller
+        int want = 0;
+        while (want < jmax && seq[want] < taus[q]) ++want;
+        ++checks;
+        if (!a.ok || a.j != want || a.s != seq[want]) {
+          if (fails < 10)
+            std::printf("advance_to s0=%a d=%a tau=%a got %lld %a want %d %a\n", s0, d,
+                        taus[q], static_cast<long long>(a.j), a.s, want, seq[want]);
+          ++fails;
+        }
+        jc = a.j;
+        sc = a.s;
       }
     }
     delete[] seq;
