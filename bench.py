@@ -426,12 +426,7 @@ def run_serving(args, budget_gb=None, seconds=None):
     # centred at its pose
     pool_steps = [[[count_steps(sw.halves[r], sw.resolution, sw.max_range, None, [p], [o])[0]
                     for (p, o) in cls] for cls in sw.pool[r]] for r in range(sw.n_robots)]
-    # A tick holds at most one 262,144-point scan plus one 65,536-point scan:
-    # a request waits for the tick in flight, so capping the tick bounds the
-    # tail (20 s runs: 65,536-point p99 2.16 ms with a 1M-point cap, 1.94 ms
-    # with this one; fetch p99 3.7 -> 2.7 ms).  Ticks hold ~1 scan on average
-    # at this load either way, so throughput is unchanged.
-    s = C.Server(hbm_budget_bytes=int(budget_gb * (1 << 30)), max_tick_points=3 << 17,
+    s = C.Server(hbm_budget_bytes=int(budget_gb * (1 << 30)), max_tick_points=1 << 20,
                  graphs=True)
     lo = C.yaml_log_odds()
     ids = [s.add_map(sw.halves[r], sw.resolution, False, sw.threshold, max_range=sw.max_range,
