@@ -301,6 +301,32 @@ def test_empty_and_invalid_inputs():
     assert g.first_run()
 
 
+def test_stress_scale_drive_exact():
+    """The largest configuration: 1025x1025x257 voxels at 0.05 m, 262,144-point
+    scans to 100 m, recentering every scan — map and OCCUPIED fetches equal
+    the oracle's after the drive."""
+    sw = synth.stress(5)
+    g, o = pair(sw.half, sw.resolution, thr=sw.threshold, max_range=sw.sensor.max_range)
+    for k in range(5):
+        pts, so = sw.scan(k), sw.sensor_origin(k)
+        g.update(pts, so)
+        g.recenter(so)
+        o.update(pts, so, threads=8)
+        o.recenter(so)
+        assert tuple(g.getOriginIndex()) == tuple(o.origin()[0]), k
+    assert same_bits(g.export(), o.occ())
+    rng = np.random.default_rng(5)
+    org = np.asarray(g.getOriginPosition(), np.float32)
+    cen = (org + rng.uniform(-20, 20, (12, 3)) * np.float32([1, 1, 0.1])).astype(np.float32)
+    off, pos, _ = g.fetch_batch(cen, sw.fetch_radius, C.VoxelState.OCCUPIED)
+    for i in range(len(cen)):
+        p, _, _ = o.fetch(cen[i], sw.fetch_radius, int(C.VoxelState.OCCUPIED))
+        got = np.unique(np.asarray(pos[off[i]:off[i + 1]], np.float32).view(np.uint32), axis=0)
+        want = np.unique(np.asarray(p, np.float32).view(np.uint32), axis=0)
+        assert np.array_equal(got, want), i
+    assert g.check() == 0
+
+
 def test_readme_scale_scan_exact():
     """One full-size 64x1024 scan on the 701x701x151 (74.2M voxel) grid."""
     w = synth.readme_scale(2)
