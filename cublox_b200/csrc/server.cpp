@@ -345,17 +345,26 @@ void worker_loop(cublox_server *s) {
       std::vector<float> sensors;
       size_t floats = 0;
       for (Request *r : ok) floats += r->pts.size();
-      std::vector<float> xyz(floats);
+      // One scan (the usual tick) is passed in place; several are
+      // concatenated into an uninitialised buffer.  Either way the batch
+      // stages the points into pinned memory once.
+      std::unique_ptr<float[]> joined;
+      const float *xyz = ok.size() == 1 ? ok[0]->pts.data() : nullptr;
+      if (!xyz) {
+        joined.reset(new float[floats > 0 ? floats : 1]);
+        xyz = joined.get();
+      }
       size_t at = 0;
       for (Request *r : ok) {
         grids.push_back(s->maps[r->map]->g);
-        std::memcpy(xyz.data() + at, r->pts.data(), r->pts.size() * sizeof(float));
+        if (joined)
+          std::memcpy(joined.get() + at, r->pts.data(), r->pts.size() * sizeof(float));
         at += r->pts.size();
         offsets.push_back(static_cast<int64_t>(at / 3));
         sensors.insert(sensors.end(), r->sensor, r->sensor + 3);
       }
-      int rc = cublox_batch_update(s->batch, static_cast<int>(ok.size()), grids.data(),
-                                   xyz.data(), offsets.data(), sensors.data());
+      int rc = cublox_batch_update(s->batch, static_cast<int>(ok.size()), grids.data(), xyz,
+                                   offsets.data(), sensors.data());
       for (size_t i = 0; !rc && i < ok.size(); ++i) {
         if (!ok[i]->recenter) continue;
         int action = 0;
