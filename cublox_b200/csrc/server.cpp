@@ -49,7 +49,10 @@ struct Request {
   int kind = kScan;
   int map = 0;
   // scan
-  std::vector<float> pts;  // x0 y0 z0 x1 ...
+  std::vector<float> pts;  // x0 y0 z0 x1 ... (when no pinned block was free)
+  float *pin = nullptr;    // or the same in a pinned block of the server's pool
+  int pin_cls = -1;
+  size_t pin_floats = 0;
   float sensor[3] = {0, 0, 0};
   int recenter = 0;
   // fetch
@@ -97,8 +100,58 @@ struct Tick {
 
 }  // namespace
 
+// Pinned host blocks for scan points, reused by size class (64 KiB << c).
+// A scan submitted into one is copied to the device by DMA straight from
+// it, so the worker thread copies nothing for a one-scan tick.  A block
+// returns to the pool when its request ends (its tick's copy has run by
+// then); the pool holds at most kCapBytes, beyond which points stay in
+// pageable memory and the batch stages them.
+struct PinnedPool {
+  static constexpr size_t kMinBytes = size_t(64) << 10;
+  static constexpr size_t kCapBytes = size_t(1) << 30;
+  std::mutex mu;
+  std::vector<std::vector<float *>> free_by_class;
+  std::vector<float *> all;
+  size_t total = 0;
+
+  float *take(size_t bytes, int *cls) {
+    int c = 0;
+    while ((kMinBytes << c) < bytes) ++c;
+    std::lock_guard<std::mutex> lk(mu);
+    if (c < static_cast<int>(free_by_class.size()) && !free_by_class[c].empty()) {
+      float *p = free_by_class[c].back();
+      free_by_class[c].pop_back();
+      *cls = c;
+      return p;
+    }
+    const size_t sz = kMinBytes << c;
+    if (total + sz > kCapBytes) return nullptr;
+    void *p = nullptr;
+    if (cudaMallocHost(&p, sz) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    all.push_back(static_cast<float *>(p));
+    total += sz;
+    *cls = c;
+    return static_cast<float *>(p);
+  }
+  void give(float *p, int c) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (static_cast<int>(free_by_class.size()) <= c) free_by_class.resize(c + 1);
+    free_by_class[c].push_back(p);
+  }
+  void release_all() {
+    for (float *p : all) cudaFreeHost(p);
+    all.clear();
+    free_by_class.clear();
+    total = 0;
+  }
+};
+
 struct cublox_server {
   cublox_server_config cfg{};
+  PinnedPool pinned;  // scan points
   cublox_batch *batch = nullptr;
   cudaStream_t stream = nullptr;
   int device = 0;
@@ -129,7 +182,15 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+const float *pts_data(const Request *r) { return r->pin ? r->pin : r->pts.data(); }
+size_t pts_floats(const Request *r) { return r->pin ? r->pin_floats : r->pts.size(); }
+
 void finish(cublox_server *s, Request *r, int error, const std::string &msg) {
+  if (r->pin) {
+    s->pinned.give(r->pin, r->pin_cls);
+    r->pin = nullptr;
+    r->pin_floats = 0;
+  }
   r->t_done = Clock::now();
   r->error = error;
   r->message = msg;
@@ -296,7 +357,7 @@ void worker_loop(cublox_server *s) {
             m.fetching = true;
             continue;
           }
-          const int64_t n = static_cast<int64_t>(r->pts.size() / 3);
+          const int64_t n = static_cast<int64_t>(pts_floats(r) / 3);
           if (!scans.empty() && (pts + n > s->cfg.max_tick_points ||
                                  (s->cfg.max_tick_maps > 0 &&
                                   static_cast<int>(scans.size()) >= s->cfg.max_tick_maps)))
@@ -344,12 +405,12 @@ void worker_loop(cublox_server *s) {
       std::vector<int64_t> offsets(1, 0);
       std::vector<float> sensors;
       size_t floats = 0;
-      for (Request *r : ok) floats += r->pts.size();
-      // One scan (the usual tick) is passed in place; several are
-      // concatenated into an uninitialised buffer.  Either way the batch
-      // stages the points into pinned memory once.
+      for (Request *r : ok) floats += pts_floats(r);
+      // One scan (the usual tick) is passed in place — from its pinned block
+      // the batch copies it to the device directly; several are
+      // concatenated into an uninitialised buffer, which the batch stages.
       std::unique_ptr<float[]> joined;
-      const float *xyz = ok.size() == 1 ? ok[0]->pts.data() : nullptr;
+      const float *xyz = ok.size() == 1 ? pts_data(ok[0]) : nullptr;
       if (!xyz) {
         joined.reset(new float[floats > 0 ? floats : 1]);
         xyz = joined.get();
@@ -358,8 +419,8 @@ void worker_loop(cublox_server *s) {
       for (Request *r : ok) {
         grids.push_back(s->maps[r->map]->g);
         if (joined)
-          std::memcpy(joined.get() + at, r->pts.data(), r->pts.size() * sizeof(float));
-        at += r->pts.size();
+          std::memcpy(joined.get() + at, pts_data(r), pts_floats(r) * sizeof(float));
+        at += pts_floats(r);
         offsets.push_back(static_cast<int64_t>(at / 3));
         sensors.insert(sensors.end(), r->sensor, r->sensor + 3);
       }
@@ -379,13 +440,20 @@ void worker_loop(cublox_server *s) {
         cudaGetLastError();
         rc = fail(CUBLOX_ERR_CUDA, "server: event record failed");
       }
+      std::string fail_msg;
+      if (rc) {
+        // the failed tick may have queued a copy out of its requests' pinned
+        // blocks: let it run before the blocks go back to the pool
+        fail_msg = cublox_last_error();
+        cudaStreamSynchronize(s->stream);
+        cudaGetLastError();
+      }
       std::lock_guard<std::mutex> lk(s->mu);
       ++s->stats.ticks;
       s->stats.scans += static_cast<int64_t>(ok.size());
       s->stats.points += offsets.back();
       if (rc) {
-        const std::string msg = cublox_last_error();
-        for (Request *r : ok) finish(s, r, rc, msg);
+        for (Request *r : ok) finish(s, r, rc, fail_msg);
         s->cv_done.notify_all();
       } else {
         s->inflight.push_back(Tick{ev, ok});
@@ -517,6 +585,7 @@ int cublox_server_destroy(cublox_server *s) {
   for (auto &m : s->maps)
     if (m->g) cublox_grid_destroy(m->g);
   cublox_batch_destroy(s->batch);
+  s->pinned.release_all();
   cudaStreamDestroy(s->stream);
   cudaStreamDestroy(s->fstream);
   delete s;
@@ -582,7 +651,17 @@ int cublox_server_submit_scan(cublox_server *s, int map_id, const float *xyz, in
   auto r = std::make_unique<Request>();
   r->kind = kScan;
   r->map = map_id;
-  r->pts.assign(xyz, xyz + 3 * static_cast<size_t>(n));
+  const size_t floats = 3 * static_cast<size_t>(n);
+  int cls = -1;
+  float *pin = floats ? s->pinned.take(floats * sizeof(float), &cls) : nullptr;
+  if (pin) {
+    std::memcpy(pin, xyz, floats * sizeof(float));
+    r->pin = pin;
+    r->pin_cls = cls;
+    r->pin_floats = floats;
+  } else {
+    r->pts.assign(xyz, xyz + floats);
+  }
   std::memcpy(r->sensor, sensor_origin, sizeof(r->sensor));
   r->recenter = recenter;
   return submit(s, std::move(r), request_id);
