@@ -334,7 +334,8 @@ int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float re
                           const float log_odds[6], int *map_id);
 /* update(cloud, sensor_origin) (OccupancyGrid.cpp:181-238) on the map, then
  * recenter(sensor_origin) if `recenter`; xyz is x0 y0 z0 x1 ... on the host,
- * copied before the call returns.                                           */
+ * copied before the call returns (into the server's pinned pool, up to
+ * 1 GiB, else pageable memory).                                             */
 int cublox_server_submit_scan(cublox_server *s, int map_id, const float *xyz, int n,
                               const float sensor_origin[3], int recenter,
                               int64_t *request_id);
