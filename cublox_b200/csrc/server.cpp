@@ -114,7 +114,9 @@ struct PinnedPool {
   std::vector<float *> all;
   size_t total = 0;
 
-  float *take(size_t bytes, int *cls) {
+  // `device`: the server's GPU, current during a new allocation (the
+  // calling thread's own current device is put back afterwards).
+  float *take(size_t bytes, int device, int *cls) {
     int c = 0;
     while ((kMinBytes << c) < bytes) ++c;
     std::lock_guard<std::mutex> lk(mu);
@@ -127,7 +129,15 @@ struct PinnedPool {
     const size_t sz = kMinBytes << c;
     if (total + sz > kCapBytes) return nullptr;
     void *p = nullptr;
-    if (cudaMallocHost(&p, sz) != cudaSuccess) {
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    const bool switched = prev >= 0 && prev != device && cudaSetDevice(device) == cudaSuccess;
+    const cudaError_t e = cudaMallocHost(&p, sz);
+    if (switched) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
@@ -653,7 +663,7 @@ int cublox_server_submit_scan(cublox_server *s, int map_id, const float *xyz, in
   r->map = map_id;
   const size_t floats = 3 * static_cast<size_t>(n);
   int cls = -1;
-  float *pin = floats ? s->pinned.take(floats * sizeof(float), &cls) : nullptr;
+  float *pin = floats ? s->pinned.take(floats * sizeof(float), s->device, &cls) : nullptr;
   if (pin) {
     std::memcpy(pin, xyz, floats * sizeof(float));
     r->pin = pin;
