@@ -65,8 +65,9 @@ constexpr int kFoldItemGroups = 1 << 12;  // 16-byte counter groups per fold ite
 // kErrWaitTimeout in the map's error word.
 constexpr int kWaitIters = 1 << 23;
 
-// Near phase.  Returns true if the ray's loop ended in it; false once the
-// walk is inside the window and outside the cube (f then holds it).
+// Near phase of the two-phase walk (far_walk.cuh), from the ray's start.
+// Returns true if the ray's loop ended in it; false once the walk is inside
+// the window and outside the cube (f then holds it).
 template <int S>
 __device__ __forceinline__ bool walk_near(const RayParams &p, uint32_t *cube, const int clo[3],
                                           RayWalk &w, FarWalk &f, uint32_t &incs) {
