@@ -8,8 +8,9 @@ scan (65,536 points, 50 m max range, sigma 0.02 m, seeded scene of a ground
 plane and 400 boxes over +-60 m, robot m at trajectory offset 25 m along a
 circle of radius 25 m at 1.5 m/s, 10 Hz) and recenters with the 4 m
 threshold.  All K scans of a step go through one cublox_batch_update (one
-walk and one fold launch, replayed from a CUDA graph, launch shape chosen by
-the online tuner during warm-up).
+walk and one fold launch, replayed from a CUDA graph; the launch shape is
+chosen by the batch's tuner in a separate pass before warm-up, so no timed
+step runs a candidate shape).
 
 Metric: voxel-steps/s, the reference's own work unit (DDA iterations that
 did not break + 1 endpoint per ray, counted for every scan against the
@@ -22,7 +23,9 @@ window it was integrated in), with p50/p99 per-step latency.
          the last map back (one stream orders every map's work before it)
   --impl reference  the reference's own kernels (oracle/_ref, its
          src/kernels.cu built for sm_100a) on the same K maps, one map after
-         another in its OccupancyGrid call sequence
+         another in its OccupancyGrid call sequence; that process maps no
+         library of this package (its scans and work-unit counts come from
+         oracle/_ref/libcublox_refinputs.so)
 
 Beside the headline (one GPU only): "plain" (one README map through the
 drop-in OccupancyGrid), "batching" (32 maps of 257x257x65 / 401x401x81 /
@@ -168,17 +171,23 @@ def cpu_baseline(w, scans, origins, steps, budget_s=12.0):
 
 
 def profiled_traffic(n_maps: int):
-    """DRAM bytes of one batched step (walk + fold) from the committed ncu
-    launch list of 8 README-scale maps, scaled to n_maps (traffic grows with
-    the maps: each map's fold sweeps its own counters)."""
+    """DRAM bytes of one batched step (walk + fold) per map, from the ncu
+    capture recorded in profiles/traffic.json, scaled to n_maps (each map's
+    walk and fold touch only its own voxels).  Returns (bytes, source)."""
     try:
-        with open(os.path.join(ROOT, "profiles", "batch_walk_fold_batch8_readme.md")) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_step:"):
-                    return float(line.split(":")[1]) * n_maps / 8.0
-    except OSError:
-        pass
-    return None
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return float(t["update_bytes_per_map"]) * n_maps, t.get("source")
+    except (OSError, KeyError, ValueError):
+        return None, None
+
+
+def headline_config(K: int) -> dict:
+    """The headline workload, identical in both arms' lines."""
+    return {"workload": f"batch{K}_readme_701x701x151_64x1024", "maps": K,
+            "grid": [701, 701, 151], "resolution_m": 0.1, "points_per_scan": 65536,
+            "max_range_m": 50.0, "recenter_threshold_m": 4.0,
+            "l2": "flushed between steps (512 MiB write)"}
 
 
 def pct(a, q):
@@ -188,6 +197,26 @@ def pct(a, q):
 # ---------------------------------------------------------------------------
 # headline: batched README-scale maps
 # ---------------------------------------------------------------------------
+def tune_shape(new_batch, dev, sensors, offsets, fixed=-1, max_updates=256):
+    """The launch shape the batch's tuner picks for this workload, from a
+    throw-away batch that integrates the step scans in order (wrapping
+    around) until the tuner has timed every candidate.  Returns (shape,
+    updates the tuner took); a fixed shape (>= 0) is returned as is."""
+    import cublox_b200 as C
+    if fixed >= 0:
+        return fixed, 0
+    b, gs = new_batch(graphs=False)
+    k = 0
+    while b.tuning() and k < max_updates:
+        j = k % len(dev)
+        b.update(gs, dev[j], sensors[j], offsets=offsets[j])
+        b.recenter(gs, sensors[j])
+        k += 1
+    shape = b.get_option(C.BATCH_OPT_SHAPE)
+    b.close()
+    return shape, k
+
+
 def run_headline(args, rank, world, dist):
     import torch
     import cublox_b200 as C
@@ -204,11 +233,11 @@ def run_headline(args, rank, world, dist):
     torch.cuda.set_stream(stream)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
-    def new_batch(graphs=True):
+    def new_batch(graphs=True, shape=None):
         b = C.Batch(stream=stream.cuda_stream)
         b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
-        if args.shape >= 0:
-            b.set_option(C.BATCH_OPT_SHAPE, args.shape)
+        if shape is not None:
+            b.set_option(C.BATCH_OPT_SHAPE, shape)
         gs = []
         for _ in range(K):
             g = b.add_grid(w.half, w.resolution, False, w.threshold)
@@ -223,9 +252,11 @@ def run_headline(args, rank, world, dist):
         off[1:] = np.cumsum([s.shape[0] for s in scans[k]])
         offsets.append(off)
     sensors = [np.stack(origins[k]).astype(np.float32) for k in range(n_steps)]
-    # ---- value: device-resident scans ------------------------------------
     dev = [torch.from_numpy(np.concatenate(scans[k])).cuda() for k in range(n_steps)]
-    b, gs = new_batch()
+    # ---- launch shape: the batch's tuner, in its own pass before warm-up ---
+    shape, tune_updates = tune_shape(new_batch, dev, sensors, offsets, args.shape)
+    # ---- value: device-resident scans ------------------------------------
+    b, gs = new_batch(shape=shape)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(n_steps)]
     actions = []
@@ -249,15 +280,13 @@ def run_headline(args, rank, world, dist):
     own_ms = float(step_ms.sum())
     value = replicas.job_rate(timed_vs, own_ms / 1e3, dist, device="cuda")
     tot_ms = replicas.max_over_ranks(own_ms, dist, device="cuda")
-    shape = b.get_option(C.BATCH_OPT_SHAPE)
+    assert b.get_option(C.BATCH_OPT_SHAPE) == shape and not b.tuning()
     for g in gs:
         assert g.check() == 0, "device error word set"
     b.close()
 
     # ---- kernel split, touched voxels: a separate pass with timing + stats --
-    b, gs = new_batch(graphs=False)
-    b.set_option(C.BATCH_OPT_AUTOTUNE, 0)
-    b.set_option(C.BATCH_OPT_SHAPE, shape)
+    b, gs = new_batch(graphs=False, shape=shape)
     b.set_option(C.BATCH_OPT_TIMING, 1)
     for g in gs:
         g.enable_stats(True)
@@ -278,7 +307,7 @@ def run_headline(args, rank, world, dist):
 
     # ---- e2e: public API from pinned host memory ---------------------------
     pinned = [torch.from_numpy(np.concatenate(scans[k])).pin_memory() for k in range(n_steps)]
-    b, gs = new_batch()
+    b, gs = new_batch(shape=shape)
     wall = []
     for k in range(n_steps):
         flush.zero_()
@@ -302,7 +331,7 @@ def run_headline(args, rank, world, dist):
     return {
         "value": value, "tot_ms": tot_ms, "step_ms": step_ms, "e2e": e2e, "wall": wall,
         "workload": f"batch{K}_readme_701x701x151_64x1024", "K": K, "n_points": n_points,
-        "shape": shape, "walk_ms": walk_ms, "fold_ms": fold_ms, "touched": touched, "incs": incs,
+        "shape": shape, "tune_updates": tune_updates, "walk_ms": walk_ms, "fold_ms": fold_ms, "touched": touched, "incs": incs,
         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "launches": launches,
         "recenters": sum(1 for a in actions if a), "clocks": clk.summary(), "w": w,
         "scans": scans, "origins": origins, "steps": steps,
@@ -378,20 +407,28 @@ def run_batching(args):
     stream = torch.cuda.current_stream()
     assert stream.cuda_stream != 0, "run_headline sets a dedicated stream"
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    b = C.Batch(stream=stream.cuda_stream)
-    b.set_option(C.BATCH_OPT_GRAPHS, 1)
-    gs = []
-    for m in range(bw.n_maps):
-        g = b.add_grid(bw.halves[m], bw.resolution, False, bw.threshold)
-        g.setLogOddsParams(*C.yaml_log_odds())
-        g.setMaxRaycastRange(bw.max_range)
-        gs.append(g)
+
+    def new_batch(graphs=True, shape=None):
+        b = C.Batch(stream=stream.cuda_stream)
+        b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
+        if shape is not None:
+            b.set_option(C.BATCH_OPT_SHAPE, shape)
+        gs = []
+        for m in range(bw.n_maps):
+            g = b.add_grid(bw.halves[m], bw.resolution, False, bw.threshold)
+            g.setLogOddsParams(*C.yaml_log_odds())
+            g.setMaxRaycastRange(bw.max_range)
+            gs.append(g)
+        return b, gs
+
     dev, offs = [], []
     for clouds, _ in data:
         off = np.zeros(bw.n_maps + 1, np.int64)
         off[1:] = np.cumsum([c.shape[0] for c in clouds])
         offs.append(off)
         dev.append(torch.from_numpy(np.concatenate(clouds)).cuda())
+    shape, _ = tune_shape(new_batch, dev, [d[1] for d in data], offs, args.shape)
+    b, gs = new_batch(shape=shape)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in data]
     torch.cuda.synchronize()
     for k in range(n_steps):
@@ -403,7 +440,6 @@ def run_batching(args):
     torch.cuda.synchronize()
     ms = np.asarray([ev[k][0].elapsed_time(ev[k][1]) for k in range(args.warmup, n_steps)])
     vs = int(steps[args.warmup:].sum())
-    shape = b.get_option(C.BATCH_OPT_SHAPE)
     b.close()
     pts = np.mean([o[-1] for o in offs[args.warmup:]])
     return {"workload": bw.name, "maps": bw.n_maps, "steps": args.batch_steps,
@@ -486,59 +522,76 @@ def run_serving(args, budget_gb=None, seconds=None):
 # reference arm
 # ---------------------------------------------------------------------------
 def run_reference(args):
+    """The reference's own kernels (oracle/_ref/libcublox_ref.so) on the
+    headline maps.  Scans and work-unit counts come from
+    oracle/_ref/libcublox_refinputs.so (the same synthesiser source and the
+    oracle's exact step count), so this process maps no library of the
+    product."""
     import oracle as O
-    import cublox_b200 as C
+    from cublox_b200 import synth
+    from cublox_b200 import yaml_log_odds  # pure Python (libm's logf)
 
-    if not O.ref_available():
-        return {"impl": "reference", "unavailable": "reference harness oracle/_ref/libcublox_ref.so "
-                                                     "was not built (needs the reference tree)"}
+    if not (O.ref_available() and os.path.exists(O.REF_INPUTS_SO)):
+        return {"impl": "reference", "unavailable": "reference harness oracle/_ref was not built "
+                                                     "(needs the reference tree)"}
+    synth.use_library(O.REF_INPUTS_SO)
     import torch
     K = args.maps
     n_steps = args.warmup + args.steps
     w, scans, origins = readme_batch(K, n_steps)
-    steps = np.stack([count_steps(w.half, w.resolution, w.sensor.max_range, w.threshold,
-                                  [scans[k][m] for k in range(n_steps)],
-                                  [origins[k][m] for k in range(n_steps)]) for m in range(K)], axis=1)
+    steps = np.asarray([[O.count_steps(scans[k][m], origins[k][m], w.resolution, False,
+                                       w.sensor.max_range, lib_path=O.REF_INPUTS_SO)
+                         for m in range(K)] for k in range(n_steps)], dtype=np.int64)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     refs = []
     for m in range(K):
         r = O.RefGrid(w.half, w.resolution, False, w.threshold)
-        r.set_log_odds(*C.yaml_log_odds())
+        r.set_log_odds(*yaml_log_odds())
         r.set_max_range(w.sensor.max_range)
         refs.append(r)
     soa = [[tuple(np.ascontiguousarray(s[:, a]) for a in range(3)) for s in row] for row in scans]
     wall = []
+    fired = 0
     with Clocks(torch.cuda.current_device()) as clk:
         for k in range(n_steps):
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
+            acts = []
             for m in range(K):
                 refs[m].update(None, origins[k][m], xyz=soa[k][m])
-                refs[m].recenter(origins[k][m])
+                acts.append(refs[m].recenter(origins[k][m]))
             t1 = time.perf_counter()
             if k >= args.warmup:
                 wall.append(t1 - t0)
+                fired += sum(1 for a in acts if not a["host_skip"])
     for r in refs:
         r.close()
     tot = float(np.sum(wall))
     value = int(steps[args.warmup:].sum()) / tot
+    n_points = int(sum(s.shape[0] for s in scans[0]))
+    # the harness's copies, as the reference's OccupancyGrid issues them:
+    # x, y, z (pageable, 4 B each) and the 68-byte RayCastCfg per update; the
+    # 28-byte RecenterResult back per recenter that passes the host gate
+    h2d = 12 * n_points + 68 * K
+    d2h = 28.0 * fired / max(args.steps, 1)
+    loaded = sorted({ln.split()[-1] for ln in open("/proc/self/maps") if ln.rstrip().endswith(".so")
+                     and os.path.realpath(ln.split()[-1]).startswith(ROOT)})
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ray-cast LiDAR scans)", "impl": "reference",
-        "config": {"workload": f"batch{K}_readme_701x701x151_64x1024", "maps": K,
-                   "grid": [701, 701, 151], "resolution_m": 0.1, "points_per_scan": 65536,
-                   "max_range_m": 50.0, "recenter_threshold_m": 4.0,
-                   "form": "reference OccupancyGrid call sequence, one map after another",
-                   "l2": "flushed between steps (512 MiB write)", "parallelism": "single GPU"},
+        "config": headline_config(K),
+        "form": "the reference's OccupancyGrid call sequence (three pageable copies, raycast, "
+                "sync, apply, sync; recenter plan with a D2H round trip), one map after another",
         "p50_ms": pct(wall, 50) * 1e3, "p99_ms": pct(wall, 99) * 1e3,
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": "the reference's src/kernels.cu (sm_100a build) driven by one host "
                                    f"thread in its OccupancyGrid sequence, {args.steps} steps of {K} "
                                    "maps on the B200 (the reference has no CPU path)"},
+        "repo_libraries_mapped": [os.path.relpath(p, ROOT) for p in loaded],
         "clocks": clk.summary(),
     }
 
@@ -956,13 +1009,12 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": h["tot_ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ray-cast LiDAR scans)",
-        "config": {"workload": h["workload"], "maps": h["K"], "grid": [701, 701, 151],
-                   "resolution_m": 0.1, "points_per_scan": 65536, "max_range_m": 50.0,
-                   "recenter_threshold_m": 4.0,
-                   "form": "batched: one walk + one fold launch per step over all maps, CUDA graph "
-                           "replay, launch shape tuned online",
-                   "launch_shape": h["shape"], "l2": "flushed between steps (512 MiB write)",
-                   "parallelism": f"replicas x{world} (map-sharded, no collective)"},
+        "config": headline_config(h["K"]),
+        "form": "batched: one walk + one fold launch per step over all maps, CUDA graph replay",
+        "launch_shape": h["shape"],
+        "tuning": f"separate pass before warm-up ({h['tune_updates']} updates of a throw-away "
+                  "batch); no timed step runs a candidate shape",
+        "parallelism": f"replicas x{world} (map-sharded, no collective)",
         "p50_ms": pct(h["step_ms"], 50), "p99_ms": pct(h["step_ms"], 99),
         "kernel_ms": {"walk": float(np.mean(h["walk_ms"])), "fold": float(np.mean(h["fold_ms"]))},
         "recenters": h["recenters"],
@@ -972,9 +1024,8 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "update = batch walk + batch fold",
                      "achieved": h["achieved"], "peak": h["peak"], "unit": "GB/s",
                      "frac": h["achieved"] / h["peak"], "peak_source": h["peak_kind"],
-                     "traffic": profiled_traffic(h["K"]),
-                     "traffic_source": "profiles/batch_walk_fold_batch8_readme.md (ncu, 8 maps, "
-                                       "scaled by maps), bytes per step",
+                     "traffic": profiled_traffic(h["K"])[0],
+                     "traffic_source": profiled_traffic(h["K"])[1],
                      "algorithmic_bytes": "12 B per point + 8 B per touched voxel (occ read+write); "
                                           "the fold's 4 B/voxel counter sweep is not algorithmic",
                      "atomics_per_s": float(np.mean(h["incs"]) / (np.mean(h["walk_ms"]) / 1e3))},

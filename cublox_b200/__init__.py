@@ -82,6 +82,7 @@ def lib():
         sig = {
             "cublox_last_error": ([], ctypes.c_char_p),
             "cublox_version": ([], ctypes.c_char_p),
+            "cublox_binary_version": ([i], ctypes.c_int),
             "cublox_grid_create": ([i, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_double, f,
                                     ctypes.c_void_p, ctypes.POINTER(G)], ctypes.c_int),
             "cublox_grid_destroy": ([G], ctypes.c_int),
@@ -568,6 +569,7 @@ class OccupancyGrid:
 
 BATCH_OPT_GRAPHS, BATCH_OPT_AUTOTUNE, BATCH_OPT_SHAPE, BATCH_OPT_TIMING, BATCH_OPT_NUM_SHAPES = 1, 2, 3, 4, 5
 BATCH_OPT_FOLD = 6
+BATCH_OPT_TUNING = 7
 
 
 class Batch:
@@ -614,6 +616,10 @@ class Batch:
         v = ctypes.c_int()
         _check(lib().cublox_batch_get_option(self._b, int(key), ctypes.byref(v)), "batch get_option")
         return v.value
+
+    def tuning(self) -> bool:
+        """True while the launch-shape tuner is still timing candidates."""
+        return bool(self.get_option(BATCH_OPT_TUNING))
 
     def update(self, grids, clouds, sensors, offsets=None):
         """One scan into each grid.  `clouds`: a list of (N_i, 3) float32 host
@@ -771,6 +777,14 @@ class Server:
 
 
 _libm = None
+
+
+def binary_version() -> int:
+    """The loaded kernels' binary version on the current device (100 for
+    sm_100a)."""
+    v = ctypes.c_int(0)
+    _check(lib().cublox_binary_version(ctypes.byref(v)), "binary_version")
+    return v.value
 
 
 def logit(p: float) -> float:

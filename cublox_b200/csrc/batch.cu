@@ -872,6 +872,9 @@ int cublox_batch_get_option(const cublox_batch *b, int key, int *value) {
     case CUBLOX_BATCH_OPT_TIMING: *value = b->timed; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_NUM_SHAPES: *value = kNumShapes; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD: *value = b->fold_variant; return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_TUNING:
+      *value = b->autotune && b->tune_step < kNumShapes * b->tune_rounds;
+      return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "batch_get_option: unknown key");

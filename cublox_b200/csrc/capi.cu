@@ -98,7 +98,14 @@ int mem_kind(const void *p) {
 extern "C" {
 
 const char *cublox_last_error(void) { return g_err.c_str(); }
-const char *cublox_version(void) { return "cublox_b200 0.1 (sm_100a)"; }
+const char *cublox_version(void) { return "cublox_b200 0.2 (sm_100a)"; }
+
+int cublox_binary_version(int *binary_version) {
+  if (!binary_version) return fail(CUBLOX_ERR_INVALID, "binary_version: null argument");
+  *binary_version = kernel_binary_version();
+  if (*binary_version < 0) return fail(CUBLOX_ERR_CUDA, "binary_version: no kernel image for this device");
+  return CUBLOX_OK;
+}
 
 static void free_all(cublox_grid *g) {
   cudaFree(g->d_occ);

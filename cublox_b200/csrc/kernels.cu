@@ -495,6 +495,15 @@ void launch_raycast(const RayParams &p, cudaStream_t s) {
     raycast_kernel<false><<<grid, block, 0, s>>>(p);
 }
 
+int kernel_binary_version() {
+  cudaFuncAttributes a{};
+  if (cudaFuncGetAttributes(&a, step_count_kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return a.binaryVersion;
+}
+
 void launch_step_count(const RayParams &p, cudaStream_t s) {
   if (p.n <= 0) return;
   step_count_kernel<<<(p.n + 255) / 256, 256, 0, s>>>(p);

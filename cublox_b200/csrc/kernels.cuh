@@ -130,6 +130,9 @@ void launch_raycast_split(const RayParams &p, int cube, int seg_len, const Split
 // duplicate voxel keys within a warp; sort: walk rays in direction order.
 void launch_raycast_binned(const RayParams &p, const BinnedScratch &b, int cube,
                            bool match, bool sort, cudaStream_t s);
+// The loaded kernels' binary version on the current device (100 for
+// sm_100a), -1 if it cannot be read.
+int kernel_binary_version();
 // Accounting: stats[0] += the reference loop's iterations + 1 per ray.
 void launch_step_count(const RayParams &p, cudaStream_t s);
 void launch_apply(const ApplyParams &p, cudaStream_t s);

@@ -15,6 +15,12 @@
 // each call; every other scratch word is fully overwritten before it is
 // read.  Calls whose GPU work overlaps (different streams, or different host
 // threads, at the same time) race on the scratch and must not be issued.
+//
+// The direction-binned walk and the counter sweep used here have no
+// device-side check that can fail (every index they form is in range by
+// construction), so this entry point reports no device error word: the
+// kernels are given none (RayParams::err is null, and neither kernel
+// dereferences it).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -33,11 +39,11 @@ namespace {
 constexpr int kMaxPoints = CUBLOX_NOALLOC_MAX_POINTS;
 constexpr int kBinsWords = 4096;  // direction bins (binned_bins())
 // Layout: bins[kMaxPoints] | hist[kBinsWords] | cursor[kBinsWords] |
-//         err word (+pad to 16 B) | sorted[3 * kMaxPoints]
+//         sorted[3 * kMaxPoints] (16-byte aligned)
 constexpr size_t kOffHist = sizeof(int) * kMaxPoints;
 constexpr size_t kOffCursor = kOffHist + sizeof(int) * kBinsWords;
-constexpr size_t kOffErr = kOffCursor + sizeof(int) * kBinsWords;
-constexpr size_t kOffSorted = kOffErr + 16;
+constexpr size_t kOffSorted = kOffCursor + sizeof(int) * kBinsWords;
+static_assert(kOffSorted % 16 == 0, "sorted points must start on a 16-byte boundary");
 constexpr size_t kScratchBytes = kOffSorted + sizeof(float) * 3 * kMaxPoints;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -72,16 +78,20 @@ int cublox_integrate_noalloc(const cublox_map_view *map, const float *xyz_soa, i
     return noalloc_fail(CUBLOX_ERR_INVALID, "cublox_integrate_noalloc: null points");
   if (!(map->resolution > 0.0f))
     return noalloc_fail(CUBLOX_ERR_INVALID, "cublox_integrate_noalloc: resolution must be > 0");
+  // 2 * half + 1 per axis and their product, in 64-bit arithmetic: every
+  // factor is checked against int32 before the next multiplication, so no
+  // intermediate can overflow (Grid.cpp:33, :44-50).
   int64_t vnum = 1;
   int mapsz[3];
   for (int a = 0; a < 3; ++a) {
     if (map->half_map_size[a] < 0)
       return noalloc_fail(CUBLOX_ERR_INVALID, "cublox_integrate_noalloc: negative half size");
-    mapsz[a] = 2 * map->half_map_size[a] + 1;
-    vnum *= mapsz[a];
+    const int64_t ms = 2 * static_cast<int64_t>(map->half_map_size[a]) + 1;
+    if (ms > 2147483647 || vnum * ms > 2147483647)
+      return noalloc_fail(CUBLOX_ERR_RANGE, "cublox_integrate_noalloc: voxel count above int32");
+    mapsz[a] = static_cast<int>(ms);
+    vnum *= ms;
   }
-  if (vnum > 2147483647)
-    return noalloc_fail(CUBLOX_ERR_RANGE, "cublox_integrate_noalloc: voxel count above int32");
   if (n == 0) return CUBLOX_OK;
 
   int dev = 0;
@@ -131,7 +141,7 @@ int cublox_integrate_noalloc(const cublox_map_view *map, const float *xyz_soa, i
   p.cnt = map->cnt;
   p.hit = map->hit;
   p.stats = nullptr;
-  p.err = reinterpret_cast<uint32_t *>(base + kOffErr);
+  p.err = nullptr;  // no check on this path can fail (file comment)
 
   BinnedScratch b{reinterpret_cast<int *>(base), reinterpret_cast<int *>(base + kOffHist),
                   reinterpret_cast<int *>(base + kOffCursor),

@@ -42,6 +42,16 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+def use_library(path: str) -> None:
+    """Cast scans with another build of scan_synth.c (same symbols), e.g. one
+    linked into a test harness, instead of libcublox_synth.so.  Call before
+    the first scan."""
+    global _LIB_PATH, _lib
+    if _lib is not None and path != _LIB_PATH:
+        raise RuntimeError("synth: the caster library is already loaded")
+    _LIB_PATH = path
+
+
 def _load():
     global _lib
     if _lib is None:

@@ -47,6 +47,9 @@ typedef struct {
 
 const char *cublox_last_error(void);
 const char *cublox_version(void);
+/* Binary version of this library's kernels as loaded on the current device
+ * (major * 10 + minor: 100 for sm_100a).  No counterpart in the reference.  */
+int cublox_binary_version(int *binary_version);
 
 /* OccupancyGrid(half_map_size_i, resolution, origin_at_center,
  * recenter_threshold, origin)  — OccupancyGrid.hpp:42-45,
@@ -260,6 +263,11 @@ typedef struct cublox_batch cublox_batch;
                                          1: four, 2: one; 3: counters
                                          streamed to shared memory by the
                                          bulk-copy engine                   */
+#define CUBLOX_BATCH_OPT_TUNING 7     /* read only: 1 while the tuner is
+                                         still timing candidate shapes (the
+                                         updates until it reads 0 run
+                                         shapes other than the best, each
+                                         synchronised to be timed)          */
 
 int cublox_batch_create(void *stream, cublox_batch **out);
 int cublox_batch_destroy(cublox_batch *b);
@@ -382,7 +390,10 @@ int cublox_server_get_stats(cublox_server *s, cublox_server_stats *out);
  * array's address up (cudaGetSymbolAddress); make that first call before
  * any stream capture.  All calls share the scratch: calls whose GPU work
  * overlaps in time race and give wrong maps.  Errors: the message is in
- * cublox_noalloc_last_error().                                             */
+ * cublox_noalloc_last_error().  There is no device-side error word: the
+ * kernels of this path form only in-range indices and have no check that
+ * can fail on the device; CUDA launch errors are returned as
+ * CUBLOX_ERR_CUDA.                                                         */
 #define CUBLOX_NOALLOC_MAX_POINTS 262144
 
 typedef struct {

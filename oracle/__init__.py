@@ -21,7 +21,14 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libcublox_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcublox_ref.so")
-REFERENCE_TREE = "/root/reference"
+# The reference arm's inputs: this oracle and the scan synthesiser compiled
+# into one library beside the reference harness, so that a process timing
+# the reference maps no library of the product.
+REF_INPUTS_SO = os.path.join(HERE, "_ref", "libcublox_refinputs.so")
+# The reference tree: $CUBLOX_REFERENCE_TREE, else a directory named
+# `reference` beside the repository.
+REFERENCE_TREE = os.environ.get("CUBLOX_REFERENCE_TREE") or os.path.normpath(
+    os.path.join(HERE, "..", "..", "reference"))
 
 # contraction-site selectors, mirrored from cublox_oracle.h
 SOS_PLAIN, SOS_FY_FZ, SOS_FX_FZ, SOS_P_FZ, SOS_FY_P, SOS_FX_P = range(6)
@@ -53,7 +60,7 @@ def fp_mode(ray_sos=SOS_FX_FZ, clip=False, bound=False, center=True, miss=True, 
 def build(ref: bool | None = None) -> None:
     """Build the oracle (always) and the reference harness (when the
     reference tree is present).  Uses oracle/Makefile."""
-    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle"])
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle", "refinputs"])
     if ref is None:
         ref = os.path.isdir(REFERENCE_TREE)
     if ref:
@@ -84,7 +91,7 @@ class _OrcGrid(ctypes.Structure):
     ]
 
 
-_olib = None
+_olibs: dict = {}
 
 
 def _fp(a):
@@ -95,12 +102,14 @@ def _ip(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
 
 
-def oracle_lib():
-    global _olib
-    if _olib is None:
-        if not os.path.exists(ORACLE_SO):
+def oracle_lib(path: str | None = None):
+    """The oracle's C library: libcublox_oracle.so, or the same code in the
+    reference arm's inputs library (REF_INPUTS_SO)."""
+    path = path or ORACLE_SO
+    if path not in _olibs:
+        if not os.path.exists(path):
             build(ref=False)
-        L = ctypes.CDLL(ORACLE_SO)
+        L = ctypes.CDLL(path)
         G = ctypes.POINTER(_OrcGrid)
         f3 = ctypes.POINTER(ctypes.c_float)
         i3 = ctypes.POINTER(ctypes.c_int)
@@ -146,8 +155,25 @@ def oracle_lib():
         L.orc_fetch_sos.restype = ctypes.c_float
         L.orc_find_trace_diff.argtypes = [G, ctypes.c_uint, ctypes.c_uint, f3, ctypes.c_int, f3, i3,
                                           ctypes.c_int]
-        _olib = L
-    return _olib
+        L.orc_count_steps.argtypes = [ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_uint,
+                                      f3, f3, f3, ctypes.c_int, f3, ctypes.c_int]
+        L.orc_count_steps.restype = ctypes.c_int64
+        _olibs[path] = L
+    return _olibs[path]
+
+
+def count_steps(points, sensor, resolution, origin_at_center=False, max_range=25.0, fp=None,
+                threads=None, lib_path=None) -> int:
+    """The reference's voxel steps of one scan: its loop's iterations that did
+    not break + 1 endpoint per ray it keeps (src/kernels.cu:44-137).  The
+    count does not depend on the window, so no grid is needed."""
+    L = oracle_lib(lib_path)
+    x, y, z = _soa(points)
+    s = (ctypes.c_float * 3)(*[float(v) for v in np.asarray(sensor, np.float32)])
+    return int(L.orc_count_steps(float(np.float32(resolution)), int(origin_at_center),
+                                 float(np.float32(max_range)), FP_PINNED if fp is None else fp,
+                                 _fp(x), _fp(y), _fp(z), len(x), s,
+                                 threads or (os.cpu_count() or 1)))
 
 
 def _soa(points):

@@ -473,6 +473,55 @@ void orc_raycast(orc_grid *g, const float *x, const float *y, const float *z,
   }
 }
 
+/* The reference's work units of one scan (kernels.cu:44-137 iterations that
+ * did not break, + 1 endpoint per ray that was not dropped).  The loop
+ * length does not depend on the window (the window test only decides which
+ * iterations increment a counter), so only the binning, the range clip and
+ * the contraction pattern enter; no grid is needed. */
+int64_t orc_count_steps(float res, int origin_at_center, float max_range, unsigned fp_mode,
+                        const float *x, const float *y, const float *z, int n,
+                        const float sensor[3], int nthreads) {
+  if (n <= 0) return 0;
+  ray_cfg c;
+  memset(&c, 0, sizeof(c));
+  for (int a = 0; a < 3; ++a) {
+    c.o[a] = sensor[a];
+    c.map[a] = 1;
+  }
+  c.res = res;
+  c.inv = 1.0f / res;
+  c.max_range = max_range;
+  c.vnum = 1;
+  c.ctr = origin_at_center;
+  c.fp = fp_mode;
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  if (nthreads > n) nthreads = n;
+  ray_job jobs[256];
+  pthread_t th[256];
+  for (int t = 0; t < nthreads; ++t) {
+    jobs[t].c = &c;
+    jobs[t].x = x;
+    jobs[t].y = y;
+    jobs[t].z = z;
+    jobs[t].lo = (int)((int64_t)n * t / nthreads);
+    jobs[t].hi = (int)((int64_t)n * (t + 1) / nthreads);
+    jobs[t].op = NULL;
+    jobs[t].hit = NULL;
+    jobs[t].atomic = 0;
+    memset(&jobs[t].acc, 0, sizeof(ray_acc));
+  }
+  if (nthreads == 1) {
+    ray_worker(&jobs[0]);
+  } else {
+    for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, ray_worker, &jobs[t]);
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  }
+  int64_t steps = 0;
+  for (int t = 0; t < nthreads; ++t) steps += jobs[t].acc.iters;
+  return steps;
+}
+
 /* ---- apply ------------------------------------------------------------------ */
 typedef struct {
   orc_grid *g;

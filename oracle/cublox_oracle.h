@@ -135,6 +135,12 @@ long long orc_viz(const float *pos, long long n, float inv, int ctr, int step, f
  * POSIX threads with relaxed atomic increments.                            */
 void orc_raycast(orc_grid *g, const float *x, const float *y, const float *z,
                  int n, const float sensor[3], orc_stats *st, int nthreads);
+/* Voxel steps of one scan (the reference loop's iterations that did not
+ * break + 1 endpoint per kept ray), with no grid: the count does not depend
+ * on the window.  res_inv is 1 / res as Grid.cpp computes it.              */
+int64_t orc_count_steps(float res, int origin_at_center, float max_range, unsigned fp_mode,
+                        const float *x, const float *y, const float *z, int n,
+                        const float sensor[3], int nthreads);
 /* Fold counters into occ and zero them (kernels.cu:167-210).               */
 void orc_apply(orc_grid *g, orc_stats *st, int nthreads);
 /* OccupancyGrid::update (OccupancyGrid.cpp:181-238).                       */

@@ -90,4 +90,6 @@ def main(out_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py OUTPUT_DIR")
+    main(sys.argv[1])

@@ -426,3 +426,33 @@ def test_split_walk_many_geometries():
         o.raycast(pts, s)
         assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit()), (half, res, ctr)
         assert g.check() == 0
+
+
+def test_loaded_kernels_are_sm100a():
+    assert C.binary_version() == 100
+
+
+@pytest.mark.parametrize("cfg", ["plain_small", "readme_scale"])
+def test_reference_steps_equal_oracle_count(cfg):
+    """The work unit every voxel-steps/s figure divides by: the GPU count
+    (cublox_grid_reference_steps) equals the oracle's exact count of the
+    reference loop's iterations + 1 endpoint per kept ray, scan by scan, on
+    the plain-small config and on README-scale scans along the trajectory."""
+    if cfg == "plain_small":
+        w = synth.plain_small()
+        idx = [0]
+    else:
+        w = synth.readme_scale(60)
+        idx = [0, 7, 31, 59]
+    g = C.OccupancyGrid(w.half, w.resolution, False, w.threshold)
+    g.setMaxRaycastRange(w.sensor.max_range)
+    for k in idx:
+        pts, so = w.scan(k), w.sensor_origin(k)
+        want = O.count_steps(pts, so, w.resolution, False, w.sensor.max_range)
+        assert g.reference_steps(pts, so) == want, k
+        o = O.OracleGrid(w.half, w.resolution, False, w.threshold,
+                         origin=tuple(float(v) for v in so))
+        o.set_max_range(w.sensor.max_range)
+        if cfg == "plain_small":  # the oracle's own per-scan accounting agrees
+            assert o.raycast(pts, so, threads=8)["voxel_steps"] == want
+    g.close()

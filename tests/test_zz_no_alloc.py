@@ -92,3 +92,43 @@ def test_noalloc_refuses_oversized_clouds():
     rc = fn(ctypes.byref(view), 1, 262145, so, None)
     assert rc == C.ERR_INVALID
     assert b"at most 262144" in L.cublox_noalloc_last_error()
+
+
+def test_noalloc_at_the_point_cap_matches_grid_update():
+    """A cloud of exactly CUBLOX_NOALLOC_MAX_POINTS (262,144) points: four
+    README-scale scans from one pose, concatenated, twice in a row."""
+    import torch
+
+    fn, L = _entry()
+    w = synth.readme_scale(4)
+    pts = np.concatenate([w.scan(k) for k in range(4)]).astype(np.float32)
+    assert pts.shape[0] == 262144
+    sensor = w.sensor_origin(0)
+    lo = C.yaml_log_odds()
+    g = C.OccupancyGrid(w.half, w.resolution, False, None)
+    g.setLogOddsParams(*lo)
+    g.setMaxRaycastRange(w.sensor.max_range)
+    V = g.voxel_num
+    occ = torch.zeros(V, dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(V, dtype=torch.int32, device="cuda")
+    hit = torch.zeros(V, dtype=torch.int32, device="cuda")
+    view = MapView()
+    view.occ, view.cnt, view.hit = occ.data_ptr(), cnt.data_ptr(), hit.data_ptr()
+    view.half_map_size[:] = list(w.half)
+    view.resolution = w.resolution
+    view.origin_at_center = 0
+    view.max_range = w.sensor.max_range
+    view.l_hit, view.l_miss, view.l_min, view.l_max = lo[0], lo[1], lo[2], lo[3]
+    stream = torch.cuda.current_stream().cuda_stream
+    dev = torch.from_numpy(np.ascontiguousarray(pts.T)).cuda()
+    so = (ctypes.c_float * 3)(*[float(v) for v in sensor])
+    for k in range(2):
+        g.update(pts, sensor)
+        if k == 0:
+            view.origin_index[:] = list(g.getOriginIndex())
+        rc = fn(ctypes.byref(view), dev.data_ptr(), pts.shape[0], so, stream)
+        assert rc == 0, L.cublox_noalloc_last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(occ.cpu().numpy().view(np.uint32), g.export().view(np.uint32)), k
+        assert not cnt.any().item() and not hit.any().item()
+    g.close()
