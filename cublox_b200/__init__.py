@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcublox_b200.so")
 
 OK = 0
-ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_RANGE, ERR_DEVICE = -1, -2, -3, -4, -5
+ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_RANGE, ERR_DEVICE, ERR_CANCELLED = -1, -2, -3, -4, -5, -6
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
 DEPTH_U16_MM, DEPTH_F32_M = 0, 1
 OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT, OPT_SEGMENT, OPT_FOLD, OPT_BLOCK, OPT_CONTIGUOUS = (
@@ -51,7 +51,8 @@ class ServerConfig(ctypes.Structure):
     """cublox_server_config."""
     _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_tick_points", ctypes.c_int),
                 ("max_tick_maps", ctypes.c_int), ("max_inflight_ticks", ctypes.c_int),
-                ("graphs", ctypes.c_int)]
+                ("graphs", ctypes.c_int), ("pinned_pool_bytes", ctypes.c_uint64),
+                ("max_fetch_centres", ctypes.c_int), ("max_fetch_samples", ctypes.c_int64)]
 
 
 class ServerStats(ctypes.Structure):
@@ -59,7 +60,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("ticks", ctypes.c_int64), ("scans", ctypes.c_int64), ("fetches", ctypes.c_int64),
                 ("points", ctypes.c_int64), ("admissions", ctypes.c_int64),
                 ("evictions", ctypes.c_int64), ("resident_bytes", ctypes.c_uint64),
-                ("peak_resident_bytes", ctypes.c_uint64), ("resident_maps", ctypes.c_int)]
+                ("peak_resident_bytes", ctypes.c_uint64), ("resident_maps", ctypes.c_int),
+                ("cancelled", ctypes.c_int64)]
 
 
 _lib = None
@@ -155,6 +157,12 @@ def lib():
             "cublox_server_release": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
             "cublox_server_export": ([ctypes.c_void_p, ctypes.c_int, f, i], ctypes.c_int),
             "cublox_server_get_stats": ([ctypes.c_void_p, ctypes.POINTER(ServerStats)], ctypes.c_int),
+            "cublox_server_cancel": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+            "cublox_server_scratch_bytes": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_uint64)],
+                                            ctypes.c_int),
+            "cublox_runtime_counters": ([i64, ctypes.c_int], ctypes.c_int),
+            "cublox_batch_reserve_maps": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int64],
+                                          ctypes.c_int),
             "cublox_grid_enable_timing": ([G, ctypes.c_int], ctypes.c_int),
             "cublox_grid_set_option": ([G, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "cublox_grid_get_option": ([G, ctypes.c_int, i], ctypes.c_int),
@@ -682,9 +690,11 @@ class Server:
     and integrated in continuously formed batches by a worker thread."""
 
     def __init__(self, hbm_budget_bytes: int = 120 << 30, max_tick_points: int = 1 << 20,
-                 max_tick_maps: int = 0, max_inflight_ticks: int = 2, graphs: bool = False):
+                 max_tick_maps: int = 0, max_inflight_ticks: int = 2, graphs: bool = False,
+                 pinned_pool_bytes: int = 0, max_fetch_centres: int = 0, max_fetch_samples: int = 0):
         cfg = ServerConfig(int(hbm_budget_bytes), int(max_tick_points), int(max_tick_maps),
-                           int(max_inflight_ticks), int(bool(graphs)))
+                           int(max_inflight_ticks), int(bool(graphs)), int(pinned_pool_bytes),
+                           int(max_fetch_centres), int(max_fetch_samples))
         self._s = ctypes.c_void_p()
         _check(lib().cublox_server_create(ctypes.byref(cfg), ctypes.byref(self._s)), "Server")
         self.maps = []
@@ -774,6 +784,31 @@ class Server:
         st = ServerStats()
         _check(lib().cublox_server_get_stats(self._s, ctypes.byref(st)), "server stats")
         return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def cancel(self, request_id: int):
+        """Withdraw a request still queued (it ends FAILED, ERR_CANCELLED)."""
+        _check(lib().cublox_server_cancel(self._s, int(request_id)), "cancel")
+
+    @staticmethod
+    def scratch_bytes(max_tick_points: int = 1 << 20, max_fetch_centres: int = 0,
+                      max_fetch_samples: int = 0) -> int:
+        """Device bytes a server holds besides its maps (the least budget)."""
+        cfg = ServerConfig(0, int(max_tick_points), 0, 0, 0, 0, int(max_fetch_centres),
+                           int(max_fetch_samples))
+        v = ctypes.c_uint64()
+        _check(lib().cublox_server_scratch_bytes(ctypes.byref(cfg), ctypes.byref(v)), "scratch_bytes")
+        return v.value
+
+
+COUNTER_NAMES = ("device_allocs", "device_frees", "pinned_allocs", "pinned_frees", "graph_builds")
+
+
+def runtime_counters() -> dict:
+    """Process-wide counts of this library's allocations, frees and CUDA
+    graph builds (cublox_runtime_counters)."""
+    out = (ctypes.c_int64 * len(COUNTER_NAMES))()
+    _check(lib().cublox_runtime_counters(out, len(COUNTER_NAMES)), "runtime_counters")
+    return dict(zip(COUNTER_NAMES, list(out)))
 
 
 _libm = None

@@ -658,9 +658,9 @@ struct cublox_batch {
 namespace {
 
 int ensure_pinned(void **p, size_t bytes) {
-  if (*p) cudaFreeHost(*p);
+  if (*p) cublox_b200::detail::hfree(*p);
   *p = nullptr;
-  if (cudaMallocHost(p, bytes) != cudaSuccess) {
+  if (cublox_b200::detail::hmalloc(p, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(CUBLOX_ERR_NOMEM, "batch: pinned allocation failed");
   }
@@ -668,9 +668,9 @@ int ensure_pinned(void **p, size_t bytes) {
 }
 
 int ensure_dev(void **p, size_t bytes) {
-  cudaFree(*p);
+  cublox_b200::detail::dfree(*p);
   *p = nullptr;
-  if (cudaMalloc(p, bytes) != cudaSuccess) {
+  if (cublox_b200::detail::dmalloc(p, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(CUBLOX_ERR_NOMEM, "batch: device allocation failed");
   }
@@ -784,8 +784,8 @@ int cublox_batch_create(void *stream, cublox_batch **out) {
     }
     b->own_stream = true;
   }
-  if (cudaMalloc(&b->d_counters, sizeof(int) * kCounters) != cudaSuccess ||
-      cudaMallocHost(&b->h_counters, sizeof(int) * kCounters) != cudaSuccess ||
+  if (cublox_b200::detail::dmalloc(&b->d_counters, sizeof(int) * kCounters) != cudaSuccess ||
+      cublox_b200::detail::hmalloc(&b->h_counters, sizeof(int) * kCounters) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     delete b;
@@ -803,17 +803,17 @@ int cublox_batch_destroy(cublox_batch *b) {
   cudaStreamSynchronize(b->stream);
   for (cublox_grid *g : b->grids) cublox_grid_destroy(g);
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  cudaFree(b->d_maps);
-  cudaFree(b->d_witems);
-  cudaFree(b->d_fitems);
-  cudaFree(b->d_counters);
-  cudaFree(b->d_done);
-  cudaFree(b->d_points);
-  if (b->h_maps) cudaFreeHost(b->h_maps);
-  if (b->h_witems) cudaFreeHost(b->h_witems);
-  if (b->h_fitems) cudaFreeHost(b->h_fitems);
-  if (b->h_counters) cudaFreeHost(b->h_counters);
-  if (b->h_points) cudaFreeHost(b->h_points);
+  cublox_b200::detail::dfree(b->d_maps);
+  cublox_b200::detail::dfree(b->d_witems);
+  cublox_b200::detail::dfree(b->d_fitems);
+  cublox_b200::detail::dfree(b->d_counters);
+  cublox_b200::detail::dfree(b->d_done);
+  cublox_b200::detail::dfree(b->d_points);
+  if (b->h_maps) cublox_b200::detail::hfree(b->h_maps);
+  if (b->h_witems) cublox_b200::detail::hfree(b->h_witems);
+  if (b->h_fitems) cublox_b200::detail::hfree(b->h_fitems);
+  if (b->h_counters) cublox_b200::detail::hfree(b->h_counters);
+  if (b->h_points) cublox_b200::detail::hfree(b->h_points);
   if (b->staged) cudaEventDestroy(b->staged);
   for (int i = 0; i < 4; ++i)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
@@ -1032,6 +1032,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
         return cuda_fail(le, (std::string("batch graph capture: ") + what).c_str(), __LINE__);
       if (e != cudaSuccess) return cuda_fail(e, "batch graph end capture", __LINE__);
       e = cudaGraphInstantiate(&b->graph, gr, 0);
+      detail::count(detail::kGraphBuilds);
       cudaGraphDestroy(gr);
       if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate", __LINE__);
       b->graph_shape = active_shape;
@@ -1068,7 +1069,24 @@ int cublox_batch_reserve(cublox_batch *b, int64_t points, int maps) {
   int rc = reserve_points(b, 3 * static_cast<size_t>(points));
   if (rc) return rc;
   const int items = maps + static_cast<int>(points / 256) + 1;
-  return ensure_capacity(b, std::max(maps, 1), items, maps * 64 + 1);
+  return ensure_capacity(b, std::max(maps, 1), items + maps * 64, maps * 64 + 1);
+}
+
+int cublox_batch_reserve_maps(cublox_batch *b, int64_t points, int maps, int64_t voxels) {
+  if (!b || points < 0 || maps < 0 || voxels < 0)
+    return fail(CUBLOX_ERR_INVALID, "batch_reserve_maps: bad argument");
+  if (cudaEventSynchronize(b->staged) != cudaSuccess) cudaGetLastError();
+  int rc = reserve_points(b, 3 * static_cast<size_t>(points));
+  if (rc) return rc;
+  // fold items: per map ceil(voxels / 4 / groups per item) + 1 (the tail
+  // item); walk items: at least 256 rays each (every shape), one partial
+  // item per map, and a fused shape queues the fold items behind them
+  const int64_t folds = voxels / (4 * static_cast<int64_t>(kFoldItemGroups)) + 2 * maps + 1;
+  const int64_t walks = points / 256 + maps + 1;
+  if (folds + walks > (int64_t(1) << 30))
+    return fail(CUBLOX_ERR_INVALID, "batch_reserve_maps: too many work items");
+  return ensure_capacity(b, std::max(maps, 1), static_cast<int>(walks + folds),
+                         static_cast<int>(folds));
 }
 
 int cublox_batch_recenter(cublox_batch *b, int n, cublox_grid *const *grids,

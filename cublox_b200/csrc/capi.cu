@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -23,10 +24,35 @@ using namespace cublox_b200;
 
 namespace {
 thread_local std::string g_err;
+std::atomic<int64_t> g_counters[cublox_b200::detail::kNumCounters];
 }  // namespace
 
 namespace cublox_b200 {
 namespace detail {
+void count(Counter c) { g_counters[c].fetch_add(1, std::memory_order_relaxed); }
+
+cudaError_t dev_alloc(void **p, size_t bytes) {
+  count(kDevAllocs);
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t dev_free(void *p) {
+  if (!p) return cudaSuccess;
+  count(kDevFrees);
+  return cudaFree(p);
+}
+
+cudaError_t pinned_alloc(void **p, size_t bytes) {
+  count(kPinnedAllocs);
+  return cudaMallocHost(p, bytes);
+}
+
+cudaError_t pinned_free(void *p) {
+  if (!p) return cudaSuccess;
+  count(kPinnedFrees);
+  return cudaFreeHost(p);
+}
+
 int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
@@ -100,6 +126,13 @@ extern "C" {
 const char *cublox_last_error(void) { return g_err.c_str(); }
 const char *cublox_version(void) { return "cublox_b200 0.2 (sm_100a)"; }
 
+int cublox_runtime_counters(int64_t *out, int n) {
+  if (!out || n < 0) return fail(CUBLOX_ERR_INVALID, "runtime_counters: bad argument");
+  for (int i = 0; i < n; ++i)
+    out[i] = i < cublox_b200::detail::kNumCounters ? g_counters[i].load() : 0;
+  return CUBLOX_OK;
+}
+
 int cublox_binary_version(int *binary_version) {
   if (!binary_version) return fail(CUBLOX_ERR_INVALID, "binary_version: null argument");
   *binary_version = kernel_binary_version();
@@ -108,31 +141,30 @@ int cublox_binary_version(int *binary_version) {
 }
 
 static void free_all(cublox_grid *g) {
-  cudaFree(g->d_occ);
-  cudaFree(g->d_cnt);
-  cudaFree(g->d_hit);
-  cudaFree(g->d_stats);
-  cudaFree(g->d_err);
-  cudaFree(g->d_masks);
-  if (g->h_masks) cudaFreeHost(g->h_masks);
-  if (g->mask_ev) cudaEventDestroy(g->mask_ev);
-  cudaFree(g->d_cloud);
-  cudaFree(g->d_world);
-  cudaFree(g->d_kept);
-  cudaFree(g->d_image);
-  cudaFree(g->d_bins);
-  cudaFree(g->d_work);
-  cudaFree(g->d_segs);
-  cudaFree(g->d_rays);
-  cudaFree(g->d_hist);
-  cudaFree(g->d_sorted);
-  cudaFree(g->d_fq);
-  cudaFree(g->d_fpos);
-  cudaFree(g->d_fstate);
-  cudaFree(g->d_qout);
-  cudaFree(g->d_qin);
+  cublox_b200::detail::dfree(g->d_occ);
+  cublox_b200::detail::dfree(g->d_cnt);
+  cublox_b200::detail::dfree(g->d_hit);
+  cublox_b200::detail::dfree(g->d_stats);
+  cublox_b200::detail::dfree(g->d_err);
+  cublox_b200::detail::dfree(g->d_masks);
+  if (g->h_masks) cublox_b200::detail::hfree(g->h_masks);
+  for (cudaEvent_t e : g->mask_ev)
+    if (e) cudaEventDestroy(e);
+  cublox_b200::detail::dfree(g->d_cloud);
+  cublox_b200::detail::dfree(g->d_world);
+  cublox_b200::detail::dfree(g->d_kept);
+  cublox_b200::detail::dfree(g->d_image);
+  cublox_b200::detail::dfree(g->d_bins);
+  cublox_b200::detail::dfree(g->d_work);
+  cublox_b200::detail::dfree(g->d_segs);
+  cublox_b200::detail::dfree(g->d_rays);
+  cublox_b200::detail::dfree(g->d_hist);
+  cublox_b200::detail::dfree(g->d_sorted);
+  cublox_b200::detail::free_fetch(&g->fs);
+  cublox_b200::detail::dfree(g->d_qout);
+  cublox_b200::detail::dfree(g->d_qin);
   for (int i = 0; i < 2; ++i) {
-    if (g->h_stage[i]) cudaFreeHost(g->h_stage[i]);
+    if (g->h_stage[i]) cublox_b200::detail::hfree(g->h_stage[i]);
     if (g->stage_ev[i]) cudaEventDestroy(g->stage_ev[i]);
   }
   for (int i = 0; i < 6; ++i)
@@ -215,17 +247,23 @@ int cublox_grid_create(const int half_map_size[3], float resolution,
     g->own_stream = true;
   }
   const size_t n = static_cast<size_t>(g->voxel_num);
-  if ((e = cudaMalloc(&g->d_occ, n * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc occ");
-  if ((e = cudaMalloc(&g->d_cnt, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc cnt");
-  if ((e = cudaMalloc(&g->d_hit, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc hit");
-  if ((e = cudaMalloc(&g->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "cudaMalloc stats");
-  if ((e = cudaMalloc(&g->d_err, sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc err");
+  if ((e = cublox_b200::detail::dmalloc(&g->d_occ, n * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc occ");
+  if ((e = cublox_b200::detail::dmalloc(&g->d_cnt, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc cnt");
+  if ((e = cublox_b200::detail::dmalloc(&g->d_hit, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc hit");
+  if ((e = cublox_b200::detail::dmalloc(&g->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "cudaMalloc stats");
+  if ((e = cublox_b200::detail::dmalloc(&g->d_err, sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc err");
   int words = 0;
   for (int a = 0; a < 3; ++a) {
     g->mask_words[a] = (g->map[a] + 31) / 32;
     words += g->mask_words[a];
   }
-  if ((e = cudaMalloc(&g->d_masks, words * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc masks");
+  if ((e = cublox_b200::detail::dmalloc(&g->d_masks, words * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc masks");
+  // pinned staging of the recenter masks, two halves used in turn
+  g->mask_stage_words = words;
+  if ((e = cublox_b200::detail::hmalloc(&g->h_masks, 2 * words * sizeof(uint32_t))) != cudaSuccess) return bail(e, "pinned masks");
+  for (int i = 0; i < 2; ++i)
+    if ((e = cudaEventCreateWithFlags(&g->mask_ev[i], cudaEventDisableTiming)) != cudaSuccess)
+      return bail(e, "mask event");
   if ((e = cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream)) != cudaSuccess) return bail(e, "memset occ");
   if ((e = cudaMemsetAsync(g->d_cnt, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess) return bail(e, "memset cnt");
   if ((e = cudaMemsetAsync(g->d_hit, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess) return bail(e, "memset hit");
@@ -360,10 +398,10 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode) {
 static int ensure_cloud(cublox_grid *g, int n) {
   if (n <= g->cloud_cap) return CUBLOX_OK;
   CK(cudaStreamSynchronize(g->stream));
-  cudaFree(g->d_cloud);
+  cublox_b200::detail::dfree(g->d_cloud);
   g->d_cloud = nullptr;
   g->cloud_cap = 0;
-  cudaError_t e = cudaMalloc(&g->d_cloud, sizeof(float) * 3 * static_cast<size_t>(n));
+  cudaError_t e = cublox_b200::detail::dmalloc(&g->d_cloud, sizeof(float) * 3 * static_cast<size_t>(n));
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update: cloud buffer allocation failed");
@@ -376,12 +414,12 @@ static int ensure_stage(cublox_grid *g, int n) {
   if (n <= g->stage_cap) return CUBLOX_OK;
   for (int i = 0; i < 2; ++i) {
     if (g->stage_ev[i]) CK(cudaEventSynchronize(g->stage_ev[i]));
-    if (g->h_stage[i]) cudaFreeHost(g->h_stage[i]);
+    if (g->h_stage[i]) cublox_b200::detail::hfree(g->h_stage[i]);
     g->h_stage[i] = nullptr;
   }
   g->stage_cap = 0;
   for (int i = 0; i < 2; ++i) {
-    cudaError_t e = cudaMallocHost(&g->h_stage[i], sizeof(float) * 3 * static_cast<size_t>(n));
+    cudaError_t e = cublox_b200::detail::hmalloc(&g->h_stage[i], sizeof(float) * 3 * static_cast<size_t>(n));
     if (e != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update: pinned staging allocation failed");
@@ -422,17 +460,17 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   p.err = g->d_err;
   if ((g->opt_raycast == 1 || (g->opt_raycast == 2 && g->opt_sort)) && n > g->bin_cap) {
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(g->d_bins);
-    cudaFree(g->d_sorted);
+    cublox_b200::detail::dfree(g->d_bins);
+    cublox_b200::detail::dfree(g->d_sorted);
     g->d_bins = nullptr;
     g->d_sorted = nullptr;
     g->bin_cap = 0;
-    if (!g->d_hist && cudaMalloc(&g->d_hist, sizeof(int) * 2 * binned_bins()) != cudaSuccess) {
+    if (!g->d_hist && cublox_b200::detail::dmalloc(&g->d_hist, sizeof(int) * 2 * binned_bins()) != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "update: bin buffer allocation failed");
     }
-    if (cudaMalloc(&g->d_bins, sizeof(int) * static_cast<size_t>(n)) != cudaSuccess ||
-        cudaMalloc(&g->d_sorted, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
+    if (cublox_b200::detail::dmalloc(&g->d_bins, sizeof(int) * static_cast<size_t>(n)) != cudaSuccess ||
+        cublox_b200::detail::dmalloc(&g->d_sorted, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "update: sort buffer allocation failed");
     }
@@ -455,15 +493,15 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   constexpr int kMaxSegsPerRay = 16;
   if (g->opt_raycast == 2 && (n > g->split_cap || !g->d_work)) {
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(g->d_segs);
-    cudaFree(g->d_rays);
+    cublox_b200::detail::dfree(g->d_segs);
+    cublox_b200::detail::dfree(g->d_rays);
     g->d_segs = nullptr;
     g->d_rays = nullptr;
     g->split_cap = 0;
-    if ((!g->d_work && cudaMalloc(&g->d_work, 2 * sizeof(int)) != cudaSuccess) ||
-        cudaMalloc(&g->d_segs, split_seg_bytes() * kMaxSegsPerRay * static_cast<size_t>(n)) !=
+    if ((!g->d_work && cublox_b200::detail::dmalloc(&g->d_work, 2 * sizeof(int)) != cudaSuccess) ||
+        cublox_b200::detail::dmalloc(&g->d_segs, split_seg_bytes() * kMaxSegsPerRay * static_cast<size_t>(n)) !=
             cudaSuccess ||
-        cudaMalloc(&g->d_rays, split_ray_bytes() * static_cast<size_t>(n)) != cudaSuccess) {
+        cublox_b200::detail::dmalloc(&g->d_rays, split_ray_bytes() * static_cast<size_t>(n)) != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "update: split-walk scratch allocation failed");
     }
@@ -553,7 +591,7 @@ size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
   size_t b = 12 * static_cast<size_t>(g->d_occ ? g->voxel_num : 0);
   b += sizeof(float) * 3 * (static_cast<size_t>(g->cloud_cap) + static_cast<size_t>(g->world_cap));
   b += g->image_cap;
-  b += g->fq_bytes + 13 * static_cast<size_t>(g->fcap) + 13 * static_cast<size_t>(g->qcap);
+  b += g->fs.fq_bytes + 13 * static_cast<size_t>(g->fs.fcap) + 13 * static_cast<size_t>(g->qcap);
   b += static_cast<size_t>(g->split_cap) * (16 * split_seg_bytes() + split_ray_bytes());
   b += static_cast<size_t>(g->bin_cap) * 16;
   return b;
@@ -565,9 +603,9 @@ int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
     e = cudaMemcpy(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->voxel_num),
                    cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "release_device", __LINE__);
-  cudaFree(g->d_occ);
-  cudaFree(g->d_cnt);
-  cudaFree(g->d_hit);
+  cublox_b200::detail::dfree(g->d_occ);
+  cublox_b200::detail::dfree(g->d_cnt);
+  cublox_b200::detail::dfree(g->d_hit);
   g->d_occ = nullptr;
   g->d_cnt = g->d_hit = nullptr;
   return release_scratch(g);
@@ -576,39 +614,37 @@ int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
 int cublox_b200::detail::release_scratch(cublox_grid *g) {
   const cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "release_scratch", __LINE__);
-  cudaFree(g->d_world);
+  cublox_b200::detail::dfree(g->d_world);
   g->d_world = nullptr;
   g->world_cap = 0;
-  cudaFree(g->d_image);
+  cublox_b200::detail::dfree(g->d_image);
   g->d_image = nullptr;
   g->image_cap = 0;
   void **bufs[] = {reinterpret_cast<void **>(&g->d_cloud), reinterpret_cast<void **>(&g->d_bins),
                    reinterpret_cast<void **>(&g->d_work),  reinterpret_cast<void **>(&g->d_segs),
                    reinterpret_cast<void **>(&g->d_rays),  reinterpret_cast<void **>(&g->d_hist),
-                   reinterpret_cast<void **>(&g->d_sorted), reinterpret_cast<void **>(&g->d_fq),
-                   reinterpret_cast<void **>(&g->d_fpos),  reinterpret_cast<void **>(&g->d_fstate),
+                   reinterpret_cast<void **>(&g->d_sorted),
                    reinterpret_cast<void **>(&g->d_qout),  reinterpret_cast<void **>(&g->d_qin)};
   for (void **b : bufs) {
-    cudaFree(*b);
+    cublox_b200::detail::dfree(*b);
     *b = nullptr;
   }
   g->cloud_cap = g->split_cap = g->bin_cap = g->qcap = 0;
-  g->fcap = 0;
-  g->fq_bytes = 0;
+  cublox_b200::detail::free_fetch(&g->fs);
   return CUBLOX_OK;
 }
 
 int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host) {
   const size_t n = static_cast<size_t>(g->voxel_num);
   cudaError_t e = cudaSuccess;
-  if (!g->d_occ) e = cudaMalloc(&g->d_occ, n * sizeof(float));
-  if (e == cudaSuccess && !g->d_cnt) e = cudaMalloc(&g->d_cnt, n * sizeof(uint32_t));
-  if (e == cudaSuccess && !g->d_hit) e = cudaMalloc(&g->d_hit, n * sizeof(uint32_t));
+  if (!g->d_occ) e = cublox_b200::detail::dmalloc(&g->d_occ, n * sizeof(float));
+  if (e == cudaSuccess && !g->d_cnt) e = cublox_b200::detail::dmalloc(&g->d_cnt, n * sizeof(uint32_t));
+  if (e == cudaSuccess && !g->d_hit) e = cublox_b200::detail::dmalloc(&g->d_hit, n * sizeof(uint32_t));
   if (e != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(g->d_occ);
-    cudaFree(g->d_cnt);
-    cudaFree(g->d_hit);
+    cublox_b200::detail::dfree(g->d_occ);
+    cublox_b200::detail::dfree(g->d_cnt);
+    cublox_b200::detail::dfree(g->d_hit);
     g->d_occ = nullptr;
     g->d_cnt = g->d_hit = nullptr;
     return fail(CUBLOX_ERR_NOMEM, "acquire_device: voxel buffers do not fit");
@@ -709,10 +745,10 @@ constexpr int kDriverCloudCap = 1000000;
 static int ensure_world(cublox_grid *g, int n) {
   if (n <= g->world_cap) return CUBLOX_OK;
   CK(cudaStreamSynchronize(g->stream));
-  cudaFree(g->d_world);
+  cublox_b200::detail::dfree(g->d_world);
   g->d_world = nullptr;
   g->world_cap = 0;
-  if (cudaMalloc(&g->d_world, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
+  if (cublox_b200::detail::dmalloc(&g->d_world, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess) {
     cudaGetLastError();
     return fail(CUBLOX_ERR_NOMEM, "sensor-frame update: world buffer allocation failed");
   }
@@ -735,7 +771,7 @@ static int world_params(cublox_grid *g, int n, const float rotation[9],
   ip->dst = g->d_world;
   ip->count = nullptr;
   if (g->first_run) {
-    if (!g->d_kept && cudaMalloc(&g->d_kept, sizeof(int)) != cudaSuccess) {
+    if (!g->d_kept && cublox_b200::detail::dmalloc(&g->d_kept, sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "sensor-frame update: allocation failed");
     }
@@ -823,10 +859,10 @@ int cublox_grid_update_depth(cublox_grid *g, const void *image, int encoding, in
   if (mem_kind(image) != 2) {
     if (bytes > g->image_cap) {
       CK(cudaStreamSynchronize(g->stream));
-      cudaFree(g->d_image);
+      cublox_b200::detail::dfree(g->d_image);
       g->d_image = nullptr;
       g->image_cap = 0;
-      if (cudaMalloc(&g->d_image, bytes) != cudaSuccess) {
+      if (cublox_b200::detail::dmalloc(&g->d_image, bytes) != cudaSuccess) {
         cudaGetLastError();
         return fail(CUBLOX_ERR_NOMEM, "cublox_grid_update_depth: image buffer allocation failed");
       }
@@ -934,17 +970,16 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
     g->last_cleared = g->voxel_num - keep;
   }
   const size_t mb = masks.size() * sizeof(uint32_t);
-  // Pinned staging, reused once the previous recenter's copy has run, so the
-  // host does not wait for the stream.
-  if (!g->h_masks) {
-    CK(cudaMallocHost(&g->h_masks, mb));
-    CK(cudaEventCreateWithFlags(&g->mask_ev, cudaEventDisableTiming));
-  } else {
-    CK(cudaEventSynchronize(g->mask_ev));
-  }
-  std::memcpy(g->h_masks, masks.data(), mb);
-  CK(cudaMemcpyAsync(g->d_masks, g->h_masks, mb, cudaMemcpyHostToDevice, g->stream));
-  CK(cudaEventRecord(g->mask_ev, g->stream));
+  // Pinned staging in two halves used in turn: a half is reused once the
+  // recenter before last has copied out of it, so the host does not wait
+  // for the stream's current work.
+  const int half = g->mask_half;
+  g->mask_half ^= 1;
+  uint32_t *stage = g->h_masks + half * g->mask_stage_words;
+  CK(cudaEventSynchronize(g->mask_ev[half]));
+  std::memcpy(stage, masks.data(), mb);
+  CK(cudaMemcpyAsync(g->d_masks, stage, mb, cudaMemcpyHostToDevice, g->stream));
+  CK(cudaEventRecord(g->mask_ev[half], g->stream));
   ClearParams cp{};
   cp.occ = g->d_occ;
   cp.xmask = g->d_masks;
@@ -1039,49 +1074,54 @@ QueryBox plan_query(const cublox_grid *g, const float c[3], float radius) {
 
 // Fetch scratch grows geometrically: a reallocation frees memory, which
 // waits for the whole device.
-static int ensure_fq(cublox_grid *g, cudaStream_t st, size_t bytes) {
-  if (bytes <= g->fq_bytes) return CUBLOX_OK;
-  bytes = std::max({bytes, 2 * g->fq_bytes, static_cast<size_t>(4) << 10});
+static int ensure_fq(FetchScratch *sc, cudaStream_t st, size_t bytes) {
+  if (bytes <= sc->fq_bytes) return CUBLOX_OK;
+  bytes = std::max({bytes, 2 * sc->fq_bytes, static_cast<size_t>(4) << 10});
   CK(cudaStreamSynchronize(st));
-  cudaFree(g->d_fq);
-  g->d_fq = nullptr;
-  g->fq_bytes = 0;
-  if (cudaMalloc(&g->d_fq, bytes) != cudaSuccess) {
+  cublox_b200::detail::dfree(sc->fq);
+  sc->fq = nullptr;
+  sc->fq_bytes = 0;
+  if (cublox_b200::detail::dmalloc(&sc->fq, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(CUBLOX_ERR_NOMEM, "fetch: query buffer allocation failed");
   }
-  g->fq_bytes = bytes;
+  sc->fq_bytes = bytes;
   return CUBLOX_OK;
 }
-
-static int ensure_fout(cublox_grid *g, cudaStream_t st, int64_t n) {
-  if (n <= g->fcap) return CUBLOX_OK;
-  n = std::max({n, 2 * g->fcap, static_cast<int64_t>(1) << 12});
+static int ensure_fout(FetchScratch *sc, cudaStream_t st, int64_t n) {
+  if (n <= sc->fcap) return CUBLOX_OK;
+  n = std::max({n, 2 * sc->fcap, static_cast<int64_t>(1) << 12});
   CK(cudaStreamSynchronize(st));
-  cudaFree(g->d_fpos);
-  cudaFree(g->d_fstate);
-  g->d_fpos = nullptr;
-  g->d_fstate = nullptr;
-  g->fcap = 0;
-  if (cudaMalloc(&g->d_fpos, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess ||
-      cudaMalloc(&g->d_fstate, static_cast<size_t>(n)) != cudaSuccess) {
+  cublox_b200::detail::dfree(sc->fpos);
+  cublox_b200::detail::dfree(sc->fstate);
+  sc->fpos = nullptr;
+  sc->fstate = nullptr;
+  sc->fcap = 0;
+  if (cublox_b200::detail::dmalloc(&sc->fpos, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess ||
+      cublox_b200::detail::dmalloc(&sc->fstate, static_cast<size_t>(n)) != cudaSuccess) {
     cudaGetLastError();
     return fail(CUBLOX_ERR_NOMEM, "fetch: output buffer allocation failed");
   }
-  g->fcap = n;
+  sc->fcap = n;
   return CUBLOX_OK;
 }
 
-// Plans, counts and (if out_pos) writes.  counts_out gets the kept count per
-// query (min(count, cap) as fetchOccupancyAround returns it).
-// On stream st (the grid's own, or a caller's ordered after the grid's
-// work).  With vpos / vstate the outputs are sized there after counting.
+// Bytes of the query block for nq centres cut into nu work units (the
+// layout fetch_impl uses).
+static size_t fetch_query_bytes(int nq, int nu) {
+  auto al = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  const size_t ll = al(sizeof(long long) * std::max(nu, 1));
+  return al(sizeof(float) * 3 * nq) + al(sizeof(int) * 8 * nq) + al(sizeof(float) * nq) +
+         al(sizeof(int) * std::max(nu, 1)) + 4 * ll;
+}
+
 static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int nq,
                       float radius, int filter, int max_results, int64_t *kept,
                       int64_t *offsets, float *out_pos, uint8_t *out_state, int64_t capacity,
                       bool write, std::vector<float> *vpos = nullptr,
-                      std::vector<uint8_t> *vstate = nullptr) {
+                      std::vector<uint8_t> *vstate = nullptr, FetchScratch *sc = nullptr) {
   if (!g || (nq > 0 && !centers)) return fail(CUBLOX_ERR_INVALID, "fetch: null argument");
+  if (!sc) sc = &g->fs;
   if (filter < -1 || filter > 2) return fail(CUBLOX_ERR_INVALID, "fetch: bad filter");
   if (nq <= 0) {
     if (offsets) offsets[0] = 0;
@@ -1122,9 +1162,9 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
   const size_t o_box = al(b_cent), o_r2 = o_box + al(b_box), o_uq = o_r2 + al(b_r2),
                o_ut0 = o_uq + al(b_uq), o_cnt = o_ut0 + al(b_ll), o_off = o_cnt + al(b_ll),
                o_lim = o_off + al(b_ll), total = o_lim + al(b_ll);
-  int rc = ensure_fq(g, st, total);
+  int rc = ensure_fq(sc, st, total);
   if (rc) return rc;
-  char *base = static_cast<char *>(g->d_fq);
+  char *base = static_cast<char *>(sc->fq);
   CK(cudaMemcpyAsync(base, centers, b_cent, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_box, boxes.data(), b_box, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_r2, r2.data(), b_r2, cudaMemcpyHostToDevice, st));
@@ -1198,21 +1238,21 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
     return fail(CUBLOX_ERR_INVALID, "fetch: output capacity " + std::to_string(capacity) +
                                         " < " + std::to_string(total_s) + " samples");
   if (total_s == 0) return CUBLOX_OK;
-  rc = ensure_fout(g, st, total_s);
+  rc = ensure_fout(sc, st, total_s);
   if (rc) return rc;
   CK(cudaMemcpyAsync(base + o_off, uoff.data(), sizeof(long long) * nu, cudaMemcpyHostToDevice,
                      st));
   CK(cudaMemcpyAsync(base + o_lim, ulim.data(), sizeof(long long) * nu, cudaMemcpyHostToDevice,
                      st));
-  p.out_pos = g->d_fpos;
-  p.out_state = g->d_fstate;
+  p.out_pos = sc->fpos;
+  p.out_state = sc->fstate;
   launch_fetch(p, 2, st);
   CK_LAUNCH();
   if (out_pos)
-    CK(cudaMemcpyAsync(out_pos, g->d_fpos, sizeof(float) * 3 * static_cast<size_t>(total_s),
+    CK(cudaMemcpyAsync(out_pos, sc->fpos, sizeof(float) * 3 * static_cast<size_t>(total_s),
                        cudaMemcpyDeviceToHost, st));
   if (out_state)
-    CK(cudaMemcpyAsync(out_state, g->d_fstate, static_cast<size_t>(total_s),
+    CK(cudaMemcpyAsync(out_state, sc->fstate, static_cast<size_t>(total_s),
                        cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return CUBLOX_OK;
@@ -1223,10 +1263,25 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
 int cublox_b200::detail::fetch_into(cublox_grid *g, cudaStream_t st, const float *centers,
                                     int nq, float radius, int filter, int max_results,
                                     std::vector<int64_t> &offsets, std::vector<float> &pos,
-                                    std::vector<uint8_t> &state) {
+                                    std::vector<uint8_t> &state, FetchScratch *sc) {
   offsets.assign(static_cast<size_t>(nq) + 1, 0);
   return fetch_impl(g, st, centers, nq, radius, filter, max_results, nullptr, offsets.data(),
-                    nullptr, nullptr, 0, true, &pos, &state);
+                    nullptr, nullptr, 0, true, &pos, &state, sc);
+}
+
+int cublox_b200::detail::reserve_fetch(FetchScratch *sc, int centres, int64_t samples,
+                                       cudaStream_t st) {
+  // work units: at most 32 per SM plus one per centre (fetch_impl's cut)
+  int rc = ensure_fq(sc, st, fetch_query_bytes(centres, centres + 32 * 160));
+  if (rc) return rc;
+  return ensure_fout(sc, st, samples);
+}
+
+void cublox_b200::detail::free_fetch(FetchScratch *sc) {
+  cublox_b200::detail::dfree(sc->fq);
+  cublox_b200::detail::dfree(sc->fpos);
+  cublox_b200::detail::dfree(sc->fstate);
+  *sc = FetchScratch{};
 }
 
 extern "C" {
@@ -1257,21 +1312,21 @@ int cublox_grid_fetch_viz(cublox_grid *g, const float center[3], float radius, i
   const size_t need = sizeof(float) * 4 * static_cast<size_t>(cap);
   if (static_cast<size_t>(g->qcap) * 12 < need || g->qcap < 8) {
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(g->d_qin);
-    cudaFree(g->d_qout);
+    cublox_b200::detail::dfree(g->d_qin);
+    cublox_b200::detail::dfree(g->d_qout);
     g->d_qin = nullptr;
     g->d_qout = nullptr;
     g->qcap = 0;
     const int q = static_cast<int>(std::max<size_t>((need + 11) / 12, 8));
-    if (cudaMalloc(&g->d_qin, sizeof(float) * 3 * static_cast<size_t>(q)) != cudaSuccess ||
-        cudaMalloc(&g->d_qout, static_cast<size_t>(q)) != cudaSuccess) {
+    if (cublox_b200::detail::dmalloc(&g->d_qin, sizeof(float) * 3 * static_cast<size_t>(q)) != cudaSuccess ||
+        cublox_b200::detail::dmalloc(&g->d_qout, static_cast<size_t>(q)) != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "fetch_viz: allocation failed");
     }
     g->qcap = q;
   }
   VizParams vp{};
-  vp.pos = g->d_fpos;
+  vp.pos = g->fs.fpos;
   vp.n = total;
   vp.inv = g->res_inv;
   vp.ctr = g->ctr ? 1 : 0;
@@ -1340,13 +1395,13 @@ int cublox_grid_query_states(cublox_grid *g, const float *xyz, int n,
   if (n <= 0) return CUBLOX_OK;
   if (n > g->qcap) {
     CK(cudaStreamSynchronize(g->stream));
-    cudaFree(g->d_qin);
-    cudaFree(g->d_qout);
+    cublox_b200::detail::dfree(g->d_qin);
+    cublox_b200::detail::dfree(g->d_qout);
     g->d_qin = nullptr;
     g->d_qout = nullptr;
     g->qcap = 0;
-    if (cudaMalloc(&g->d_qin, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess ||
-        cudaMalloc(&g->d_qout, static_cast<size_t>(n)) != cudaSuccess) {
+    if (cublox_b200::detail::dmalloc(&g->d_qin, sizeof(float) * 3 * static_cast<size_t>(n)) != cudaSuccess ||
+        cublox_b200::detail::dmalloc(&g->d_qout, static_cast<size_t>(n)) != cudaSuccess) {
       cudaGetLastError();
       return fail(CUBLOX_ERR_NOMEM, "query_states: allocation failed");
     }

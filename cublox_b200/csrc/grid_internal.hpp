@@ -10,6 +10,20 @@
 #include "exact_fp.cuh"
 #include "kernels.cuh"
 
+namespace cublox_b200 {
+// Device scratch of a sphere fetch: the query block (centres | boxes |
+// radii | work units | per-unit counts, offsets and limits) and the sample
+// outputs.  A grid grows its own on demand; the server owns one, sized when
+// it is created, shared by its fetches (they run one at a time).
+struct FetchScratch {
+  void *fq = nullptr;
+  size_t fq_bytes = 0;
+  float *fpos = nullptr;
+  uint8_t *fstate = nullptr;
+  int64_t fcap = 0;
+};
+}  // namespace cublox_b200
+
 struct cublox_grid {
   // Grid::Config (Grid.hpp:44-53)
   int half[3] = {0, 0, 0};
@@ -61,8 +75,10 @@ struct cublox_grid {
   unsigned long long *d_stats = nullptr;  // 4
   uint32_t *d_err = nullptr;
   uint32_t *d_masks = nullptr;  // recenter slab masks
-  uint32_t *h_masks = nullptr;  // pinned staging of the masks
-  cudaEvent_t mask_ev = nullptr;  // staging free again
+  uint32_t *h_masks = nullptr;  // pinned staging of the masks, two halves
+  cudaEvent_t mask_ev[2] = {nullptr, nullptr};  // a half free again
+  int mask_half = 0;  // the half the next recenter stages into
+  int mask_stage_words = 0;  // words per half
   int mask_words[3] = {0, 0, 0};
 
   float *d_cloud = nullptr;  // SoA [x|y|z]
@@ -77,12 +93,7 @@ struct cublox_grid {
   int stage_cap = 0;
   int stage_idx = 0;
 
-  // fetch scratch
-  void *d_fq = nullptr;  // centers | qbox | qr2 | counts | offsets | limits
-  size_t fq_bytes = 0;
-  float *d_fpos = nullptr;
-  uint8_t *d_fstate = nullptr;
-  int64_t fcap = 0;
+  cublox_b200::FetchScratch fs;  // fetch scratch, grown on demand
   uint8_t *d_qout = nullptr;
   float *d_qin = nullptr;
   int qcap = 0;
@@ -90,6 +101,26 @@ struct cublox_grid {
 
 namespace cublox_b200 {
 namespace detail {
+// Every device and pinned-host allocation and free this library makes goes
+// through these, which count them (cublox_runtime_counters), so that a
+// caller can check that a steady state allocates nothing.
+enum Counter { kDevAllocs = 0, kDevFrees, kPinnedAllocs, kPinnedFrees, kGraphBuilds, kNumCounters };
+void count(Counter c);
+cudaError_t dev_alloc(void **p, size_t bytes);
+cudaError_t dev_free(void *p);
+cudaError_t pinned_alloc(void **p, size_t bytes);
+cudaError_t pinned_free(void *p);
+template <class T>
+inline cudaError_t dmalloc(T **p, size_t bytes) {
+  return dev_alloc(reinterpret_cast<void **>(p), bytes);
+}
+template <class T>
+inline cudaError_t hmalloc(T **p, size_t bytes) {
+  return pinned_alloc(reinterpret_cast<void **>(p), bytes);
+}
+inline cudaError_t dfree(const void *p) { return dev_free(const_cast<void *>(p)); }
+inline cudaError_t hfree(const void *p) { return pinned_free(const_cast<void *>(p)); }
+
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what, int line);
 // First update: snap the window origin to the sensor voxel
@@ -114,9 +145,15 @@ int release_scratch(cublox_grid *g);
 // unknown if null), counters zero.
 int acquire_device(cublox_grid *g, const float *occ_host);
 // fetch_batch on stream st (ordered after the grid's work by the caller),
-// outputs sized to the samples found.
+// outputs sized to the samples found, in the scratch `sc` (the grid's own if
+// null).
 int fetch_into(cublox_grid *g, cudaStream_t st, const float *centers, int nq, float radius,
                int filter, int max_results, std::vector<int64_t> &offsets,
-               std::vector<float> &pos, std::vector<uint8_t> &state);
+               std::vector<float> &pos, std::vector<uint8_t> &state,
+               FetchScratch *sc = nullptr);
+// Size `sc` for fetches of up to `centres` centres and `samples` samples, so
+// that such fetches allocate nothing.
+int reserve_fetch(FetchScratch *sc, int centres, int64_t samples, cudaStream_t st);
+void free_fetch(FetchScratch *sc);
 }  // namespace detail
 }  // namespace cublox_b200

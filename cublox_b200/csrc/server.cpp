@@ -82,7 +82,8 @@ struct MapState {
   cublox_grid *g = nullptr;  // created at first admission
   bool resident = false;
   std::vector<float> snapshot;  // stored log-odds while evicted
-  size_t vox_bytes = 0;
+  size_t vox_bytes = 0;  // device bytes of the map's arrays
+  int64_t voxels = 0;
   uint64_t last_use = 0;
   std::deque<Request *> queue;  // pending requests, arrival order
   std::atomic<bool> fetching{false};  // a fetch of this map is in flight
@@ -102,21 +103,40 @@ struct Tick {
 
 // Pinned host blocks for scan points, reused by size class (64 KiB << c).
 // A scan submitted into one is copied to the device by DMA straight from
-// it, so the worker thread copies nothing for a one-scan tick.  A block
-// returns to the pool when its request ends (its tick's copy has run by
-// then); the pool holds at most kCapBytes, beyond which points stay in
-// pageable memory and the batch stages them.
+// it, so the worker thread copies nothing for a one-scan tick.  Blocks are
+// carved from one pinned arena allocated when the server is created: a
+// class with no free block takes the next piece of the arena, and a block
+// returns to its class when its request ends (its tick's copy has run by
+// then).  Submitting never allocates; a scan that finds no room stays in
+// pageable memory and the batch stages it.
 struct PinnedPool {
   static constexpr size_t kMinBytes = size_t(64) << 10;
-  static constexpr size_t kCapBytes = size_t(1) << 30;
   std::mutex mu;
   std::vector<std::vector<float *>> free_by_class;
-  std::vector<float *> all;
-  size_t total = 0;
+  char *arena = nullptr;
+  size_t arena_bytes = 0, carved = 0;
 
-  // `device`: the server's GPU, current during a new allocation (the
-  // calling thread's own current device is put back afterwards).
-  float *take(size_t bytes, int device, int *cls) {
+  // Allocates the arena with `device` current (the calling thread's own
+  // current device is put back afterwards).
+  int init(size_t bytes, int device) {
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    const bool switched = prev >= 0 && prev != device && cudaSetDevice(device) == cudaSuccess;
+    void *p = nullptr;
+    const cudaError_t e = bytes ? cublox_b200::detail::hmalloc(&p, bytes) : cudaSuccess;
+    if (switched) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CUBLOX_ERR_NOMEM, "server: pinned arena allocation failed");
+    }
+    arena = static_cast<char *>(p);
+    arena_bytes = bytes;
+    return CUBLOX_OK;
+  }
+  float *take(size_t bytes, int *cls) {
     int c = 0;
     while ((kMinBytes << c) < bytes) ++c;
     std::lock_guard<std::mutex> lk(mu);
@@ -127,24 +147,11 @@ struct PinnedPool {
       return p;
     }
     const size_t sz = kMinBytes << c;
-    if (total + sz > kCapBytes) return nullptr;
-    void *p = nullptr;
-    int prev = -1;
-    if (cudaGetDevice(&prev) != cudaSuccess) {
-      cudaGetLastError();
-      prev = -1;
-    }
-    const bool switched = prev >= 0 && prev != device && cudaSetDevice(device) == cudaSuccess;
-    const cudaError_t e = cudaMallocHost(&p, sz);
-    if (switched) cudaSetDevice(prev);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    all.push_back(static_cast<float *>(p));
-    total += sz;
+    if (carved + sz > arena_bytes) return nullptr;
+    float *p = reinterpret_cast<float *>(arena + carved);
+    carved += sz;
     *cls = c;
-    return static_cast<float *>(p);
+    return p;
   }
   void give(float *p, int c) {
     std::lock_guard<std::mutex> lk(mu);
@@ -152,16 +159,18 @@ struct PinnedPool {
     free_by_class[c].push_back(p);
   }
   void release_all() {
-    for (float *p : all) cudaFreeHost(p);
-    all.clear();
+    cublox_b200::detail::hfree(arena);
+    arena = nullptr;
+    arena_bytes = carved = 0;
     free_by_class.clear();
-    total = 0;
   }
 };
 
 struct cublox_server {
   cublox_server_config cfg{};
   PinnedPool pinned;  // scan points
+  cublox_b200::FetchScratch fscratch;  // shared by fetches (one at a time)
+  int reserved_maps = 0;  // maps the batch's item buffers are sized for
   cublox_batch *batch = nullptr;
   cudaStream_t stream = nullptr;
   int device = 0;
@@ -208,9 +217,27 @@ void finish(cublox_server *s, Request *r, int error, const std::string &msg) {
   --s->pending;
 }
 
-size_t scratch_bytes(cublox_server *s) {
-  // batch point buffer at the tick budget, plus descriptors
-  return 12 * static_cast<size_t>(s->cfg.max_tick_points) + (1u << 20);
+// Fetch scratch sized for cfg's fetch limits (the query block, 13 B a
+// sample).
+size_t fetch_scratch_bytes(const cublox_server_config &cfg) {
+  const size_t nq = static_cast<size_t>(cfg.max_fetch_centres);
+  const size_t nu = nq + 32 * 160;
+  return 4 * nq * 12 + 4 * nu * 40 + 13 * static_cast<size_t>(cfg.max_fetch_samples) +
+         (size_t(16) << 10);
+}
+
+size_t scratch_bytes(const cublox_server_config &cfg) {
+  // batch point buffer at the tick budget, descriptors, fetch scratch
+  return 12 * static_cast<size_t>(cfg.max_tick_points) + (1u << 20) + fetch_scratch_bytes(cfg);
+}
+
+size_t scratch_bytes(cublox_server *s) { return scratch_bytes(s->cfg); }
+
+void fill_defaults(cublox_server_config *cfg) {
+  if (cfg->max_tick_points <= 0) cfg->max_tick_points = 1 << 20;
+  if (cfg->pinned_pool_bytes == 0) cfg->pinned_pool_bytes = size_t(256) << 20;
+  if (cfg->max_fetch_centres <= 0) cfg->max_fetch_centres = 1024;
+  if (cfg->max_fetch_samples <= 0) cfg->max_fetch_samples = int64_t(1) << 22;
 }
 
 constexpr int kMaxMaps = 4096;
@@ -283,6 +310,11 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
   return CUBLOX_OK;
 }
 
+// Tick and fetch-order events: the completer thread waits on them, and a
+// blocking-sync event lets it sleep instead of spinning a core.
+constexpr unsigned kEventFlags = cudaEventDisableTiming | cudaEventBlockingSync;
+constexpr int kEventPool = 64;  // created with the server
+
 // Caller holds the lock.
 cudaEvent_t take_event(cublox_server *s) {
   if (!s->free_events.empty()) {
@@ -291,7 +323,7 @@ cudaEvent_t take_event(cublox_server *s) {
     return e;
   }
   cudaEvent_t e = nullptr;
-  cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&e, kEventFlags);
   return e;
 }
 
@@ -327,11 +359,7 @@ void fetcher_loop(cublox_server *s) {
       rc = cublox_b200::detail::fetch_into(m.g, s->fstream, r->centers.data(),
                                            static_cast<int>(r->centers.size() / 3), r->radius,
                                            r->filter, r->max_results, r->offsets, r->fpos,
-                                           r->fstate);
-    // Outputs stay on the host: give the device scratch back when the
-    // budget is exceeded.
-    if (!rc && used_bytes(s) > s->cfg.hbm_budget_bytes)
-      rc = cublox_b200::detail::release_scratch(m.g);
+                                           r->fstate, &s->fscratch);
     const std::string msg = rc ? cublox_last_error() : "";
     std::lock_guard<std::mutex> lk(s->mu);
     ++s->stats.fetches;
@@ -388,6 +416,14 @@ void worker_loop(cublox_server *s) {
       const auto now = Clock::now();
       for (Request *r : scans) r->state = CUBLOX_REQ_RUNNING, r->t_start = now;
       for (Request *r : fetches) r->state = CUBLOX_REQ_RUNNING, r->t_start = now;
+    }
+    // The batch's work-item buffers, sized once for every map known so far
+    // (a tick never holds more), so that ticks allocate nothing.
+    if (nm > s->reserved_maps) {
+      int64_t vox = 0;
+      for (int j = 0; j < nm; ++j) vox += s->maps[j]->voxels;
+      if (cublox_batch_reserve_maps(s->batch, s->cfg.max_tick_points, nm, vox) == CUBLOX_OK)
+        s->reserved_maps = nm;
     }
     // A map gives a tick one request, its oldest: a scan or a fetch.
     // scans: admit, concatenate, one batched update, recenters
@@ -544,9 +580,10 @@ int cublox_server_create(const cublox_server_config *cfg, cublox_server **out) {
   auto s = std::make_unique<cublox_server>();
   s->cfg = *cfg;
   s->maps.reserve(kMaxMaps);
-  if (s->cfg.max_tick_points <= 0) s->cfg.max_tick_points = 1 << 20;
+  fill_defaults(&s->cfg);
   if (s->cfg.hbm_budget_bytes < scratch_bytes(s.get()))
-    return fail(CUBLOX_ERR_INVALID, "server_create: budget below the tick scratch");
+    return fail(CUBLOX_ERR_INVALID, "server_create: budget below the tick and fetch scratch (" +
+                                        std::to_string(scratch_bytes(s.get())) + " bytes)");
   cudaGetDevice(&s->device);
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->fstream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -562,12 +599,24 @@ int cublox_server_create(const cublox_server_config *cfg, cublox_server **out) {
   }
   cublox_batch_set_option(s->batch, CUBLOX_BATCH_OPT_GRAPHS, s->cfg.graphs ? 1 : 0);
   rc = cublox_batch_reserve(s->batch, s->cfg.max_tick_points, 64);
+  if (!rc) rc = s->pinned.init(s->cfg.pinned_pool_bytes, s->device);
+  if (!rc)
+    rc = cublox_b200::detail::reserve_fetch(&s->fscratch, s->cfg.max_fetch_centres,
+                                            s->cfg.max_fetch_samples, s->fstream);
   if (rc) {
+    const std::string msg = cublox_last_error();
+    cublox_b200::detail::free_fetch(&s->fscratch);
+    s->pinned.release_all();
     cublox_batch_destroy(s->batch);
     cudaStreamDestroy(s->stream);
     cudaStreamDestroy(s->fstream);
-    return rc;
+    return fail(rc, msg);
   }
+  for (int i = 0; i < kEventPool; ++i) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, kEventFlags) == cudaSuccess) s->free_events.push_back(e);
+  }
+  cudaGetLastError();
   cublox_server *raw = s.release();
   raw->worker = std::thread(worker_loop, raw);
   raw->completer = std::thread(completer_loop, raw);
@@ -595,6 +644,7 @@ int cublox_server_destroy(cublox_server *s) {
   for (auto &m : s->maps)
     if (m->g) cublox_grid_destroy(m->g);
   cublox_batch_destroy(s->batch);
+  cublox_b200::detail::free_fetch(&s->fscratch);
   s->pinned.release_all();
   cudaStreamDestroy(s->stream);
   cudaStreamDestroy(s->fstream);
@@ -629,6 +679,7 @@ int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float re
     std::memcpy(m->lo, log_odds, sizeof(m->lo));
     m->has_lo = true;
   }
+  m->voxels = vox;
   m->vox_bytes = 12 * static_cast<size_t>(vox);
   std::lock_guard<std::mutex> lk(s->mu);
   if (static_cast<int>(s->maps.size()) >= kMaxMaps)
@@ -663,7 +714,7 @@ int cublox_server_submit_scan(cublox_server *s, int map_id, const float *xyz, in
   r->map = map_id;
   const size_t floats = 3 * static_cast<size_t>(n);
   int cls = -1;
-  float *pin = floats ? s->pinned.take(floats * sizeof(float), s->device, &cls) : nullptr;
+  float *pin = floats ? s->pinned.take(floats * sizeof(float), &cls) : nullptr;
   if (pin) {
     std::memcpy(pin, xyz, floats * sizeof(float));
     r->pin = pin;
@@ -766,7 +817,7 @@ int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int orig
   if (map_id < 0 || map_id >= static_cast<int>(s->maps.size()))
     return fail(CUBLOX_ERR_INVALID, "server_export: unknown map id");
   MapState &m = *s->maps[map_id];
-  const size_t vox = m.vox_bytes / 12;
+  const size_t vox = static_cast<size_t>(m.voxels);
   if (!m.g) {
     std::fill(occ_host, occ_host + vox, 0.0f);
     if (origin_index) {
@@ -785,6 +836,32 @@ int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int orig
     std::copy(m.snapshot.begin(), m.snapshot.end(), occ_host);
   }
   if (origin_index) cublox_grid_origin(m.g, origin_index, nullptr);
+  return CUBLOX_OK;
+}
+
+int cublox_server_cancel(cublox_server *s, int64_t request_id) {
+  if (!s) return fail(CUBLOX_ERR_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Request *r = find(s, request_id);
+  if (!r) return fail(CUBLOX_ERR_INVALID, "cancel: unknown request");
+  std::deque<Request *> &q = s->maps[r->map]->queue;
+  const auto it = std::find(q.begin(), q.end(), r);
+  // Only a request still waiting in its map's queue can be withdrawn; one
+  // the worker has taken is being served (or done).
+  if (r->state != CUBLOX_REQ_QUEUED || it == q.end())
+    return fail(CUBLOX_ERR_INVALID, "cancel: request is already being served or finished");
+  q.erase(it);
+  ++s->stats.cancelled;
+  finish(s, r, CUBLOX_ERR_CANCELLED, "cancelled before it was served");
+  s->cv_done.notify_all();
+  return CUBLOX_OK;
+}
+
+int cublox_server_scratch_bytes(const cublox_server_config *cfg, uint64_t *bytes) {
+  if (!cfg || !bytes) return fail(CUBLOX_ERR_INVALID, "server_scratch_bytes: null argument");
+  cublox_server_config c = *cfg;
+  fill_defaults(&c);
+  *bytes = scratch_bytes(c);
   return CUBLOX_OK;
 }
 

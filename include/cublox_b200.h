@@ -25,6 +25,7 @@ extern "C" {
 #define CUBLOX_ERR_NOMEM -3   /* device or pinned allocation failed       */
 #define CUBLOX_ERR_RANGE -4   /* voxel count above int32 (Grid.cpp:44-50) */
 #define CUBLOX_ERR_DEVICE -5  /* device-side check failed (error word)    */
+#define CUBLOX_ERR_CANCELLED -6 /* served request withdrawn before it ran  */
 
 #define CUBLOX_STATE_UNKNOWN 0 /* OccupancyGrid.hpp:31-35 */
 #define CUBLOX_STATE_FREE 1
@@ -50,6 +51,12 @@ const char *cublox_version(void);
 /* Binary version of this library's kernels as loaded on the current device
  * (major * 10 + minor: 100 for sm_100a).  No counterpart in the reference.  */
 int cublox_binary_version(int *binary_version);
+/* Process-wide counts of what this library has done so far, for checking
+ * that a steady state allocates nothing: out[0] device allocations, [1]
+ * device frees, [2] pinned host allocations, [3] pinned host frees, [4] CUDA
+ * graphs instantiated.  Fills the first n (entries past 5 read 0).  No
+ * counterpart in the reference.                                             */
+int cublox_runtime_counters(int64_t *out, int n);
 
 /* OccupancyGrid(half_map_size_i, resolution, origin_at_center,
  * recenter_threshold, origin)  — OccupancyGrid.hpp:42-45,
@@ -291,6 +298,9 @@ int cublox_batch_recenter(cublox_batch *b, int n, cublox_grid *const *grids,
  * grids now, so that later updates of that size allocate nothing (growing
  * a buffer frees the old one, which waits for the whole device).           */
 int cublox_batch_reserve(cublox_batch *b, int64_t points, int maps);
+/* The same for updates over up to `maps` grids of `voxels` voxels in all,
+ * whatever their sizes (the fold's work items grow with the voxels).       */
+int cublox_batch_reserve_maps(cublox_batch *b, int64_t points, int maps, int64_t voxels);
 int cublox_batch_synchronize(cublox_batch *b);
 int cublox_batch_last_timing(cublox_batch *b, float *walk_ms, float *fold_ms);
 int cublox_batch_stream(const cublox_batch *b, void **stream);
@@ -318,6 +328,13 @@ typedef struct cublox_server_config {
   int max_tick_maps;         /* scans per batched launch (0: no limit)       */
   int max_inflight_ticks;    /* ticks queued on the device (0: 2)            */
   int graphs;                /* replay batched launches from CUDA graphs     */
+  /* Everything below is sized when the server is created, so that serving
+   * within these sizes allocates nothing (cublox_runtime_counters).        */
+  uint64_t pinned_pool_bytes; /* pinned host arena that submitted scans are
+                                 copied into (0: 256 MiB); a scan that finds
+                                 no room stays in pageable memory           */
+  int max_fetch_centres;      /* centres per fetch request (0: 1024)        */
+  int64_t max_fetch_samples;  /* samples per fetch request (0: 1 << 22)     */
 } cublox_server_config;
 
 typedef struct cublox_server_stats {
@@ -325,6 +342,7 @@ typedef struct cublox_server_stats {
   int64_t admissions, evictions;         /* maps brought in / sent to host */
   uint64_t resident_bytes, peak_resident_bytes;
   int resident_maps;
+  int64_t cancelled;                     /* requests withdrawn             */
 } cublox_server_stats;
 
 #define CUBLOX_REQ_QUEUED 0
@@ -368,6 +386,15 @@ int cublox_server_release(cublox_server *s, int64_t request_id); /* forget */
  * window origin.                                                            */
 int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int origin_index[3]);
 int cublox_server_get_stats(cublox_server *s, cublox_server_stats *out);
+/* Withdraw a request still waiting in its map's queue: it ends FAILED with
+ * CUBLOX_ERR_CANCELLED and has no effect on the map.  A request the worker
+ * has already taken cannot be withdrawn (CUBLOX_ERR_INVALID).  The
+ * reference's driver has no queue to withdraw from (main.cpp:464-491).     */
+int cublox_server_cancel(cublox_server *s, int64_t request_id);
+/* Device bytes a server with this configuration holds besides its maps
+ * (tick point buffers, descriptors, fetch scratch): the least usable
+ * hbm_budget_bytes.                                                        */
+int cublox_server_scratch_bytes(const cublox_server_config *cfg, uint64_t *bytes);
 
 /* ---- allocation-free integration ------------------------------------------
  * No counterpart in the reference: it exists for callers that must not
