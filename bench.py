@@ -198,13 +198,14 @@ def pct(a, q):
 # headline: batched README-scale maps
 # ---------------------------------------------------------------------------
 def tune_shape(new_batch, dev, sensors, offsets, fixed=-1, max_updates=256):
-    """The launch shape the batch's tuner picks for this workload, from a
-    throw-away batch that integrates the step scans in order (wrapping
-    around) until the tuner has timed every candidate.  Returns (shape,
-    updates the tuner took); a fixed shape (>= 0) is returned as is."""
+    """The launch shape and voxel layout the batch's tuner picks for this
+    workload, from a throw-away batch that integrates the step scans in
+    order (wrapping around) until the tuner has timed every candidate.
+    Returns ((shape, layout), updates the tuner took); a fixed shape (>= 0)
+    is returned as is, with the default layout."""
     import cublox_b200 as C
     if fixed >= 0:
-        return fixed, 0
+        return (fixed, C.LAYOUTS[0]), 0
     b, gs = new_batch(graphs=False)
     k = 0
     while b.tuning() and k < max_updates:
@@ -212,9 +213,9 @@ def tune_shape(new_batch, dev, sensors, offsets, fixed=-1, max_updates=256):
         b.update(gs, dev[j], sensors[j], offsets=offsets[j])
         b.recenter(gs, sensors[j])
         k += 1
-    shape = b.get_option(C.BATCH_OPT_SHAPE)
+    choice = (b.get_option(C.BATCH_OPT_SHAPE), b.get_option(C.BATCH_OPT_LAYOUT))
     b.close()
-    return shape, k
+    return choice, k
 
 
 def run_headline(args, rank, world, dist):
@@ -236,8 +237,9 @@ def run_headline(args, rank, world, dist):
     def new_batch(graphs=True, shape=None):
         b = C.Batch(stream=stream.cuda_stream)
         b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
-        if shape is not None:
-            b.set_option(C.BATCH_OPT_SHAPE, shape)
+        if shape is not None:  # (launch shape, voxel layout)
+            b.set_option(C.BATCH_OPT_SHAPE, shape[0])
+            b.set_option(C.BATCH_OPT_LAYOUT, shape[1])
         gs = []
         for _ in range(K):
             g = b.add_grid(w.half, w.resolution, False, w.threshold)
@@ -280,7 +282,7 @@ def run_headline(args, rank, world, dist):
     own_ms = float(step_ms.sum())
     value = replicas.job_rate(timed_vs, own_ms / 1e3, dist, device="cuda")
     tot_ms = replicas.max_over_ranks(own_ms, dist, device="cuda")
-    assert b.get_option(C.BATCH_OPT_SHAPE) == shape and not b.tuning()
+    assert b.get_option(C.BATCH_OPT_SHAPE) == shape[0] and not b.tuning()
     for g in gs:
         assert g.check() == 0, "device error word set"
     b.close()
@@ -290,18 +292,36 @@ def run_headline(args, rank, world, dist):
     b.set_option(C.BATCH_OPT_TIMING, 1)
     for g in gs:
         g.enable_stats(True)
+        g.enable_timing(True)
     walk_ms, fold_ms, touched, incs = [], [], [], []
+    clear_ms, cleared = [], []  # recenters that fired (every step, warm-up included)
     for k in range(n_steps):
         flush.zero_()
         b.update(gs, dev[k], sensors[k], offsets=offsets[k])
         wm, fm = b.last_timing()
-        b.recenter(gs, sensors[k])
+        acts = b.recenter(gs, sensors[k])
+        for g, a in zip(gs, acts):
+            if a == 1:
+                clear_ms.append(g.last_timing()[2])
+                cleared.append(g.last_clear())
         if k >= args.warmup:
             walk_ms.append(wm)
             fold_ms.append(fm)
             st = [g.last_stats() for g in gs]
             touched.append(sum(s["touched"] for s in st))
             incs.append(sum(s["op_incs"] + s["hit_incs"] for s in st))
+    # a served-style fetch on the last map after the drive: 256 centres
+    # within 3 m of the robot, r 1.5 m, the driver's OCCUPIED filter
+    rng = np.random.default_rng(9)
+    so = sensors[-1][-1]
+    cen = (so + np.stack([rng.uniform(-3, 3, 256), rng.uniform(-3, 3, 256),
+                          rng.uniform(-1.5, 1.5, 256)], axis=1)).astype(np.float32)
+    fetch_ms, n_samples = [], 0
+    for _ in range(6):
+        t0 = time.perf_counter()
+        off_f, _, _ = gs[-1].fetch_batch(cen, 1.5, C.VoxelState.OCCUPIED)
+        fetch_ms.append((time.perf_counter() - t0) * 1e3)
+        n_samples = int(off_f[-1])
     b.close()
     del dev
 
@@ -334,6 +354,8 @@ def run_headline(args, rank, world, dist):
         "shape": shape, "tune_updates": tune_updates, "walk_ms": walk_ms, "fold_ms": fold_ms, "touched": touched, "incs": incs,
         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "launches": launches,
         "recenters": sum(1 for a in actions if a), "clocks": clk.summary(), "w": w,
+        "clear_ms": clear_ms, "cleared": cleared, "fetch_ms": fetch_ms[1:],
+        "fetch_samples": n_samples,
         "scans": scans, "origins": origins, "steps": steps,
     }
 
@@ -411,8 +433,9 @@ def run_batching(args):
     def new_batch(graphs=True, shape=None):
         b = C.Batch(stream=stream.cuda_stream)
         b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
-        if shape is not None:
-            b.set_option(C.BATCH_OPT_SHAPE, shape)
+        if shape is not None:  # (launch shape, voxel layout)
+            b.set_option(C.BATCH_OPT_SHAPE, shape[0])
+            b.set_option(C.BATCH_OPT_LAYOUT, shape[1])
         gs = []
         for m in range(bw.n_maps):
             g = b.add_grid(bw.halves[m], bw.resolution, False, bw.threshold)
@@ -445,7 +468,8 @@ def run_batching(args):
     return {"workload": bw.name, "maps": bw.n_maps, "steps": args.batch_steps,
             "mean_points_per_step": float(pts), "value": vs / (ms.sum() / 1e3), "unit": UNIT,
             "rays_per_s": float(pts * len(ms) / (ms.sum() / 1e3)),
-            "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99), "launch_shape": shape,
+            "p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99), "launch_shape": shape[0],
+            "voxel_layout": shape[1],
             "l2": "flushed between steps (512 MiB write)"}
 
 
@@ -1011,7 +1035,7 @@ def main():
         "data": "synthetic (seeded ray-cast LiDAR scans)",
         "config": headline_config(h["K"]),
         "form": "batched: one walk + one fold launch per step over all maps, CUDA graph replay",
-        "launch_shape": h["shape"],
+        "launch_shape": h["shape"][0], "voxel_layout": h["shape"][1],
         "tuning": f"separate pass before warm-up ({h['tune_updates']} updates of a throw-away "
                   "batch); no timed step runs a candidate shape",
         "parallelism": f"replicas x{world} (map-sharded, no collective)",
@@ -1027,11 +1051,38 @@ def main():
                      "traffic": profiled_traffic(h["K"])[0],
                      "traffic_source": profiled_traffic(h["K"])[1],
                      "algorithmic_bytes": "12 B per point + 8 B per touched voxel (occ read+write); "
-                                          "the fold's 4 B/voxel counter sweep is not algorithmic",
-                     "atomics_per_s": float(np.mean(h["incs"]) / (np.mean(h["walk_ms"]) / 1e3))},
+                                          "the fold reads and writes whole 128-byte lines of the "
+                                          "lines the walk flagged",
+                     },
+        "recenter": ({"fired": len(h["clear_ms"]),
+                      "clear_ms_mean": float(np.mean(h["clear_ms"])),
+                      "cleared_voxels_mean": float(np.mean(h["cleared"])),
+                      "gb_per_s": float(4.0 * np.sum(h["cleared"]) / (np.sum(h["clear_ms"]) / 1e3)
+                                        / 1e9),
+                      "peak_gbs": h["peak"],
+                      "note": "device time of the slab clear of each recenter that fired "
+                              "(4 m threshold, about every 27 scans; 4 B written per cleared "
+                              "voxel); the reference publishes 4.822 ms per recenter on an "
+                              "RTX 3090 (README.md:35)"}
+                     if h["clear_ms"] else {"fired": 0}),
+        "fetch": {"centres": 256, "radius_m": 1.5, "filter": "OCCUPIED",
+                  "wall_ms_median": float(np.median(h["fetch_ms"])),
+                  "samples": h["fetch_samples"],
+                  "note": "cublox_grid_fetch_batch on one README map after the drive, samples "
+                          "copied to host, wall time"},
         "gpu_launches": h["launches"],
         "clocks": h["clocks"],
     }
+    red_l2 = C.red_rate(64 << 20, 1 << 30)      # buffer in L2
+    red_hbm = C.red_rate(4 << 30, 1 << 30)      # buffer far beyond L2
+    ach = float(np.mean(h["incs"]) / (np.mean(h["walk_ms"]) / 1e3))
+    out["roofline"]["l2_atomic"] = {
+        "kernel": "batch walk", "achieved": ach, "unit": "atomic adds/s",
+        "peak": red_l2, "frac": ach / red_l2, "peak_beyond_l2": red_hbm,
+        "peak_source": "cublox_probe_red_rate on this GPU, this run (distinct pseudo-random "
+                       "addresses; 64 MiB buffer in L2, and 4 GiB beyond it)",
+        "note": "effective: U + H in-window increments per walk time; the shared-memory "
+                "sensor cube takes part of them off the global atomics"}
     if world == 1 and not args.only_headline:
         out["plain"] = run_plain(args, h)
         out["batching"] = run_batching(args)

@@ -25,6 +25,8 @@ LAYOUT_SOA, LAYOUT_AOS = 0, 1
 DEPTH_U16_MM, DEPTH_F32_M = 0, 1
 OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT, OPT_SEGMENT, OPT_FOLD, OPT_BLOCK, OPT_CONTIGUOUS = (
     1, 2, 3, 4, 5, 6, 7, 8)
+OPT_LAYOUT = 9
+LAYOUTS = (320, 230, 221, 0)  # 8x4x1, 4x8x1, 4x4x2 bricks; the reference's hash order
 
 
 class VoxelState(enum.IntEnum):
@@ -161,6 +163,8 @@ def lib():
             "cublox_server_scratch_bytes": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_uint64)],
                                             ctypes.c_int),
             "cublox_runtime_counters": ([i64, ctypes.c_int], ctypes.c_int),
+            "cublox_probe_red_rate": ([ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                       ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "cublox_batch_reserve_maps": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int64],
                                           ctypes.c_int),
             "cublox_grid_enable_timing": ([G, ctypes.c_int], ctypes.c_int),
@@ -578,6 +582,9 @@ class OccupancyGrid:
 BATCH_OPT_GRAPHS, BATCH_OPT_AUTOTUNE, BATCH_OPT_SHAPE, BATCH_OPT_TIMING, BATCH_OPT_NUM_SHAPES = 1, 2, 3, 4, 5
 BATCH_OPT_FOLD = 6
 BATCH_OPT_TUNING = 7
+BATCH_OPT_LAYOUT = 8
+BATCH_OPT_WAIT_LIMIT, BATCH_OPT_INJECT_MISSING_WALK = 9, 10
+DEVICE_WAIT_TIMEOUT = 1 << 3
 
 
 class Batch:
@@ -798,6 +805,15 @@ class Server:
         v = ctypes.c_uint64()
         _check(lib().cublox_server_scratch_bytes(ctypes.byref(cfg), ctypes.byref(v)), "scratch_bytes")
         return v.value
+
+
+def red_rate(buffer_bytes: int, total_ops: int = 1 << 30, stream: int = 0) -> float:
+    """Atomic adds per second (results unused) to distinct pseudo-random
+    addresses of a buffer_bytes buffer (cublox_probe_red_rate)."""
+    v = ctypes.c_double()
+    _check(lib().cublox_probe_red_rate(int(buffer_bytes), int(total_ops), ctypes.c_void_p(stream),
+                                       ctypes.byref(v)), "probe_red_rate")
+    return v.value
 
 
 COUNTER_NAMES = ("device_allocs", "device_frees", "pinned_allocs", "pinned_frees", "graph_builds")

@@ -7,8 +7,9 @@
 //        ray, the exact walk of ray_walk.cuh), and flushes the cube into the
 //        map's counters.  Points are read in place from one concatenated
 //        x0 y0 z0 x1 ... buffer.
-//  fold  persistent CTAs take (map, voxel range) items and fold counters
-//        into stored log-odds with 16-byte accesses.
+//  fold  persistent CTAs take (map, line range) items; their warps fold the
+//        32-voxel lines the walk flagged, a whole 128-byte line per access
+//        (fold.cuh, fold_lines).
 //
 // The per-step launch sequence reads everything it needs (map descriptors,
 // item lists and counts) from device buffers, so it can be captured once
@@ -52,17 +53,17 @@ struct WalkItem {
 };
 
 struct FoldItem {
-  int map, g4_start, g4_count, tail;  // tail: handle the vnum % 4 voxels
+  int map, start, count, pad;  // lines [start, start + count) of the map
 };
 
 // counters: [0] walk queue, [1] walk items, [2] fold queue, [3] fold items,
 // [4] a fused launch's fold wait gave up (the rest of the launch then skips
-// its waits and folds)
-constexpr int kCounters = 5;
-constexpr int kFoldItemGroups = 1 << 12;  // 16-byte counter groups per fold item
+// its waits and folds), [5] the fused launch's wait limit (sleep rounds)
+constexpr int kCounters = 6;
+constexpr int kFoldItemLines = 1 << 12;  // 32-voxel lines per fold item
 // Fused launch: how long a fold item waits for its map's walk items
-// (iterations of a ~256 ns sleep, about 2 s) before it gives up and flags
-// kErrWaitTimeout in the map's error word.
+// (rounds of a ~256 ns sleep, about 2 s) before it gives up and flags
+// kErrWaitTimeout in the map's error word (CUBLOX_BATCH_OPT_WAIT_LIMIT).
 constexpr int kWaitIters = 1 << 23;
 
 // Near phase of the two-phase walk (far_walk.cuh), from the ray's start.
@@ -111,20 +112,7 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
     apply_end<S>(p, cube, re, incs, hits);
   }
   __syncthreads();
-  if constexpr (S > 0) {
-    // Only in-window voxels reach the cube, so every non-zero cell hashes
-    // inside the map.
-    for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
-      const uint32_t v = cube[q];
-      if (!v) continue;
-      const int g[3] = {clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S};
-      const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-                     (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
-                        p.map[2] +
-                    (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
-      atomicAdd(p.cnt + h, v);
-    }
-  }
+  flush_cube<S>(p, cube, clo);
   if (p.stats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -146,15 +134,15 @@ __device__ __forceinline__ FoldView fold_view(const MapDesc &m) {
                   m.l_unknown, m.ray.fp};
 }
 
-// One fold item: counter groups [g4_start, g4_start + g4_count), plus the
-// vnum % 4 tail on the map's first item.
-template <int U, bool kL2>
+// One fold item: the flagged lines among [start, start + count), the CTA's
+// warps taking groups of 32 lines in turn.  kAll: fold every line of the
+// item, flagged or not (the reference's full sweep, for comparison).
+template <bool kL2, bool kAll = false>
 __device__ __forceinline__ uint32_t fold_item(const MapDesc &m, const FoldItem &item) {
   const FoldView v = fold_view(m);
-  uint32_t touched = fold_groups<U, kL2>(v, item.g4_start + threadIdx.x,
-                                         item.g4_start + item.g4_count, blockDim.x);
-  if (item.tail) touched += fold_tail(v);
-  return touched;
+  const int warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  return fold_lines<4, kL2, kAll>(v, m.ray.dirty, item.start + 32 * warp, item.start + item.count,
+                                  32 * warps);
 }
 
 __device__ __forceinline__ void add_touched(const MapDesc &m, uint32_t t) {
@@ -239,18 +227,7 @@ __global__ void __launch_bounds__(1024) batch_walk_wq_kernel(const MapDesc *maps
       apply_end<S>(p, cube, re, incs, hits);
     }
     __syncthreads();
-    if constexpr (S > 0) {
-      for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
-        const uint32_t v = cube[q];
-        if (!v) continue;
-        const int g[3] = {clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S};
-        const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-                       (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
-                          p.map[2] +
-                      (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
-        atomicAdd(p.cnt + h, v);
-      }
-    }
+    flush_cube<S>(p, cube, clo);
     if (p.stats) {
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
@@ -269,9 +246,9 @@ __global__ void __launch_bounds__(1024) batch_walk_wq_kernel(const MapDesc *maps
   }
 }
 
-// Persistent fold: CTAs take fold items from counters[2].  U: counter
-// groups in flight per thread (fewer registers, more resident warps).
-template <int U>
+// Persistent fold: CTAs take fold items from counters[2].  kAll: every
+// line, not only the flagged ones.
+template <bool kAll>
 __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
                                                          const FoldItem *items,
                                                          int *counters) {
@@ -285,153 +262,8 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
     if (it >= n_items) break;
     const FoldItem item = items[it];
     const MapDesc &m = maps[item.map];
-    add_touched(m, fold_item<U, false>(m, item));
+    add_touched(m, fold_item<false, kAll>(m, item));
   }
-}
-
-// ---- fold with the counter sweep on the bulk-copy engine ------------------
-// The counters of a fold item stream into shared memory in 16 KB chunks by
-// cp.async.bulk (no registers, no per-thread latency), kBulkStages chunks in
-// flight, each completing an mbarrier; the threads only look at the chunk in
-// shared memory and spend their loads on the stored values of the groups that
-// have a set counter (all of a thread's such loads of a chunk are issued
-// together).  Every wait is bounded: one that gives up flags
-// kErrWaitTimeout, skips the rest of the launch's folds and still waits
-// (bounded) for the copies it issued before the CTA exits.
-constexpr int kBulkGroups = 1024;  // 16-byte counter groups per chunk (16 KB)
-constexpr int kBulkStages = 4;
-constexpr size_t kBulkSmem = sizeof(uint4) * kBulkGroups * kBulkStages;
-constexpr int kBulkSpin = 1 << 24;  // try_wait polls before a wait gives up
-constexpr int kBulkItemGroups = 1 << 16;  // groups per fold item of this kernel
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// Issue one chunk: arm the barrier with its byte count, start the copy.
-__device__ __forceinline__ void bulk_chunk(void *dst, const void *src, uint32_t bytes,
-                                           uint64_t *bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int i = 0; i < kBulkSpin; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__global__ void __launch_bounds__(256) batch_fold_bulk_kernel(const MapDesc *maps,
-                                                              const FoldItem *items,
-                                                              int *counters) {
-  extern __shared__ __align__(128) uint4 stage[];  // kBulkStages x kBulkGroups
-  __shared__ __align__(8) uint64_t bar[kBulkStages];
-  __shared__ int s_item, s_ok;
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < kBulkStages; ++i) mbar_init(&bar[i]);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  uint32_t parity = 0;   // bit i: phase parity of stage i's next completion
-  uint32_t pending = 0;  // bit i: a copy into stage i is in flight
-  const int n_items = counters[3];
-  for (;;) {
-    if (threadIdx.x == 0)
-      s_item = *reinterpret_cast<volatile int *>(counters + 4) ? n_items
-                                                               : atomicAdd(&counters[2], 1);
-    __syncthreads();
-    const int it = s_item;
-    if (it >= n_items) break;
-    const FoldItem item = items[it];
-    const MapDesc &m = maps[item.map];
-    const FoldView v = fold_view(m);
-    const uint4 *src = reinterpret_cast<const uint4 *>(v.cnt) + item.g4_start;
-    uint4 *c4 = reinterpret_cast<uint4 *>(v.cnt) + item.g4_start;
-    float4 *o4 = reinterpret_cast<float4 *>(v.occ) + item.g4_start;
-    const int n_chunks = (item.g4_count + kBulkGroups - 1) / kBulkGroups;
-    auto chunk_groups = [&](int c) { return min(kBulkGroups, item.g4_count - c * kBulkGroups); };
-    if (threadIdx.x == 0)
-      for (int c = 0; c < min(kBulkStages, n_chunks); ++c) {
-        bulk_chunk(stage + c * kBulkGroups, src + c * kBulkGroups, 16u * chunk_groups(c), &bar[c]);
-        pending |= 1u << c;
-      }
-    uint32_t touched = 0;
-    bool ok = true;
-    for (int c = 0; c < n_chunks; ++c) {
-      const int st = c % kBulkStages;
-      // every thread waits for the chunk; the vote keeps the decision uniform
-      const bool got = __syncthreads_and(mbar_wait(&bar[st], (parity >> st) & 1u));
-      if (!got) {
-        ok = false;
-        break;
-      }
-      parity ^= 1u << st;
-      if (threadIdx.x == 0) pending &= ~(1u << st);
-      const uint4 *sc = stage + st * kBulkGroups;
-      const int ng = chunk_groups(c);
-      const int base = c * kBulkGroups;
-      uint4 cv[4];
-      float4 ov[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int q = threadIdx.x + u * 256;
-        cv[u] = q < ng ? sc[q] : make_uint4(0u, 0u, 0u, 0u);
-        ov[u] = any_set(cv[u]) ? o4[base + q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (!any_set(cv[u])) continue;
-        const int g = base + threadIdx.x + u * 256;
-        const int h = (item.g4_start + g) << 2;
-        if (cv[u].x) { ov[u].x = fold_counter(v, h + 0, cv[u].x, ov[u].x); ++touched; }
-        if (cv[u].y) { ov[u].y = fold_counter(v, h + 1, cv[u].y, ov[u].y); ++touched; }
-        if (cv[u].z) { ov[u].z = fold_counter(v, h + 2, cv[u].z, ov[u].z); ++touched; }
-        if (cv[u].w) { ov[u].w = fold_counter(v, h + 3, cv[u].w, ov[u].w); ++touched; }
-        o4[g] = ov[u];
-        c4[g] = make_uint4(0u, 0u, 0u, 0u);
-      }
-      __syncthreads();  // stage st is free again
-      if (threadIdx.x == 0 && c + kBulkStages < n_chunks) {
-        const int nc = c + kBulkStages;
-        bulk_chunk(stage + st * kBulkGroups, src + nc * kBulkGroups, 16u * chunk_groups(nc),
-                   &bar[st]);
-        pending |= 1u << st;
-      }
-    }
-    if (threadIdx.x == 0) s_ok = ok;
-    __syncthreads();
-    if (!s_ok) {
-      if (threadIdx.x == 0) {
-        atomicOr(m.ray.err, kErrWaitTimeout);
-        atomicExch(counters + 4, 1);
-      }
-      break;
-    }
-    if (item.tail) touched += fold_tail(v);
-    add_touched(m, touched);
-  }
-  // copies still in flight (only after a wait gave up): bounded wait
-  if (threadIdx.x == 0)
-    for (int i = 0; i < kBulkStages; ++i)
-      if (pending & (1u << i)) mbar_wait(&bar[i], (parity >> i) & 1u);
 }
 
 // Walk and fold in one persistent launch.  Items come from one queue, in
@@ -472,7 +304,8 @@ __global__ void __launch_bounds__(1024) batch_fused_kernel(const MapDesc *maps,
         volatile int *vd = done + item.map;
         volatile int *gave_up = counters + 4;
         int ok = 0;
-        for (int k = 0; k < kWaitIters && !*gave_up; ++k) {
+        const int limit = counters[5];
+        for (int k = 0; k < limit && !*gave_up; ++k) {
           if (*vd >= m.n_walk) {
             ok = 1;
             break;
@@ -487,7 +320,7 @@ __global__ void __launch_bounds__(1024) batch_fused_kernel(const MapDesc *maps,
         s_ok = ok;
       }
       __syncthreads();
-      if (s_ok) add_touched(m, fold_item<2, true>(m, item));
+      if (s_ok) add_touched(m, fold_item<true>(m, item));
       __syncthreads();
     }
   }
@@ -507,6 +340,17 @@ const Shape kShapes[] = {{32, 512, 512, 0, 1, 0},  {32, 1024, 1024, 0, 1, 0},
                          {16, 0, 512, 0, 1, 1},    {16, 1024, 1024, 0, 2, 0},
                          {32, 1024, 1024, 1, 1, 0}, {16, 512, 512, 1, 1, 0}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+// The tuner's candidates: every launch shape with the default voxel layout
+// (8 x 4 x 1 bricks), then the first shape with the other layouts (4 x 8 x
+// 1 and 4 x 4 x 2 bricks, the reference's hash order).  A candidate with
+// another layout moves every grid of the update to it first.
+struct Candidate {
+  int shape, layout;
+};
+const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320}, {5, 320},
+                                 {6, 320}, {7, 320}, {0, 230}, {0, 221}, {0, 0}};
+constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {
   static int n = 0;
@@ -583,35 +427,13 @@ cudaError_t launch_walk(const MapDesc *maps, const WalkItem *witems, const FoldI
                           s);
 }
 
-int bulk_fold_ctas() {
-  static int grid = 0;
-  if (grid == 0) {
-    const int smem = static_cast<int>(kBulkSmem);
-    if (cudaFuncSetAttribute(batch_fold_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem) != cudaSuccess)
-      cudaGetLastError();
-    int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_fold_bulk_kernel, 256,
-                                                      kBulkSmem) != cudaSuccess) {
-      cudaGetLastError();
-      per_sm = 1;
-    }
-    grid = sm_count_batch() * (per_sm < 1 ? 1 : per_sm);
-  }
-  return grid;
-}
-
 cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counters,
                         int variant, cudaStream_t s) {
   const dim3 grid(sm_count_batch() * 8), block(256);
-  switch (variant) {
-    case 1: batch_fold_kernel<4><<<grid, block, 0, s>>>(maps, fitems, counters); break;
-    case 2: batch_fold_kernel<1><<<grid, block, 0, s>>>(maps, fitems, counters); break;
-    case 3:
-      batch_fold_bulk_kernel<<<bulk_fold_ctas(), block, kBulkSmem, s>>>(maps, fitems, counters);
-      break;
-    default: batch_fold_kernel<2><<<grid, block, 0, s>>>(maps, fitems, counters); break;
-  }
+  if (variant == 1)
+    batch_fold_kernel<true><<<grid, block, 0, s>>>(maps, fitems, counters);
+  else
+    batch_fold_kernel<false><<<grid, block, 0, s>>>(maps, fitems, counters);
   return cudaGetLastError();
 }
 
@@ -642,6 +464,9 @@ struct cublox_batch {
   cudaEvent_t staged = nullptr;  // host staging free again
   // shape choice
   int shape = 0;
+  int layout = detail::kDefaultLayout;  // voxel layout of the batch's grids
+  int wait_limit = kWaitIters;  // fused launch: sleep rounds a fold item waits
+  bool inject_missing_walk = false;  // test hook (CUBLOX_BATCH_OPT_INJECT_MISSING_WALK)
   bool autotune = true;
   int tune_step = 0;
   int tune_rounds = 2;
@@ -793,7 +618,6 @@ int cublox_batch_create(void *stream, cublox_batch **out) {
   }
   for (int i = 0; i < 4; ++i) cudaEventCreate(&b->ev[i]);
   for (int i = 0; i < kNumShapes; ++i) shape_grid(i);
-  bulk_fold_ctas();
   *out = b;
   return CUBLOX_OK;
 }
@@ -849,11 +673,23 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
       b->shape = value;
       b->autotune = false;
       return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_LAYOUT:
+      if (!detail::layout_valid(value)) break;
+      b->layout = value;
+      b->autotune = false;
+      return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_WAIT_LIMIT:
+      if (value < 1) break;
+      b->wait_limit = value;
+      return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_INJECT_MISSING_WALK:
+      b->inject_missing_walk = value != 0;
+      return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_TIMING:
       b->timed = value != 0;
       return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD:
-      if (value < 0 || value > 3) break;
+      if (value < 0 || value > 1) break;
       b->fold_variant = value;
       drop_graph(b);
       return CUBLOX_OK;
@@ -869,11 +705,14 @@ int cublox_batch_get_option(const cublox_batch *b, int key, int *value) {
     case CUBLOX_BATCH_OPT_GRAPHS: *value = b->graphs; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_AUTOTUNE: *value = b->autotune; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_SHAPE: *value = b->shape; return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_LAYOUT: *value = b->layout; return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_WAIT_LIMIT: *value = b->wait_limit; return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_INJECT_MISSING_WALK: *value = b->inject_missing_walk; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_TIMING: *value = b->timed; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_NUM_SHAPES: *value = kNumShapes; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD: *value = b->fold_variant; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_TUNING:
-      *value = b->autotune && b->tune_step < kNumShapes * b->tune_rounds;
+      *value = b->autotune && b->tune_step < kNumCandidates * b->tune_rounds;
       return CUBLOX_OK;
     default: break;
   }
@@ -896,20 +735,24 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   }
   const int64_t total = offsets[n] - offsets[0];
   if (total <= 0) return CUBLOX_OK;  // every scan empty: nothing changes
-  const int shape = b->autotune ? (b->tune_step / b->tune_rounds) % kNumShapes : b->shape;
-  const bool tuning = b->autotune && b->tune_step < kNumShapes * b->tune_rounds;
-  const int active_shape = tuning ? shape : b->shape;
+  const bool tuning = b->autotune && b->tune_step < kNumCandidates * b->tune_rounds;
+  const int cand = tuning ? (b->tune_step / b->tune_rounds) % kNumCandidates : -1;
+  const int active_shape = tuning ? kCandidates[cand].shape : b->shape;
+  const int active_layout = tuning ? kCandidates[cand].layout : b->layout;
+  // the grids' voxel layout (moved between scans, on the batch's stream)
+  for (int i = 0; i < n; ++i) {
+    if (grids[i]->lay_code == active_layout) continue;
+    const int rc = detail::set_layout(grids[i], active_layout);
+    if (rc) return rc;
+  }
   const Shape &sh = kShapes[active_shape];
   const int rays_per_item = shape_rays(active_shape, total);
-  const int fold_groups_per_item =
-      (!sh.fused && b->fold_variant == 3) ? kBulkItemGroups : kFoldItemGroups;
   // work items
   int n_w = 0, n_f = 0;
   for (int i = 0; i < n; ++i) {
     const int64_t c = offsets[i + 1] - offsets[i];
     n_w += static_cast<int>((c + rays_per_item - 1) / rays_per_item);
-    const int64_t g4 = grids[i]->voxel_num >> 2;
-    n_f += static_cast<int>((g4 + fold_groups_per_item - 1) / fold_groups_per_item) + 1;
+    n_f += (grids[i]->nlines + kFoldItemLines - 1) / kFoldItemLines;
   }
   // a fused shape queues walk and fold items in one list
   int rc = ensure_capacity(b, n, std::max(sh.fused ? n_w + n_f : n_w, 1), std::max(n_f, 1));
@@ -965,11 +808,12 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     md.n_walk = 0;
     for (int s0 = 0; s0 < c; s0 += rays_per_item, ++md.n_walk)
       b->h_witems[w++] = WalkItem{d, s0, std::min(rays_per_item, c - s0), 0};
-    const int g4 = g->voxel_num >> 2;
-    for (int s0 = 0; s0 < g4 || (s0 == 0 && g4 == 0); s0 += fold_groups_per_item) {
-      b->h_fitems[f++] = FoldItem{d, s0, std::min(fold_groups_per_item, g4 - s0), s0 == 0 ? 1 : 0};
-      if (g4 == 0) break;
-    }
+    for (int l0 = 0; l0 < g->nlines; l0 += kFoldItemLines)
+      b->h_fitems[f++] = FoldItem{d, l0, std::min(kFoldItemLines, g->nlines - l0), 0};
+    // test hook: the map's folds wait for one walk item more than it has,
+    // so a fused launch's bounded wait runs out (the walk items themselves
+    // are unchanged)
+    if (b->inject_missing_walk && d == 0) ++md.n_walk;
     w_end.push_back(w);
     f_end.push_back(f);
     ++d;
@@ -981,7 +825,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     auto put_fold = [&](int map) {
       for (int i = map ? f_end[map - 1] : 0; i < f_end[map]; ++i) {
         const FoldItem &fi = b->h_fitems[i];
-        b->h_witems[w++] = WalkItem{~fi.map, fi.g4_start, fi.g4_count, fi.tail};
+        b->h_witems[w++] = WalkItem{~fi.map, fi.start, fi.count, fi.pad};
       }
     };
     std::vector<WalkItem> order;
@@ -1002,6 +846,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     f = 0;
   }
   b->h_counters[0] = b->h_counters[2] = b->h_counters[4] = 0;
+  b->h_counters[5] = b->wait_limit;
   b->h_counters[1] = sh.wq ? d : w;  // the warp-queue walk reads maps, not items
   b->h_counters[3] = f;
   cudaError_t e;
@@ -1050,14 +895,16 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     float ms = 0.0f;  // walk + fold
     cudaEventSynchronize(b->ev[2]);
     cudaEventElapsedTime(&ms, b->ev[0], b->ev[2]);
-    if (static_cast<int>(b->tune_ms.size()) < kNumShapes) b->tune_ms.assign(kNumShapes, 0.0f);
-    b->tune_ms[active_shape] += ms;
+    if (static_cast<int>(b->tune_ms.size()) < kNumCandidates)
+      b->tune_ms.assign(kNumCandidates, 0.0f);
+    b->tune_ms[cand] += ms;
     ++b->tune_step;
-    if (b->tune_step >= kNumShapes * b->tune_rounds) {
+    if (b->tune_step >= kNumCandidates * b->tune_rounds) {
       int best = 0;
-      for (int s = 1; s < kNumShapes; ++s)
-        if (b->tune_ms[s] < b->tune_ms[best]) best = s;
-      b->shape = best;
+      for (int c = 1; c < kNumCandidates; ++c)
+        if (b->tune_ms[c] < b->tune_ms[best]) best = c;
+      b->shape = kCandidates[best].shape;
+      b->layout = kCandidates[best].layout;
     }
   }
   return CUBLOX_OK;
@@ -1081,7 +928,7 @@ int cublox_batch_reserve_maps(cublox_batch *b, int64_t points, int maps, int64_t
   // fold items: per map ceil(voxels / 4 / groups per item) + 1 (the tail
   // item); walk items: at least 256 rays each (every shape), one partial
   // item per map, and a fused shape queues the fold items behind them
-  const int64_t folds = voxels / (4 * static_cast<int64_t>(kFoldItemGroups)) + 2 * maps + 1;
+  const int64_t folds = voxels / (32 * static_cast<int64_t>(kFoldItemLines)) + 2 * maps + 1;
   const int64_t walks = points / 256 + maps + 1;
   if (folds + walks > (int64_t(1) << 30))
     return fail(CUBLOX_ERR_INVALID, "batch_reserve_maps: too many work items");

@@ -141,6 +141,7 @@ int cublox_binary_version(int *binary_version) {
 }
 
 static void free_all(cublox_grid *g) {
+  cublox_b200::detail::dfree(g->d_dirty);
   cublox_b200::detail::dfree(g->d_occ);
   cublox_b200::detail::dfree(g->d_cnt);
   cublox_b200::detail::dfree(g->d_hit);
@@ -186,6 +187,106 @@ static void set_origin(cublox_grid *g, const int o[3]) {
   }
 }
 
+}  // extern "C"
+
+// Layout of a map's arrays for a layout code (log2 brick sides as digits
+// x y z; 0: the reference's hash order).  Returns the voxels each array
+// needs (padding included, a multiple of 32) and sets the bricks per axis.
+static int64_t make_layout(const int map[3], int code, VoxLayout *L, int nbr[3]) {
+  if (code == 0) {
+    for (int a = 0; a < 3; ++a) {
+      L->lb[a] = 0;
+      nbr[a] = map[a];
+    }
+    L->bs[0] = map[1] * map[2];
+    L->bs[1] = map[2];
+    L->bs[2] = 1;
+    for (int a = 0; a < 3; ++a) L->is[a] = L->bs[a];
+    const int64_t v = static_cast<int64_t>(map[0]) * map[1] * map[2];
+    return (v + 31) & ~int64_t(31);
+  }
+  const int lb[3] = {code / 100, (code / 10) % 10, code % 10};
+  for (int a = 0; a < 3; ++a) {
+    L->lb[a] = lb[a];
+    nbr[a] = (map[a] + (1 << lb[a]) - 1) >> lb[a];
+  }
+  const int vb = 1 << (lb[0] + lb[1] + lb[2]);
+  const int64_t n = static_cast<int64_t>(nbr[0]) * nbr[1] * nbr[2] * vb;
+  if (n > (int64_t(1) << 31)) return n;  // the caller refuses it
+  L->bs[0] = nbr[1] * nbr[2] * vb;
+  L->bs[1] = nbr[2] * vb;
+  L->bs[2] = vb;
+  L->is[0] = 1 << (lb[1] + lb[2]);
+  L->is[1] = 1 << lb[2];
+  L->is[2] = 1;
+  return n;
+}
+
+size_t cublox_b200::detail::voxel_bytes_for(const int half[3]) {
+  int map[3];
+  for (int a = 0; a < 3; ++a) map[a] = 2 * half[a] + 1;
+  int64_t nalloc = 0;
+  for (int code : kLayouts) {
+    VoxLayout l{};
+    int nb[3];
+    const int64_t n = make_layout(map, code, &l, nb);
+    if (n <= (int64_t(1) << 31)) nalloc = std::max(nalloc, n);
+  }
+  return 12 * static_cast<size_t>(nalloc) + static_cast<size_t>(nalloc >> kLineShift);
+}
+
+bool cublox_b200::detail::layout_valid(int code) {
+  if (code == 0) return true;
+  if (code < 0 || code > 999) return false;
+  const int d[3] = {code / 100, (code / 10) % 10, code % 10};
+  return d[0] + d[1] + d[2] == kLineShift;  // one brick = one 32-voxel line
+}
+
+// The address of the voxel with reference hash h.
+static int hash_addr(const cublox_grid *g, int h) {
+  const int nyz = g->map[1] * g->map[2];
+  const int sx = h / nyz, r = h - sx * nyz;
+  const int sy = r / g->map[2], sz = r - sy * g->map[2];
+  return vox_addr(g->lay, sx, sy, sz);
+}
+
+void cublox_b200::detail::layout_to_reference(const cublox_grid *g, const float *arr,
+                                              float *ref) {
+  size_t h = 0;
+  for (int sx = 0; sx < g->map[0]; ++sx) {
+    const int ox = vox_axis(g->lay, 0, sx);
+    for (int sy = 0; sy < g->map[1]; ++sy) {
+      const int oxy = ox + vox_axis(g->lay, 1, sy);
+      for (int sz = 0; sz < g->map[2]; ++sz) ref[h++] = arr[oxy + vox_axis(g->lay, 2, sz)];
+    }
+  }
+}
+
+int cublox_b200::detail::set_layout(cublox_grid *g, int code) {
+  if (!layout_valid(code)) return fail(CUBLOX_ERR_INVALID, "layout: bricks must hold 32 voxels");
+  if (code == g->lay_code) return CUBLOX_OK;
+  VoxLayout nl{};
+  int nbr[3];
+  const int64_t n = make_layout(g->map, code, &nl, nbr);
+  if (n > g->nalloc)
+    return fail(CUBLOX_ERR_INVALID, "layout: needs more voxels than the grid holds");
+  if (!g->d_occ) return fail(CUBLOX_ERR_INVALID, "layout: the grid's buffers are released");
+  // occ -> the reference order in hit (zero between scans) -> occ
+  float *tmp = reinterpret_cast<float *>(g->d_hit);
+  launch_relayout(g->d_occ, tmp, g->lay, g->map, 1, g->stream);
+  CK_LAUNCH();
+  CK(cudaMemsetAsync(g->d_occ, 0, sizeof(float) * static_cast<size_t>(g->nalloc), g->stream));
+  launch_relayout(tmp, g->d_occ, nl, g->map, 0, g->stream);
+  CK_LAUNCH();
+  CK(cudaMemsetAsync(g->d_hit, 0, sizeof(uint32_t) * static_cast<size_t>(g->nalloc), g->stream));
+  g->lay = nl;
+  g->lay_code = code;
+  for (int a = 0; a < 3; ++a) g->nbr[a] = nbr[a];
+  return CUBLOX_OK;
+}
+
+extern "C" {
+
 int cublox_grid_create(const int half_map_size[3], float resolution,
                        int origin_at_center, int has_recenter_threshold,
                        double recenter_threshold, const float origin[3],
@@ -215,6 +316,24 @@ int cublox_grid_create(const int half_map_size[3], float resolution,
     g->map[a] = 2 * half_map_size[a] + 1;
   }
   g->voxel_num = static_cast<int>(total);
+  // arrays sized for every layout the grid may switch to (that fits int32
+  // addresses); the default layout unless it alone does not fit
+  g->nalloc = 0;
+  for (int code : cublox_b200::detail::kLayouts) {
+    VoxLayout l{};
+    int nb[3];
+    const int64_t n = make_layout(g->map, code, &l, nb);
+    if (n <= (int64_t(1) << 31)) g->nalloc = std::max(g->nalloc, n);
+  }
+  {
+    int nb[3];
+    int code = cublox_b200::detail::kDefaultLayout;
+    if (make_layout(g->map, code, &g->lay, nb) > g->nalloc) code = 0;
+    make_layout(g->map, code, &g->lay, nb);
+    g->lay_code = code;
+    for (int a = 0; a < 3; ++a) g->nbr[a] = nb[a];
+  }
+  g->nlines = static_cast<int>(g->nalloc >> kLineShift);
   g->has_thr = has_recenter_threshold != 0;
   if (g->has_thr) {
     const float t = static_cast<float>(recenter_threshold);
@@ -246,16 +365,20 @@ int cublox_grid_create(const int half_map_size[3], float resolution,
       return bail(e, "cudaStreamCreate");
     g->own_stream = true;
   }
-  const size_t n = static_cast<size_t>(g->voxel_num);
+  const size_t n = static_cast<size_t>(g->nalloc);
+  if ((e = cublox_b200::detail::dmalloc(&g->d_dirty, static_cast<size_t>(g->nlines))) != cudaSuccess) return bail(e, "cudaMalloc line flags");
+  if ((e = cudaMemsetAsync(g->d_dirty, 0, static_cast<size_t>(g->nlines), g->stream)) != cudaSuccess) return bail(e, "memset line flags");
   if ((e = cublox_b200::detail::dmalloc(&g->d_occ, n * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc occ");
   if ((e = cublox_b200::detail::dmalloc(&g->d_cnt, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc cnt");
   if ((e = cublox_b200::detail::dmalloc(&g->d_hit, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc hit");
   if ((e = cublox_b200::detail::dmalloc(&g->d_stats, 4 * sizeof(unsigned long long))) != cudaSuccess) return bail(e, "cudaMalloc stats");
   if ((e = cublox_b200::detail::dmalloc(&g->d_err, sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc err");
+  // recenter plan: slab masks, then (brick layouts) brick lists of up to
+  // map[a] entries per axis
   int words = 0;
   for (int a = 0; a < 3; ++a) {
     g->mask_words[a] = (g->map[a] + 31) / 32;
-    words += g->mask_words[a];
+    words += g->mask_words[a] + g->map[a];
   }
   if ((e = cublox_b200::detail::dmalloc(&g->d_masks, words * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc masks");
   // pinned staging of the recenter masks, two halves used in turn
@@ -284,10 +407,11 @@ int cublox_grid_destroy(cublox_grid *g) {
 
 int cublox_grid_reset(cublox_grid *g) {
   if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
-  const size_t n = static_cast<size_t>(g->voxel_num);
+  const size_t n = static_cast<size_t>(g->nalloc);
   CK(cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream));
   CK(cudaMemsetAsync(g->d_cnt, 0, n * sizeof(uint32_t), g->stream));
   CK(cudaMemsetAsync(g->d_hit, 0, n * sizeof(uint32_t), g->stream));
+  CK(cudaMemsetAsync(g->d_dirty, 0, static_cast<size_t>(g->nlines), g->stream));
   CK(cudaStreamSynchronize(g->stream));
   g->first_run = true;
   return CUBLOX_OK;
@@ -296,9 +420,10 @@ int cublox_grid_reset(cublox_grid *g) {
 int cublox_grid_reset_voxel(cublox_grid *g, int hash_id) {
   if (!g) return fail(CUBLOX_ERR_INVALID, "null grid");
   if (hash_id < 0 || hash_id >= g->voxel_num) return CUBLOX_OK;
-  CK(cudaMemsetAsync(g->d_occ + hash_id, 0, sizeof(float), g->stream));
-  CK(cudaMemsetAsync(g->d_cnt + hash_id, 0, sizeof(uint32_t), g->stream));
-  CK(cudaMemsetAsync(g->d_hit + hash_id, 0, sizeof(uint32_t), g->stream));
+  const int a = hash_addr(g, hash_id);
+  CK(cudaMemsetAsync(g->d_occ + a, 0, sizeof(float), g->stream));
+  CK(cudaMemsetAsync(g->d_cnt + a, 0, sizeof(uint32_t), g->stream));
+  CK(cudaMemsetAsync(g->d_hit + a, 0, sizeof(uint32_t), g->stream));
   CK(cudaStreamSynchronize(g->stream));
   return CUBLOX_OK;
 }
@@ -341,9 +466,12 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
       g->opt_seg = value;
       return CUBLOX_OK;
     case CUBLOX_OPT_FOLD:
-      if (value != 0 && value != 1) break;
+      if (value < 0 || value > 2) break;
       g->opt_fold = value;
       return CUBLOX_OK;
+    case CUBLOX_OPT_LAYOUT:
+      if (!cublox_b200::detail::layout_valid(value)) break;
+      return cublox_b200::detail::set_layout(g, value);
     case CUBLOX_OPT_BLOCK:
       if (value != 256 && value != 512 && value != 1024) break;
       g->opt_block = value;
@@ -378,6 +506,7 @@ int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
     case CUBLOX_OPT_FOLD: *value = g->opt_fold; return CUBLOX_OK;
     case CUBLOX_OPT_BLOCK: *value = g->opt_block; return CUBLOX_OK;
     case CUBLOX_OPT_CONTIGUOUS: *value = g->opt_contig; return CUBLOX_OK;
+    case CUBLOX_OPT_LAYOUT: *value = g->lay_code; return CUBLOX_OK;
     default: break;
   }
   return fail(CUBLOX_ERR_INVALID, "get_option: unknown key");
@@ -458,6 +587,8 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   p.hit = g->d_hit;
   p.stats = g->stats_on ? g->d_stats : nullptr;
   p.err = g->d_err;
+  p.lay = g->lay;
+  p.dirty = g->d_dirty;
   if ((g->opt_raycast == 1 || (g->opt_raycast == 2 && g->opt_sort)) && n > g->bin_cap) {
     CK(cudaStreamSynchronize(g->stream));
     cublox_b200::detail::dfree(g->d_bins);
@@ -542,9 +673,15 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   a.fp = g->fp;
   a.stats = g->stats_on ? g->d_stats : nullptr;
   a.variant = g->opt_fold;
+  a.dirty = g->d_dirty;
+  a.nlines = g->nlines;
+  a.vnum = static_cast<int>(std::min<int64_t>(g->nalloc, std::numeric_limits<int>::max()));
   tmark(g, 1, 0);
   launch_apply(a, g->stream);
   CK_LAUNCH();
+  // the full sweeps leave the line flags set: clear them
+  if (a.variant != 2)
+    CK(cudaMemsetAsync(g->d_dirty, 0, static_cast<size_t>(g->nlines), g->stream));
   tmark(g, 1, 1);
   return CUBLOX_OK;
 }
@@ -584,11 +721,13 @@ RayParams cublox_b200::detail::ray_params(const cublox_grid *g, const float *x,
   p.hit = g->d_hit;
   p.stats = g->stats_on ? g->d_stats : nullptr;
   p.err = g->d_err;
+  p.lay = g->lay;
+  p.dirty = g->d_dirty;
   return p;
 }
 
 size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
-  size_t b = 12 * static_cast<size_t>(g->d_occ ? g->voxel_num : 0);
+  size_t b = 12 * static_cast<size_t>(g->d_occ ? g->nalloc : 0) + static_cast<size_t>(g->nlines);
   b += sizeof(float) * 3 * (static_cast<size_t>(g->cloud_cap) + static_cast<size_t>(g->world_cap));
   b += g->image_cap;
   b += g->fs.fq_bytes + 13 * static_cast<size_t>(g->fs.fcap) + 13 * static_cast<size_t>(g->qcap);
@@ -600,7 +739,7 @@ size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
 int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
   cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e == cudaSuccess && occ_host && g->d_occ)
-    e = cudaMemcpy(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->voxel_num),
+    e = cudaMemcpy(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->nalloc),
                    cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "release_device", __LINE__);
   cublox_b200::detail::dfree(g->d_occ);
@@ -635,7 +774,7 @@ int cublox_b200::detail::release_scratch(cublox_grid *g) {
 }
 
 int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host) {
-  const size_t n = static_cast<size_t>(g->voxel_num);
+  const size_t n = static_cast<size_t>(g->nalloc);
   cudaError_t e = cudaSuccess;
   if (!g->d_occ) e = cublox_b200::detail::dmalloc(&g->d_occ, n * sizeof(float));
   if (e == cudaSuccess && !g->d_cnt) e = cublox_b200::detail::dmalloc(&g->d_cnt, n * sizeof(uint32_t));
@@ -926,7 +1065,7 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
     max_map = std::max(max_map, g->map[a]);
   }
   if (max_shift >= max_map) {  // kernels.cu:338-347, :652-662
-    CK(cudaMemsetAsync(g->d_occ, 0, sizeof(float) * static_cast<size_t>(g->voxel_num),
+    CK(cudaMemsetAsync(g->d_occ, 0, sizeof(float) * static_cast<size_t>(g->nalloc),
                        g->stream));
     g->last_cleared = g->voxel_num;
     set_origin(g, no);
@@ -969,6 +1108,53 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
     }
     g->last_cleared = g->voxel_num - keep;
   }
+  // Brick layouts: the bricks holding a marked slab, as three lists (x
+  // brick columns, y brick rows, z brick levels).  An x brick column whose
+  // slots are all marked is one contiguous run of the arrays: such columns
+  // are cleared by memsets and left off the list.
+  const bool bricks = g->lay_code != 0;
+  std::vector<int> blist;
+  int nb[3] = {0, 0, 0};
+  std::vector<std::pair<int, int>> x_runs;  // [first, end) brick columns (bricks) or slabs
+  auto marked = [&](int a, int sl) { return ((m[a][sl >> 5] >> (sl & 31)) & 1u) != 0; };
+  if (bricks) {
+    for (int a = 0; a < 3; ++a) {
+      const int B = 1 << g->lay.lb[a];
+      for (int b = 0; b < g->nbr[a]; ++b) {
+        int any = 0, all = 1;
+        for (int sl = b * B; sl < std::min((b + 1) * B, g->map[a]); ++sl) {
+          const bool mk = marked(a, sl);
+          any |= mk;
+          all &= mk;
+        }
+        if (!any) continue;
+        if (a == 0 && all) {
+          if (!x_runs.empty() && x_runs.back().second == b)
+            ++x_runs.back().second;
+          else
+            x_runs.push_back({b, b + 1});
+          continue;
+        }
+        blist.push_back(b);
+        ++nb[a];
+      }
+    }
+  } else {
+    // A marked x slab is one contiguous run of ny*nz values, and
+    // neighbouring marked slabs are neighbouring runs.
+    for (int x = 0; x < g->map[0];) {
+      if (!marked(0, x)) {
+        ++x;
+        continue;
+      }
+      int e = x;
+      while (e < g->map[0] && marked(0, e)) ++e;
+      x_runs.push_back({x, e});
+      x = e;
+    }
+  }
+  const size_t mwords = masks.size();
+  masks.insert(masks.end(), blist.begin(), blist.end());
   const size_t mb = masks.size() * sizeof(uint32_t);
   // Pinned staging in two halves used in turn: a half is reused once the
   // recenter before last has copied out of it, so the host does not wait
@@ -987,28 +1173,33 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
   cp.zmask = g->d_masks + g->mask_words[0] + g->mask_words[1];
   for (int a = 0; a < 3; ++a) cp.map[a] = g->map[a];
   cp.any_z = any_z ? 1 : 0;
+  cp.lay = g->lay;
   tmark(g, 2, 0);
-  // A marked x slab is one contiguous run of ny*nz values, and neighbouring
-  // marked slabs are neighbouring runs: clear each maximal run with one
-  // memset at copy bandwidth; the kernel then clears only y and z slabs.
-  const size_t slab = static_cast<size_t>(g->map[1]) * g->map[2];
-  for (int x = 0; x < g->map[0];) {
-    if (!((m[0][x >> 5] >> (x & 31)) & 1u)) {
-      ++x;
-      continue;
-    }
-    int e = x;
-    while (e < g->map[0] && ((m[0][e >> 5] >> (e & 31)) & 1u)) ++e;
-    CK(cudaMemsetAsync(g->d_occ + static_cast<size_t>(x) * slab, 0,
-                       sizeof(float) * slab * static_cast<size_t>(e - x), g->stream));
-    x = e;
-  }
+  // x runs: memsets at copy bandwidth
+  const size_t run = bricks ? static_cast<size_t>(g->lay.bs[0])
+                            : static_cast<size_t>(g->map[1]) * g->map[2];
+  for (const auto &r : x_runs)
+    CK(cudaMemsetAsync(g->d_occ + static_cast<size_t>(r.first) * run, 0,
+                       sizeof(float) * run * static_cast<size_t>(r.second - r.first),
+                       g->stream));
   cp.x_done = 1;
-  bool any_y = false;
-  for (int w = 0; w < g->mask_words[1]; ++w) any_y = any_y || m[1][w] != 0u;
-  if (any_y || any_z) {
-    launch_clear(cp, g->stream);
-    CK_LAUNCH();
+  if (bricks) {
+    cp.blist = reinterpret_cast<const int *>(g->d_masks + mwords);
+    for (int a = 0; a < 3; ++a) {
+      cp.nb[a] = nb[a];
+      cp.nbr[a] = g->nbr[a];
+    }
+    if (nb[0] + nb[1] + nb[2] > 0) {
+      launch_clear(cp, g->stream);
+      CK_LAUNCH();
+    }
+  } else {
+    bool any_y = false;
+    for (int w = 0; w < g->mask_words[1]; ++w) any_y = any_y || m[1][w] != 0u;
+    if (any_y || any_z) {
+      launch_clear(cp, g->stream);
+      CK_LAUNCH();
+    }
   }
   tmark(g, 2, 1);
   set_origin(g, no);
@@ -1195,6 +1386,7 @@ static int fetch_impl(cublox_grid *g, cudaStream_t st, const float *centers, int
   p.l_occ = g->l_occ;
   p.l_unknown = g->l_unknown;
   p.filter = filter;
+  p.lay = g->lay;
   p.counts = reinterpret_cast<long long *>(base + o_cnt);
   p.offsets = reinterpret_cast<const long long *>(base + o_off);
   p.limits = reinterpret_cast<const long long *>(base + o_lim);
@@ -1424,6 +1616,7 @@ int cublox_grid_query_states(cublox_grid *g, const float *xyz, int n,
   p.l_occ = g->l_occ;
   p.l_unknown = g->l_unknown;
   p.out = g->d_qout;
+  p.lay = g->lay;
   launch_query(p, g->stream);
   CK_LAUNCH();
   CK(cudaMemcpyAsync(out_state, g->d_qout, static_cast<size_t>(n), cudaMemcpyDeviceToHost,
@@ -1436,8 +1629,8 @@ int cublox_grid_stored_at(cublox_grid *g, int hash_id, float *out) {
   if (!g || !out) return fail(CUBLOX_ERR_INVALID, "stored_at: null argument");
   *out = 0.0f;
   if (hash_id < 0 || hash_id >= g->voxel_num) return CUBLOX_OK;
-  CK(cudaMemcpyAsync(out, g->d_occ + hash_id, sizeof(float), cudaMemcpyDeviceToHost,
-                     g->stream));
+  CK(cudaMemcpyAsync(out, g->d_occ + hash_addr(g, hash_id), sizeof(float),
+                     cudaMemcpyDeviceToHost, g->stream));
   CK(cudaStreamSynchronize(g->stream));
   return CUBLOX_OK;
 }
@@ -1478,18 +1671,37 @@ int cublox_grid_set_origin_index(cublox_grid *g, const int origin_i[3]) {
   return CUBLOX_OK;
 }
 
+// The stored log-odds in the reference's hash order: gathered on the device
+// from the grid's layout into the hit array (zero between scans, rezeroed),
+// then copied out.  The reference's own order needs no gather.
 int cublox_grid_export(cublox_grid *g, float *occ_host) {
   if (!g || !occ_host) return fail(CUBLOX_ERR_INVALID, "export: null argument");
-  CK(cudaMemcpyAsync(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->voxel_num),
+  const float *src = g->d_occ;
+  if (g->lay_code != 0) {
+    launch_relayout(g->d_occ, reinterpret_cast<float *>(g->d_hit), g->lay, g->map, 1, g->stream);
+    CK_LAUNCH();
+    src = reinterpret_cast<const float *>(g->d_hit);
+  }
+  CK(cudaMemcpyAsync(occ_host, src, sizeof(float) * static_cast<size_t>(g->voxel_num),
                      cudaMemcpyDeviceToHost, g->stream));
+  if (g->lay_code != 0)
+    CK(cudaMemsetAsync(g->d_hit, 0, sizeof(uint32_t) * static_cast<size_t>(g->nalloc),
+                       g->stream));
   CK(cudaStreamSynchronize(g->stream));
   return CUBLOX_OK;
 }
 
 int cublox_grid_import(cublox_grid *g, const float *occ_host) {
   if (!g || !occ_host) return fail(CUBLOX_ERR_INVALID, "import: null argument");
-  CK(cudaMemcpyAsync(g->d_occ, occ_host, sizeof(float) * static_cast<size_t>(g->voxel_num),
+  float *dst = g->lay_code != 0 ? reinterpret_cast<float *>(g->d_hit) : g->d_occ;
+  CK(cudaMemcpyAsync(dst, occ_host, sizeof(float) * static_cast<size_t>(g->voxel_num),
                      cudaMemcpyHostToDevice, g->stream));
+  if (g->lay_code != 0) {
+    launch_relayout(dst, g->d_occ, g->lay, g->map, 0, g->stream);
+    CK_LAUNCH();
+    CK(cudaMemsetAsync(g->d_hit, 0, sizeof(uint32_t) * static_cast<size_t>(g->nalloc),
+                       g->stream));
+  }
   CK(cudaStreamSynchronize(g->stream));
   return CUBLOX_OK;
 }
@@ -1544,15 +1756,19 @@ int cublox_grid_count_scan(cublox_grid *g, const float *xyz, int n,
     if (rc) return rc;
     CK(cudaStreamSynchronize(g->stream));
   }
-  std::vector<uint32_t> c(g->voxel_num);
-  CK(cudaMemcpyAsync(c.data(), g->d_cnt, vb, cudaMemcpyDeviceToHost, g->stream));
-  CK(cudaMemcpyAsync(hit_out, g->d_hit, vb, cudaMemcpyDeviceToHost, g->stream));
-  CK(cudaMemsetAsync(g->d_cnt, 0, vb, g->stream));
-  CK(cudaMemsetAsync(g->d_hit, 0, vb, g->stream));
+  (void)vb;
+  const size_t ab = sizeof(uint32_t) * static_cast<size_t>(g->nalloc);
+  std::vector<uint32_t> c(static_cast<size_t>(g->nalloc)), hh(static_cast<size_t>(g->nalloc));
+  CK(cudaMemcpyAsync(c.data(), g->d_cnt, ab, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaMemcpyAsync(hh.data(), g->d_hit, ab, cudaMemcpyDeviceToHost, g->stream));
+  CK(cudaMemsetAsync(g->d_cnt, 0, ab, g->stream));
+  CK(cudaMemsetAsync(g->d_hit, 0, ab, g->stream));
+  CK(cudaMemsetAsync(g->d_dirty, 0, static_cast<size_t>(g->nlines), g->stream));
   CK(cudaStreamSynchronize(g->stream));
   for (int h = 0; h < g->voxel_num; ++h) {
-    op_out[h] = static_cast<int32_t>(c[h] & kOpMask);
-    if (!(c[h] & kHitFlag)) hit_out[h] = 0;
+    const int a = hash_addr(g, h);
+    op_out[h] = static_cast<int32_t>(c[a] & kOpMask);
+    hit_out[h] = (c[a] & kHitFlag) ? static_cast<int32_t>(hh[a]) : 0;
   }
   return CUBLOX_OK;
 }

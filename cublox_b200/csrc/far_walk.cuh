@@ -17,18 +17,21 @@ namespace cublox_b200 {
 // counters.  The cube and the window are boxes and a ray moves monotonically
 // on every axis, so once it has left either it never comes back: the far
 // phase needs no per-step box tests, only "steps left on this axis"
-// counters, and keeps the voxel's hash incrementally, with the ring
-// buffer's wrap.  The voxels visited, and so the counts, are those of the
-// single loop.
+// counters, and keeps the voxel's address as a sum of per-axis terms
+// (VoxLayout), each updated from its ring-buffer slot when the walk steps on
+// that axis.  The voxels visited, and so the counts, are those of the single
+// loop.
 
 struct FarWalk {
   float tM[3], tD[3];  // as in RayWalk
   int e[3];     // steps to the endpoint's coordinate on the axis (all 0: at the endpoint)
   int out[3];   // steps the walk can still take on the axis inside the window
-  int wrap[3];  // steps on the axis before its ring-buffer slot wraps
-  int dh[3];    // hash change of one step on the axis
+  int slot[3];  // ring-buffer slot of the current voxel on the axis
+  int st[3];    // step on the axis (-1, 0, 1)
+  int off[3];   // the axis's term of the current voxel's address
   int left;     // loop iterations left (max_steps - k)
-  int h;        // hash of the current voxel
+  int h;        // address of the current voxel
+  int line;     // line this thread flagged last (mark_line)
 };
 
 // The update after the loop (kernels.cu:138-151), fixed at the ray's start:
@@ -65,10 +68,13 @@ template <int S>
 __device__ __forceinline__ void apply_end(const RayParams &p, uint32_t *cube, const RayEnd &r,
                                           uint32_t &incs, uint32_t &hits) {
   if (r.h < 0) return;
-  if (S > 0 && r.c >= 0)
+  if (S > 0 && r.c >= 0) {
     atomicAdd(&cube[r.c], 1u);
-  else
+  } else {
     atomicAdd(p.cnt + r.h, 1u);
+    int last = -1;
+    mark_line(p, r.h, last);
+  }
   ++incs;
   if (r.hit) {
     atomicOr(p.cnt + r.h, kHitFlag);
@@ -77,10 +83,26 @@ __device__ __forceinline__ void apply_end(const RayParams &p, uint32_t *cube, co
   }
 }
 
+// Add an S^3 shared-memory cube of counts (corner clo, global voxel index)
+// into the map's counters and flag their lines.  Only in-window voxels reach
+// the cube, so every non-zero cell has an address in the map.
+template <int S>
+__device__ __forceinline__ void flush_cube(const RayParams &p, const uint32_t *cube,
+                                           const int clo[3]) {
+  if constexpr (S > 0) {
+    for (int q = threadIdx.x; q < S * S * S; q += blockDim.x) {
+      const uint32_t v = cube[q];
+      if (!v) continue;
+      const int h = global_addr(p, clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S);
+      atomicAdd(p.cnt + h, v);
+      if (p.dirty) p.dirty[h >> kLineShift] = 1;
+    }
+  }
+}
+
 // Far-phase state of a walk whose current voxel (loop iteration k, not yet
 // counted) is inside the window.
 __device__ __forceinline__ void to_far(const RayParams &p, const RayWalk &w, int k, FarWalk &f) {
-  const int stride[3] = {p.map[1] * p.map[2], p.map[2], 1};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int d = w.en[a] - w.id[a];
@@ -89,27 +111,30 @@ __device__ __forceinline__ void to_far(const RayParams &p, const RayWalk &w, int
     f.tD[a] = w.tD[a];
     f.e[a] = st > 0 ? d : (st < 0 ? -d : d);
     f.out[a] = st > 0 ? p.half[a] - w.rel[a] : (st < 0 ? p.half[a] + w.rel[a] : kNever);
-    f.wrap[a] = st > 0 ? p.map[a] - 1 - w.slot[a] : (st < 0 ? w.slot[a] : kNever);
-    f.dh[a] = st * stride[a];
+    f.slot[a] = w.slot[a];
+    f.st[a] = st;
+    f.off[a] = vox_axis(p.lay, a, w.slot[a]);
   }
   f.left = w.max_steps - k;
-  f.h = walk_hash(w, p);
+  f.h = f.off[0] + f.off[1] + f.off[2];
+  f.line = -1;
 }
 
-// One step on axis A (the tie rule picked it).  Returns true if the new
-// voxel is outside the window, which ends the loop: the next iteration would
-// break at its step limit, at the endpoint or as out of the window for good.
+// One step on axis A (the tie rule picked it): the slot moves with the ring
+// buffer's wrap and the axis's address term follows it.  Returns true if
+// the new voxel is outside the window, which ends the loop: the next
+// iteration would break at its step limit, at the endpoint or as out of the
+// window for good.
 template <int A>
-__device__ __forceinline__ bool far_step(FarWalk &f, int map_a) {
+__device__ __forceinline__ bool far_step(FarWalk &f, const RayParams &p) {
   f.tM[A] = fadd(f.tM[A], f.tD[A]);
   --f.e[A];
-  if (f.wrap[A] == 0) {
-    f.h += f.dh[A] * (1 - map_a);
-    f.wrap[A] = map_a - 1;
-  } else {
-    f.h += f.dh[A];
-    --f.wrap[A];
-  }
+  int s = f.slot[A] + f.st[A];
+  s = s == p.map[A] ? 0 : (s < 0 ? p.map[A] - 1 : s);
+  f.slot[A] = s;
+  const int o = vox_axis(p.lay, A, s);
+  f.h += o - f.off[A];
+  f.off[A] = o;
   return f.out[A]-- == 0;
 }
 
@@ -127,7 +152,7 @@ __device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, int bud
   int to_end = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    if (f.dh[a] == 0 ? f.e[a] != 0 : f.e[a] < 0) reachable = false;
+    if (f.st[a] == 0 ? f.e[a] != 0 : f.e[a] < 0) reachable = false;
     to_end += f.e[a];
   }
   int n = reachable ? min(lim, to_end) : lim;
@@ -135,12 +160,13 @@ __device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, int bud
   for (int pass = 0; pass < 2; ++pass) {
     for (; n > 0; --n) {
       atomicAdd(p.cnt + f.h, 1u);
+      mark_line(p, f.h, f.line);
       ++done;
       bool gone;
       if (f.tM[0] < f.tM[1]) {
-        gone = f.tM[0] < f.tM[2] ? far_step<0>(f, p.map[0]) : far_step<2>(f, p.map[2]);
+        gone = f.tM[0] < f.tM[2] ? far_step<0>(f, p) : far_step<2>(f, p);
       } else {
-        gone = f.tM[1] < f.tM[2] ? far_step<1>(f, p.map[1]) : far_step<2>(f, p.map[2]);
+        gone = f.tM[1] < f.tM[2] ? far_step<1>(f, p) : far_step<2>(f, p);
       }
       if (gone) {
         f.left -= done;

@@ -84,6 +84,58 @@ __device__ __forceinline__ uint32_t fold_groups(const FoldView &v, int first, in
   return touched;
 }
 
+// Fold of the flagged lines among lines [first, end) by one warp.  The warp
+// looks at 32 line flags at a time (lines base + lane; kAll: every line
+// counts as flagged); each flagged line's counters and stored values are
+// read whole (one 128-byte access per array, kLines lines in flight),
+// folded where a counter is set, written back whole (a full line, so no
+// partial-sector write) with the counters zeroed, and its flag cleared.
+// `stride` is the distance between the warp's successive groups of 32
+// lines.  kL2: flags and counters are read at L2 (ld.global.cg), as a launch
+// that also wrote them from other CTAs needs.  Returns the voxels folded.
+template <int kLines, bool kL2, bool kAll = false>
+__device__ __forceinline__ uint32_t fold_lines(const FoldView &v, uint8_t *dirty, int first,
+                                               int end, int stride) {
+  const int lane = threadIdx.x & 31;
+  uint32_t touched = 0;
+  for (int base = first; base < end; base += stride) {
+    const int l = base + lane;
+    const bool d = l < end && (kAll || (kL2 ? __ldcg(dirty + l) : dirty[l]) != 0);
+    uint32_t mask = __ballot_sync(0xffffffffu, d);
+    if (d) dirty[l] = 0;
+    while (mask) {
+      int at[kLines];
+#pragma unroll
+      for (int k = 0; k < kLines; ++k) {
+        at[k] = -1;
+        if (mask) {
+          at[k] = ((base + __ffs(mask) - 1) << kLineShift) + lane;
+          mask &= mask - 1;
+        }
+      }
+      uint32_t c[kLines];
+      float o[kLines];
+#pragma unroll
+      for (int k = 0; k < kLines; ++k)
+        if (at[k] >= 0) c[k] = kL2 ? __ldcg(v.cnt + at[k]) : v.cnt[at[k]];
+#pragma unroll
+      for (int k = 0; k < kLines; ++k)
+        if (at[k] >= 0) o[k] = v.occ[at[k]];
+#pragma unroll
+      for (int k = 0; k < kLines; ++k) {
+        if (at[k] < 0) continue;
+        if (c[k]) {
+          o[k] = fold_counter(v, at[k], c[k], o[k]);
+          ++touched;
+        }
+        v.occ[at[k]] = o[k];
+        v.cnt[at[k]] = 0u;
+      }
+    }
+  }
+  return touched;
+}
+
 // The vnum % 4 voxels after the last whole group, one per thread 0..2.
 __device__ __forceinline__ uint32_t fold_tail(const FoldView &v) {
   if (threadIdx.x >= static_cast<unsigned>(v.vnum & 3)) return 0;

@@ -46,7 +46,7 @@ struct cublox_grid {
   // kernel options (cublox_grid_set_option)
   int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
   int opt_seg = 64;     // split walk: target in-window steps per lane
-  int opt_fold = 1;     // 0 scalar sweep, 1 vector sweep
+  int opt_fold = 2;     // 0 scalar sweep, 1 vector sweep, 2 flagged lines only
   int opt_block = 512;  // split walk CTA size
   int opt_contig = 0;   // split walk: contiguous segment runs per CTA
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
@@ -69,6 +69,16 @@ struct cublox_grid {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
 
+  // voxel layout of occ / cnt / hit (brick sides, strides) and the voxels
+  // each array holds: the largest padded size of the layouts a grid can
+  // switch between, a multiple of 32, so a layout change needs no new memory
+  cublox_b200::VoxLayout lay{};
+  int lay_code = 0;     // brick sides as log2 digits x y z (320: 8 x 4 x 1)
+  int64_t nalloc = 0;
+  int nlines = 0;       // nalloc / 32
+  uint8_t *d_dirty = nullptr;  // line flags (kernels.cuh)
+  int nbr[3] = {0, 0, 0};      // bricks per axis in the current layout
+
   float *d_occ = nullptr;
   uint32_t *d_cnt = nullptr;
   uint32_t *d_hit = nullptr;
@@ -78,7 +88,7 @@ struct cublox_grid {
   uint32_t *h_masks = nullptr;  // pinned staging of the masks, two halves
   cudaEvent_t mask_ev[2] = {nullptr, nullptr};  // a half free again
   int mask_half = 0;  // the half the next recenter stages into
-  int mask_stage_words = 0;  // words per half
+  int mask_stage_words = 0;  // words per half: slab masks + brick lists
   int mask_words[3] = {0, 0, 0};
 
   float *d_cloud = nullptr;  // SoA [x|y|z]
@@ -123,6 +133,20 @@ inline cudaError_t hfree(const void *p) { return pinned_free(const_cast<void *>(
 
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what, int line);
+// The default voxel layout of new grids (log2 brick sides as digits x y z)
+// and the layouts a grid may switch to: 32-voxel bricks and the reference's
+// hash order (0).
+constexpr int kDefaultLayout = 320;
+constexpr int kLayouts[] = {320, 230, 221, 0};
+bool layout_valid(int code);
+// Device bytes of a grid's voxel arrays and line flags (its largest layout).
+size_t voxel_bytes_for(const int half[3]);
+// Switch a grid's arrays to another layout, moving its stored log-odds
+// (counters are zero between scans).  Enqueued on the grid's stream.
+int set_layout(cublox_grid *g, int code);
+// Stored log-odds in the reference's hash order from a copy of the grid's
+// occ array in its own layout (host memory, nalloc values).
+void layout_to_reference(const cublox_grid *g, const float *arr, float *ref);
 // First update: snap the window origin to the sensor voxel
 // (OccupancyGrid.cpp:192-198).
 void snap_first_run(cublox_grid *g, const float sensor[3]);

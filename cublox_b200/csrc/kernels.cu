@@ -25,12 +25,15 @@ __device__ __forceinline__ bool cast_one(const RayParams &p, float ex,
   RayWalk w;
   if (!ray_begin(p, ex, ey, ez, w)) return false;
   uint32_t incs = 0;
+  int last = -1;  // line flagged last
   for (int step = 0; step < w.max_steps; ++step) {
     if (at_end(w)) break;
     if (kAccount) {
       ++incs;
     } else if (in_window(w, p)) {
-      atomicAdd(p.cnt + walk_hash(w, p), 1u);
+      const int h = walk_hash(w, p);
+      atomicAdd(p.cnt + h, 1u);
+      mark_line(p, h, last);
       ++incs;
     } else if (left_for_good(w, p)) {
       break;
@@ -45,6 +48,7 @@ __device__ __forceinline__ bool cast_one(const RayParams &p, float ex,
   const int h = end_hash(w, p);
   if (h >= 0) {
     atomicAdd(p.cnt + h, 1u);
+    mark_line(p, h, last);
     if (!w.clipped) {
       atomicOr(p.cnt + h, kHitFlag);
       atomicAdd(p.hit + h, 1u);
@@ -154,6 +158,23 @@ __global__ void __launch_bounds__(256) fold_vec_kernel(const ApplyParams p) {
   }
 }
 
+// Fold of the flagged lines only: each warp takes groups of 32 line flags,
+// grid-stride (fold_lines).
+template <bool kStats>
+__global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
+  const FoldView v = fold_view(p);
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t touched = fold_lines<4, false>(v, p.dirty, warp * 32, p.nlines, warps * 32);
+  if (kStats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      touched += __shfl_down_sync(0xffffffffu, touched, off);
+    if ((threadIdx.x & 31) == 0 && touched)
+      atomicAdd(p.stats + 3, static_cast<unsigned long long>(touched));
+  }
+}
+
 // Union-of-slabs clear.  One block per x slot: a marked x slab is one
 // contiguous run of ny*nz floats; otherwise every (x, y) column clears its
 // whole run if y is marked, else the marked z slots.
@@ -197,6 +218,70 @@ __global__ void __launch_bounds__(256) clear_kernel(const ClearParams p) {
         for (int k = lane; k < nzl; k += 32) col[zl[k]] = 0.0f;
       }
     }
+  }
+}
+
+// Union-of-slabs clear for 32-voxel brick layouts: one warp per listed
+// brick, one lane per voxel of it (one 128-byte line).  The bricks are the
+// listed x brick columns crossed with every y and z brick, then the listed y
+// rows, then the listed z levels; a brick on two lists is cleared twice,
+// with the same result.  A lane clears its voxel if its x, y or z slot is
+// marked; lanes of padding slots (past the map) do nothing.
+__global__ void __launch_bounds__(256) clear_bricks_kernel(const ClearParams p) {
+  const int lane = threadIdx.x & 31;
+  const int n0 = p.nb[0] * p.nbr[1] * p.nbr[2];
+  const int n1 = p.nbr[0] * p.nb[1] * p.nbr[2];
+  const int n2 = p.nbr[0] * p.nbr[1] * p.nb[2];
+  const int total = n0 + n1 + n2;
+  const int l12 = p.lay.lb[1] + p.lay.lb[2];
+  const int i0 = lane >> l12;
+  const int i1 = (lane >> p.lay.lb[2]) & ((1 << p.lay.lb[1]) - 1);
+  const int i2 = lane & ((1 << p.lay.lb[2]) - 1);
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < total;
+       k += (gridDim.x * blockDim.x) >> 5) {
+    int b[3];
+    if (k < n0) {
+      b[0] = p.blist[k / (p.nbr[1] * p.nbr[2])];
+      const int r = k % (p.nbr[1] * p.nbr[2]);
+      b[1] = r / p.nbr[2];
+      b[2] = r % p.nbr[2];
+    } else if (k < n0 + n1) {
+      const int kk = k - n0;
+      b[1] = p.blist[p.nb[0] + (kk / p.nbr[2]) % p.nb[1]];
+      b[0] = kk / (p.nb[1] * p.nbr[2]);
+      b[2] = kk % p.nbr[2];
+    } else {
+      const int kk = k - n0 - n1;
+      b[2] = p.blist[p.nb[0] + p.nb[1] + kk % p.nb[2]];
+      b[0] = kk / (p.nbr[1] * p.nb[2]);
+      b[1] = (kk / p.nb[2]) % p.nbr[1];
+    }
+    const int s0 = (b[0] << p.lay.lb[0]) + i0, s1 = (b[1] << p.lay.lb[1]) + i1,
+              s2 = (b[2] << p.lay.lb[2]) + i2;
+    if (s0 >= p.map[0] || s1 >= p.map[1] || s2 >= p.map[2]) continue;
+    const bool clear = ((p.xmask[s0 >> 5] >> (s0 & 31)) & 1u) ||
+                       ((p.ymask[s1 >> 5] >> (s1 & 31)) & 1u) ||
+                       (p.any_z && ((p.zmask[s2 >> 5] >> (s2 & 31)) & 1u));
+    if (clear) p.occ[b[0] * p.lay.bs[0] + b[1] * p.lay.bs[1] + b[2] * p.lay.bs[2] + lane] = 0.0f;
+  }
+}
+
+// Layout <-> the reference's hash order, one thread per hash.
+__global__ void __launch_bounds__(256) relayout_kernel(const float *src, float *dst,
+                                                       const VoxLayout lay, const int ny,
+                                                       const int nz, const long long vnum,
+                                                       const int to_ref) {
+  const long long nyz = static_cast<long long>(ny) * nz;
+  for (long long h = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; h < vnum;
+       h += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int sx = static_cast<int>(h / nyz);
+    const int r = static_cast<int>(h - sx * nyz);
+    const int sy = r / nz, sz = r - sy * nz;
+    const int a = vox_addr(lay, sx, sy, sz);
+    if (to_ref)
+      dst[h] = src[a];
+    else
+      dst[a] = src[h];
   }
 }
 
@@ -247,12 +332,9 @@ __global__ void __launch_bounds__(256) fetch_kernel(const FetchParams p) {
         }
         const float s = sos(d[0], d[1], d[2], (p.fp >> kFpFetchSosShift) & 7u);
         if (!(s > r2)) {
-          const int h =
-              ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) *
-                   p.map[1] +
-               (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
-                  p.map[2] +
-              (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+          const int h = vox_addr(p.lay, global_to_local(g[0], p.map[0], p.half[0]) + p.half[0],
+                                 global_to_local(g[1], p.map[1], p.half[1]) + p.half[1],
+                                 global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
           const float l = fadd(p.occ[h], p.l_unknown);
           state = l >= p.l_occ ? 2 : (l < p.l_free ? 1 : 0);
           keep = p.filter < 0 || static_cast<int>(state) == p.filter;
@@ -308,11 +390,9 @@ __global__ void __launch_bounds__(256) query_kernel(const QueryParams p) {
     }
     uint8_t st = 0;
     if (in) {
-      const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) *
-                         p.map[1] +
-                     (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
-                        p.map[2] +
-                    (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
+      const int h = vox_addr(p.lay, global_to_local(g[0], p.map[0], p.half[0]) + p.half[0],
+                             global_to_local(g[1], p.map[1], p.half[1]) + p.half[1],
+                             global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
       const float l = fadd(p.occ[h], p.l_unknown);
       st = l >= p.l_occ ? 2 : (l < p.l_free ? 1 : 0);
     }
@@ -510,6 +590,18 @@ void launch_step_count(const RayParams &p, cudaStream_t s) {
 }
 
 void launch_apply(const ApplyParams &p, cudaStream_t s) {
+  if (p.variant == 2) {
+    if (p.nlines <= 0) return;
+    const int groups = (p.nlines + 31) / 32;  // one warp per group of 32 lines
+    int grid = (groups + 7) / 8;
+    const int cap = sm_count() * 8;
+    if (grid > cap) grid = cap;
+    if (p.stats)
+      fold_lines_kernel<true><<<grid, 256, 0, s>>>(p);
+    else
+      fold_lines_kernel<false><<<grid, 256, 0, s>>>(p);
+    return;
+  }
   if (p.vnum <= 0) return;
   const int block = 256;
   const int n4 = (p.vnum >> 2) + 1;
@@ -529,7 +621,26 @@ void launch_apply(const ApplyParams &p, cudaStream_t s) {
     apply_sweep_kernel<false><<<grid, block, 0, s>>>(p);
 }
 
+void launch_relayout(const float *src, float *dst, const VoxLayout &lay, const int map[3],
+                     int to_ref, cudaStream_t s) {
+  const long long v = static_cast<long long>(map[0]) * map[1] * map[2];
+  if (v <= 0) return;
+  long long grid = (v + 255) / 256;
+  if (grid > sm_count() * 32) grid = sm_count() * 32;
+  relayout_kernel<<<static_cast<int>(grid), 256, 0, s>>>(src, dst, lay, map[1], map[2], v, to_ref);
+}
+
 void launch_clear(const ClearParams &p, cudaStream_t s) {
+  if (p.blist) {
+    const long long total = static_cast<long long>(p.nb[0]) * p.nbr[1] * p.nbr[2] +
+                            static_cast<long long>(p.nbr[0]) * p.nb[1] * p.nbr[2] +
+                            static_cast<long long>(p.nbr[0]) * p.nbr[1] * p.nb[2];
+    if (total <= 0) return;
+    long long grid = (total + 7) / 8;
+    if (grid > sm_count() * 16) grid = sm_count() * 16;
+    clear_bricks_kernel<<<static_cast<int>(grid), 256, 0, s>>>(p);
+    return;
+  }
   const int wy = (p.map[1] + 31) >> 5;
   const size_t smem = sizeof(uint32_t) * wy + sizeof(int) * (p.map[2] + 1);
   int grid = p.map[0];

@@ -1,11 +1,16 @@
 // Device kernels of the map-integration path.
 //
-// Grid storage (one map):
-//   occ  float[V]     stored log-odds, the reference's ring-buffer hash order
-//                     h = ((lx+hx)*ny + (ly+hy))*nz + (lz+hz)  (utils.cuh:131)
-//   cnt  uint32[V]    per-scan traversal count (bits 0..30) and a "has hit"
+// Grid storage (one map), every array in the same voxel layout (VoxLayout):
+//   occ    float[A]   stored log-odds
+//   cnt    uint32[A]  per-scan traversal count (bits 0..30) and a "has hit"
 //                     flag (bit 31); zero between scans
-//   hit  uint32[V]    per-scan endpoint-hit count, read only where flagged
+//   hit    uint32[A]  per-scan endpoint-hit count, read only where flagged
+//   dirty  uint8[A/32]  per 32-voxel line of the arrays: 1 if the scan being
+//                     integrated has counted a voxel of the line; zero
+//                     between scans
+// A voxel's ring-buffer slot per axis is s = l + h (local index l in
+// [-h, h], utils.cuh:60-70), as in the reference's hash
+// ((sx*ny + sy)*nz + sz) (utils.cuh:131-136).
 #pragma once
 
 #include <cstdint>
@@ -16,6 +21,29 @@ namespace cublox_b200 {
 
 constexpr uint32_t kHitFlag = 0x80000000u;
 constexpr uint32_t kOpMask = 0x7fffffffu;
+constexpr int kLineShift = 5;  // 32 voxels (128 bytes of one array) per line
+
+// Where a voxel lives in a map's arrays.  The slots are cut into bricks of
+// 2^lb[0] x 2^lb[1] x 2^lb[2] voxels stored one after another (brick index
+// x-major, z fastest), voxels inside a brick x-major too, so the address is
+// a sum of one term per axis:
+//   addr = sum_a (s_a >> lb[a]) * bs[a] + (s_a & (2^lb[a] - 1)) * is[a].
+// lb = {0, 0, 0} is the reference's hash order.  With 32-voxel bricks
+// (lb summing to 5) a brick is one 128-byte line: a ray crossing a brick
+// touches one line, and the fold reads and writes whole lines.
+struct VoxLayout {
+  int lb[3];  // log2 brick side per axis
+  int bs[3];  // address step of one brick along the axis
+  int is[3];  // address step of one voxel inside a brick along the axis
+};
+
+CBX_HD int vox_axis(const VoxLayout &L, int a, int s) {
+  return (s >> L.lb[a]) * L.bs[a] + (s & ((1 << L.lb[a]) - 1)) * L.is[a];
+}
+
+CBX_HD int vox_addr(const VoxLayout &L, int sx, int sy, int sz) {
+  return vox_axis(L, 0, sx) + vox_axis(L, 1, sy) + vox_axis(L, 2, sz);
+}
 
 // Error-word bits (never expected; set instead of trapping).
 constexpr uint32_t kErrHashRange = 1u << 0;
@@ -38,17 +66,21 @@ struct RayParams {
   uint32_t *hit;
   unsigned long long *stats;  // [rays, op_incs, hit_incs] or null
   uint32_t *err;
+  VoxLayout lay;
+  uint8_t *dirty;  // line flags to set, or null (the fold sweeps every line)
 };
 
 struct ApplyParams {
   float *occ;
   uint32_t *cnt;
   uint32_t *hit;
-  int vnum;
+  int vnum;    // voxels swept by the full sweep (variants 0, 1)
   float l_hit, l_miss, l_min, l_max, l_unknown;
   unsigned fp;
   unsigned long long *stats;  // [3] += touched
-  int variant;                // 0 scalar sweep, 1 vector sweep
+  int variant;                // 0 scalar sweep, 1 vector sweep, 2 dirty lines
+  uint8_t *dirty;             // variant 2: line flags (cleared as folded)
+  int nlines;                 // variant 2: lines
 };
 
 struct ClearParams {
@@ -57,6 +89,13 @@ struct ClearParams {
   int map[3];
   int any_z;
   int x_done;  // marked x slabs are already cleared (contiguous memsets)
+  VoxLayout lay;
+  // brick layouts: the bricks to visit, as three lists (brick index along x,
+  // y, z of a brick column, row or level that holds a marked slab), each
+  // crossed with every brick of the other two axes
+  const int *blist;  // nb[0] x indices, nb[1] y indices, nb[2] z indices
+  int nb[3];
+  int nbr[3];        // bricks per axis
 };
 
 // A fetch's candidates are cut into work units of `unit` consecutive
@@ -80,6 +119,7 @@ struct FetchParams {
   unsigned fp;
   float l_free, l_occ, l_unknown;
   int filter;
+  VoxLayout lay;
   long long *counts;         // pass 1 output: samples per unit
   const long long *offsets;  // pass 2 input: where each unit's samples go
   const long long *limits;   // pass 2: samples each unit keeps (the cap)
@@ -97,7 +137,14 @@ struct QueryParams {
   int ctr;
   float l_free, l_occ, l_unknown;
   uint8_t *out;
+  VoxLayout lay;
 };
+
+// Copy between a map's layout and the reference's hash order (export,
+// import): to_ref = 1 writes ref[h] = arr[addr(h)], else arr[addr(h)] =
+// ref[h], for every voxel h of the map.
+void launch_relayout(const float *src, float *dst, const VoxLayout &lay, const int map[3],
+                     int to_ref, cudaStream_t s);
 
 void launch_raycast(const RayParams &p, cudaStream_t s);
 

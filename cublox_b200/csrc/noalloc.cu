@@ -142,6 +142,12 @@ int cublox_integrate_noalloc(const cublox_map_view *map, const float *xyz_soa, i
   p.hit = map->hit;
   p.stats = nullptr;
   p.err = nullptr;  // no check on this path can fail (file comment)
+  // the caller's arrays are in the reference's hash order, and have no line
+  // flags: the fold below sweeps every counter
+  p.lay.bs[0] = mapsz[1] * mapsz[2];
+  p.lay.bs[1] = mapsz[2];
+  p.lay.bs[2] = 1;
+  p.dirty = nullptr;
 
   BinnedScratch b{reinterpret_cast<int *>(base), reinterpret_cast<int *>(base + kOffHist),
                   reinterpret_cast<int *>(base + kOffCursor),

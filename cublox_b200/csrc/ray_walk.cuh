@@ -96,8 +96,20 @@ __device__ __forceinline__ bool left_for_good(const RayWalk &w, const RayParams 
          (abs(w.rel[2]) > p.half[2] && w.rel[2] * w.st[2] >= 0);
 }
 
+// Address of the current voxel in the map's arrays.
 __device__ __forceinline__ int walk_hash(const RayWalk &w, const RayParams &p) {
-  return (w.slot[0] * p.map[1] + w.slot[1]) * p.map[2] + w.slot[2];
+  return vox_addr(p.lay, w.slot[0], w.slot[1], w.slot[2]);
+}
+
+// Flag the line of address h as holding a counted voxel (a plain byte
+// store: every writer stores the same 1).  `last` is the line this thread
+// flagged last, so a run of increments on one line stores once.
+__device__ __forceinline__ void mark_line(const RayParams &p, int h, int &last) {
+  const int line = h >> kLineShift;
+  if (line != last) {
+    last = line;
+    if (p.dirty) p.dirty[line] = 1;
+  }
 }
 
 // One step, tie rule of kernels.cu:120-136.  Returns the axis stepped.
@@ -127,15 +139,19 @@ __device__ __forceinline__ int ray_step(RayWalk &w, const RayParams &p) {
   return a;
 }
 
-// Endpoint hash if the endpoint voxel is in the window, else -1.
+// Address of an in-window voxel given by its global index.
+__device__ __forceinline__ int global_addr(const RayParams &p, int g0, int g1, int g2) {
+  return vox_addr(p.lay, global_to_local(g0, p.map[0], p.half[0]) + p.half[0],
+                  global_to_local(g1, p.map[1], p.half[1]) + p.half[1],
+                  global_to_local(g2, p.map[2], p.half[2]) + p.half[2]);
+}
+
+// Endpoint address if the endpoint voxel is in the window, else -1.
 __device__ __forceinline__ int end_hash(const RayWalk &w, const RayParams &p) {
   if (abs(w.en[0] - p.win[0]) > p.half[0] || abs(w.en[1] - p.win[1]) > p.half[1] ||
       abs(w.en[2] - p.win[2]) > p.half[2])
     return -1;
-  return ((global_to_local(w.en[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-          (global_to_local(w.en[1], p.map[1], p.half[1]) + p.half[1])) *
-             p.map[2] +
-         (global_to_local(w.en[2], p.map[2], p.half[2]) + p.half[2]);
+  return global_addr(p, w.en[0], w.en[1], w.en[2]);
 }
 
 }  // namespace cublox_b200

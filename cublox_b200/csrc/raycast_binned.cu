@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "kernels.cuh"
+#include "far_walk.cuh"
 #include "ray_walk.cuh"
 
 namespace cublox_b200 {
@@ -132,6 +133,7 @@ __global__ void __launch_bounds__(512, 1) walk_kernel(const RayParams p, const i
   const int r1 = min(p.n, r0 + rays_per_cta);
   const int clo[3] = {cl0, cl1, cl2};
   uint32_t rays = 0, incs = 0, hits = 0;
+  int last = -1;  // line this thread flagged last
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&next, 32);
@@ -167,16 +169,20 @@ __global__ void __launch_bounds__(512, 1) walk_kernel(const RayParams p, const i
         const uint32_t peers = __match_any_sync(0xffffffffu, key);
         if (!(key & kNoKey) && lane == __ffs(peers) - 1) {
           const uint32_t n = __popc(peers);
-          if (incube)
+          if (incube) {
             atomicAdd(&cube[(c[0] * S + c[1]) * S + c[2]], n);
-          else
+          } else {
             atomicAdd(p.cnt + key, n);
+            mark_line(p, static_cast<int>(key), last);
+          }
         }
       } else if (!(key & kNoKey)) {
-        if (incube)
+        if (incube) {
           atomicAdd(&cube[(c[0] * S + c[1]) * S + c[2]], 1u);
-        else
+        } else {
           atomicAdd(p.cnt + key, 1u);
+          mark_line(p, static_cast<int>(key), last);
+        }
       }
       if (live) {
         const int a = ray_step(w, p);
@@ -213,10 +219,12 @@ __global__ void __launch_bounds__(512, 1) walk_kernel(const RayParams p, const i
       const uint32_t peers = __match_any_sync(0xffffffffu, ekey);
       if (!(ekey & kNoKey) && lane == __ffs(peers) - 1) {
         const uint32_t n = __popc(peers);
-        if (e_incube)
+        if (e_incube) {
           atomicAdd(&cube[e_idx], n);
-        else
+        } else {
           atomicAdd(p.cnt + ekey, n);
+          mark_line(p, static_cast<int>(ekey), last);
+        }
       }
       const uint32_t hkey = e_hit ? ekey : (kNoKey | lane);
       const uint32_t hp = __match_any_sync(0xffffffffu, hkey);
@@ -228,16 +236,7 @@ __global__ void __launch_bounds__(512, 1) walk_kernel(const RayParams p, const i
   }
   __syncthreads();
   // Flush the cube: every staged voxel was in the window when counted.
-  for (int i = threadIdx.x; i < kCube; i += blockDim.x) {
-    const uint32_t v = cube[i];
-    if (!v) continue;
-    const int g[3] = {clo[0] + i / (S * S), clo[1] + (i / S) % S, clo[2] + i % S};
-    const int h = ((global_to_local(g[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-                   (global_to_local(g[1], p.map[1], p.half[1]) + p.half[1])) *
-                      p.map[2] +
-                  (global_to_local(g[2], p.map[2], p.half[2]) + p.half[2]);
-    atomicAdd(p.cnt + h, v);
-  }
+  flush_cube<S>(p, cube, clo);
   if (p.stats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {

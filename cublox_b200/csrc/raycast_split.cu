@@ -397,17 +397,7 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
     }
   }
   __syncthreads();
-  if constexpr (S > 0)
-  for (int q = threadIdx.x; q < kCube; q += blockDim.x) {
-    const uint32_t v = cube[q];
-    if (!v) continue;
-    const int gg[3] = {cl0 + q / (S * S), cl1 + (q / S) % S, cl2 + q % S};
-    const int h = ((global_to_local(gg[0], p.map[0], p.half[0]) + p.half[0]) * p.map[1] +
-                   (global_to_local(gg[1], p.map[1], p.half[1]) + p.half[1])) *
-                      p.map[2] +
-                  (global_to_local(gg[2], p.map[2], p.half[2]) + p.half[2]);
-    atomicAdd(p.cnt + h, v);
-  }
+  flush_cube<S>(p, cube, clo);
   if (p.stats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {

@@ -282,7 +282,7 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
       return fail(CUBLOX_ERR_NOMEM, "server: no map can be evicted");
     }
     MapState &v = *s->maps[victim];
-    v.snapshot.resize(static_cast<size_t>(v.g->voxel_num));
+    v.snapshot.resize(static_cast<size_t>(v.g->nalloc));  // the grid's own layout
     int rc = cublox_b200::detail::release_device(v.g, v.snapshot.data());
     if (rc) return rc;
     v.resident = false;
@@ -680,7 +680,7 @@ int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float re
     m->has_lo = true;
   }
   m->voxels = vox;
-  m->vox_bytes = 12 * static_cast<size_t>(vox);
+  m->vox_bytes = cublox_b200::detail::voxel_bytes_for(m->half);
   std::lock_guard<std::mutex> lk(s->mu);
   if (static_cast<int>(s->maps.size()) >= kMaxMaps)
     return fail(CUBLOX_ERR_INVALID, "server_add_map: at most 4096 maps");
@@ -833,7 +833,7 @@ int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int orig
     rc = cublox_grid_export(m.g, occ_host);
     if (rc) return rc;
   } else {
-    std::copy(m.snapshot.begin(), m.snapshot.end(), occ_host);
+    cublox_b200::detail::layout_to_reference(m.g, m.snapshot.data(), occ_host);
   }
   if (origin_index) cublox_grid_origin(m.g, origin_index, nullptr);
   return CUBLOX_OK;

@@ -57,6 +57,14 @@ int cublox_binary_version(int *binary_version);
  * graphs instantiated.  Fills the first n (entries past 5 read 0).  No
  * counterpart in the reference.                                             */
 int cublox_runtime_counters(int64_t *out, int n);
+/* Measures the device's throughput of 32-bit atomic adds whose result is
+ * unused (the walk's only memory operation) to pseudo-random distinct
+ * addresses of a buffer of buffer_bytes (allocated and freed by the call):
+ * about total_ops operations, timed with CUDA events on `stream`.  The
+ * denominator of the walk's L2-atomic roofline.  No counterpart in the
+ * reference.                                                                */
+int cublox_probe_red_rate(int64_t buffer_bytes, int64_t total_ops, void *stream,
+                          double *ops_per_s);
 
 /* OccupancyGrid(half_map_size_i, resolution, origin_at_center,
  * recenter_threshold, origin)  — OccupancyGrid.hpp:42-45,
@@ -103,11 +111,22 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 #define CUBLOX_OPT_MATCH 3   /* merge duplicate voxels per warp (default 0) */
 #define CUBLOX_OPT_SORT 4    /* walk rays in direction order (default 0)    */
 #define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (64)   */
-#define CUBLOX_OPT_FOLD 6    /* fold sweep: 0 scalar, 1 16-byte (default)   */
+#define CUBLOX_OPT_FOLD 6    /* fold: 0 scalar sweep of every counter, 1
+                                16-byte sweep, 2 (default) only the 32-voxel
+                                lines the scan flagged                     */
 #define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
 #define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
                                    consecutive segments (default 0: all
                                    CTAs share one segment queue)            */
+#define CUBLOX_OPT_LAYOUT 9  /* voxel layout of the grid's arrays: log2 of
+                                the brick sides as decimal digits x y z,
+                                bricks of 32 voxels (320: 8 x 4 x 1, the
+                                default; 230; 221), or 0 for the
+                                reference's hash order.  Setting it moves
+                                the stored map (between scans).  Every
+                                layout gives identical results; exports
+                                and hash arguments always use the
+                                reference's hash order.                    */
 int cublox_grid_set_option(cublox_grid *g, int key, int value);
 int cublox_grid_get_option(const cublox_grid *g, int key, int *value);
 
@@ -244,8 +263,13 @@ int cublox_grid_reference_steps(cublox_grid *g, const float *xyz, int n,
                                 int64_t *voxel_steps);
 
 /* Device error word: nonzero if a kernel's own bounds checks rejected an
- * index (a bug, never expected), or (bit 3) a fused batch launch stopped
- * waiting for the map's walk and skipped its fold.  Reading it clears it. */
+ * index (a bug, never expected), or a fused batch launch stopped waiting
+ * for the map's walk and skipped its fold (CUBLOX_DEVICE_WAIT_TIMEOUT).
+ * Reading it clears it.                                                     */
+#define CUBLOX_DEVICE_HASH_RANGE (1u << 0)
+#define CUBLOX_DEVICE_FETCH_OVERFLOW (1u << 1)
+#define CUBLOX_DEVICE_JUMP_STALL (1u << 2)
+#define CUBLOX_DEVICE_WAIT_TIMEOUT (1u << 3)
 int cublox_grid_check(cublox_grid *g, uint32_t *error_word);
 
 /* ---- batched integration ----------------------------------------------------
@@ -260,16 +284,36 @@ typedef struct cublox_batch cublox_batch;
 
 #define CUBLOX_BATCH_OPT_GRAPHS 1     /* replay the launch sequence from a CUDA
                                          graph (default 0)                  */
-#define CUBLOX_BATCH_OPT_AUTOTUNE 2   /* choose the launch shape over the
-                                         first updates (default 1)          */
+#define CUBLOX_BATCH_OPT_AUTOTUNE 2   /* choose the launch shape and the
+                                         voxel layout over the first
+                                         updates (default 1): each candidate
+                                         (every shape with 8 x 4 x 1
+                                         bricks, the first shape with the
+                                         other layouts) is timed twice      */
 #define CUBLOX_BATCH_OPT_SHAPE 3      /* fix the launch shape (0 .. n-1)    */
 #define CUBLOX_BATCH_OPT_TIMING 4     /* record walk/fold device times      */
 #define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
-#define CUBLOX_BATCH_OPT_FOLD 6       /* fold sweep: counter groups in flight
-                                         per thread, 0: two (default),
-                                         1: four, 2: one; 3: counters
-                                         streamed to shared memory by the
-                                         bulk-copy engine                   */
+#define CUBLOX_BATCH_OPT_FOLD 6       /* fold: 0 (default) only the 32-voxel
+                                         lines the walk flagged; 1 every
+                                         line (the reference's full sweep,
+                                         for comparison)                    */
+#define CUBLOX_BATCH_OPT_LAYOUT 8     /* voxel layout the batch keeps its
+                                         grids in (CUBLOX_OPT_LAYOUT codes;
+                                         default 320); setting it stops
+                                         the tuner                          */
+#define CUBLOX_BATCH_OPT_WAIT_LIMIT 9 /* fused shapes: rounds of a ~256 ns
+                                         sleep a map's fold waits for its
+                                         walk before it gives up, flags
+                                         CUBLOX_DEVICE_WAIT_TIMEOUT in the
+                                         map's error word and lets the
+                                         launch finish without folding
+                                         (default 1 << 23, about 2 s)       */
+#define CUBLOX_BATCH_OPT_INJECT_MISSING_WALK 10 /* test hook: with a fused
+                                         shape, the first map's folds wait
+                                         for a walk item that does not
+                                         exist, so the wait runs out; the
+                                         maps are then left unfolded and
+                                         must be reset                      */
 #define CUBLOX_BATCH_OPT_TUNING 7     /* read only: 1 while the tuner is
                                          still timing candidate shapes (the
                                          updates until it reads 0 run

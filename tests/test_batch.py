@@ -86,12 +86,53 @@ def feed_pinned(batch, bg, clouds, sensors):
 
 @pytest.mark.parametrize("graphs", [False, True])
 def test_batch_matches_solo_updates_through_tuning(graphs):
-    w = small_workload(n_steps=18)  # 8 shapes x 2 tuning rounds, then the chosen one
+    w = small_workload(n_steps=24)  # 11 candidates x 2 tuning rounds, then the chosen one
     b = C.Batch()
     b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
     bg, solo = setup(w, b)
     run_and_compare(w, b, bg, solo, feed_lists, skip={(3, 4), (0, 0)})
+    assert not b.tuning()
     assert 0 <= b.get_option(C.BATCH_OPT_SHAPE) < b.get_option(C.BATCH_OPT_NUM_SHAPES)
+    assert b.get_option(C.BATCH_OPT_LAYOUT) in C.LAYOUTS
+    assert all(g.get_option(C.OPT_LAYOUT) == b.get_option(C.BATCH_OPT_LAYOUT) for g in bg)
+    b.close()
+
+
+@pytest.mark.parametrize("layout", C.LAYOUTS)
+def test_every_layout_gives_the_same_maps(layout):
+    w = small_workload(n_maps=4, n_steps=4, seed=8)
+    b = C.Batch()
+    b.set_option(C.BATCH_OPT_SHAPE, 6)  # fused: folds read flags other CTAs wrote
+    b.set_option(C.BATCH_OPT_LAYOUT, layout)
+    b.set_option(C.BATCH_OPT_GRAPHS, 1)
+    bg, solo = setup(w, b)
+    run_and_compare(w, b, bg, solo, feed_lists)
+    assert all(g.get_option(C.OPT_LAYOUT) == layout for g in bg)
+    b.close()
+
+
+def test_fused_wait_runs_out_and_the_context_stays_usable():
+    """A fused launch whose first map's folds wait for a walk item that
+    does not exist (the test hook): the bounded wait (shortened here to
+    about a millisecond) gives up, the launch ends, the map's error word
+    says CUBLOX_DEVICE_WAIT_TIMEOUT, and the same batch, after the maps are
+    reset, integrates correctly again."""
+    w = small_workload(n_maps=3, n_steps=3, seed=10)
+    b = C.Batch()
+    b.set_option(C.BATCH_OPT_SHAPE, 6)
+    b.set_option(C.BATCH_OPT_WAIT_LIMIT, 4000)
+    b.set_option(C.BATCH_OPT_INJECT_MISSING_WALK, 1)
+    bg, solo = setup(w, b)
+    clouds, sensors = w.step(0)
+    b.update(bg, clouds, sensors)
+    b.synchronize()
+    words = [g.check() for g in bg]
+    assert words[0] & C.DEVICE_WAIT_TIMEOUT, words
+    b.set_option(C.BATCH_OPT_INJECT_MISSING_WALK, 0)
+    b.set_option(C.BATCH_OPT_WAIT_LIMIT, 1 << 23)
+    for g in bg:
+        g.reset()
+    run_and_compare(w, b, bg, solo, feed_lists)
     b.close()
 
 
@@ -101,7 +142,7 @@ def test_every_shape_gives_the_same_maps(shape):
     b = C.Batch()
     assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 8
     b.set_option(C.BATCH_OPT_SHAPE, shape)
-    b.set_option(C.BATCH_OPT_FOLD, shape % 4)
+    b.set_option(C.BATCH_OPT_FOLD, shape % 2)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
     bg, solo = setup(w, b)
     run_and_compare(w, b, bg, solo, feed_lists)

@@ -456,3 +456,69 @@ def test_reference_steps_equal_oracle_count(cfg):
         if cfg == "plain_small":  # the oracle's own per-scan accounting agrees
             assert o.raycast(pts, so, threads=8)["voxel_steps"] == want
     g.close()
+
+
+@pytest.mark.parametrize("layout", C.LAYOUTS)
+@pytest.mark.parametrize("raycast", [0, 1, 2])
+def test_every_layout_exact(layout, raycast):
+    """Every voxel layout (8x4x1, 4x8x1 and 4x4x2 bricks, the reference's
+    hash order) with every walk: counts, stored log-odds, recenters (slab
+    clears through partially and fully marked brick columns), fetches and
+    point queries equal the oracle's, and exports stay in the reference's
+    hash order."""
+    sensor = synth.Sensor(16, 512, -20.0, 20.0, 12.0, 0.02)
+    scene = synth.make_scene(31, 120, 25.0, keepout=synth._keepout_line(0.0, 1.5))
+    poses = synth.line_trajectory(14, 6.0, 10.0, 1.8, start=(-4.0, 0.5))
+    half = (90, 70, 22)  # 181 x 141 x 45: every axis ragged against the bricks
+    g, o = pair(half, 0.1, thr=1.0, max_range=sensor.max_range)
+    g.set_option(C.OPT_LAYOUT, layout)
+    assert g.get_option(C.OPT_LAYOUT) == layout
+    g.set_option(C.OPT_RAYCAST, raycast)
+    rng = np.random.default_rng(40 + raycast)
+    for k, (x, y, z, yaw) in enumerate(poses):
+        pts = synth.scan(scene, sensor, (x, y, z), yaw, seed=1300 + k)
+        so = np.float32([x, y, z + 0.13 * (k % 3)])  # z shifts exercise z slabs
+        g.update(pts, so)
+        o.update(pts, so)
+        assert g.recenter(so) == o.recenter(so)["action"]
+        if k % 5 == 4:
+            assert same_bits(g.export(), o.occ()), k
+            c = (so + rng.uniform(-3, 3, 3)).astype(np.float32)
+            gp, gs = g.fetchOccupancyAround(c, 1.2)
+            op_, os_, _ = o.fetch(c, 1.2)
+            assert same_bits(gp, op_) and np.array_equal(gs, os_)
+            q = (so + rng.uniform(-12, 12, (500, 3))).astype(np.float32)
+            want = np.array([2 if o.is_state(p, 2) else (1 if o.is_state(p, 1) else 0)
+                             for p in q], np.uint8)
+            assert np.array_equal(g.query_states(q), want)
+            h = int(rng.integers(0, o.voxel_num))
+            assert np.float32(g.storedAt(h)).view(np.uint32) == np.float32(o.occ()[h]).view(np.uint32)
+    assert same_bits(g.export(), o.occ())
+    # count_scan reports counts in the reference's hash order
+    pts = synth.scan(scene, sensor, poses[-1][:3], poses[-1][3], seed=1399)
+    op, hit = g.count_scan(pts, np.float32(poses[-1][:3]))
+    o.raycast(pts, np.float32(poses[-1][:3]))
+    assert np.array_equal(op, o.op()) and np.array_equal(hit, o.hit())
+    assert g.check() == 0
+
+
+def test_layout_switch_keeps_the_map_and_import_export_round_trip():
+    w = synth.plain_small()
+    pts, so = w.scan(0), w.sensor_origin(0)
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.update(pts, so)
+    o.update(pts, so)
+    for layout in (230, 0, 221, 320):
+        g.set_option(C.OPT_LAYOUT, layout)
+        assert same_bits(g.export(), o.occ()), layout
+        g.update(pts, so)
+        o.update(pts, so)
+        assert same_bits(g.export(), o.occ()), layout
+    occ = o.occ().copy()
+    occ[::97] = np.float32(1.25)
+    g.import_(occ)
+    assert same_bits(g.export(), occ)
+    g.resetVoxel(97)
+    assert g.storedAt(97) == 0.0
+    with pytest.raises(C.CubloxError):
+        g.set_option(C.OPT_LAYOUT, 321)  # 64-voxel bricks are not lines
