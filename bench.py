@@ -523,7 +523,9 @@ def run_serving(args, budget_gb=None, seconds=None):
             lat["fetch"].append(l)
     st = s.stats()
     s.close()
-    span = seconds - warm
+    # throughput over the time the work took: from the end of the warm-up
+    # window to the last completion (drain), not the arrival window
+    span = max(wall - warm, seconds - warm)
     names = {0: "16384", 1: "65536", 2: "262144"}
     out = {"workload": sw.name, "robots": sw.n_robots, "seconds": seconds,
            "arrivals": "Poisson, scans 400/s (16,384 / 65,536 / 262,144 points, p = .5/.35/.15), "

@@ -129,6 +129,140 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
   __syncthreads();
 }
 
+// ---- refill walk -----------------------------------------------------------
+// One thread per ray leaves lanes idle: a warp runs until its longest ray
+// ends, and rays of one azimuth column differ several-fold in length.  The
+// refill walk splits an item in two phases.  Phase A: every thread sets up
+// its ray and walks its near phase (the sensor cube); a ray that goes on
+// leaves its far-phase state in a shared-memory queue.  Phase B: lanes take
+// far states from the queue and walk them kRefillSteps loop iterations at a
+// time; a lane whose ray is over takes the next state, so the warp's lanes
+// stay busy until the item's queue is empty.  The loop iterations walked,
+// and so the counts, are those of the single loop.
+constexpr int kRefillRays = 512;   // rays per item (queue capacity)
+constexpr int kRefillSteps = 32;   // far-loop iterations between refills
+constexpr int kFarWords = 27;      // queued state: FarWalk (23) + RayEnd (3), odd stride
+
+__device__ __forceinline__ void far_store(uint32_t *q, const FarWalk &f, const RayEnd &re) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    q[a] = __float_as_uint(f.tM[a]);
+    q[3 + a] = __float_as_uint(f.tD[a]);
+    q[6 + a] = static_cast<uint32_t>(f.e[a]);
+    q[9 + a] = static_cast<uint32_t>(f.out[a]);
+    q[12 + a] = static_cast<uint32_t>(f.slot[a]);
+    q[15 + a] = static_cast<uint32_t>(f.st[a]);
+    q[18 + a] = static_cast<uint32_t>(f.off[a]);
+  }
+  q[21] = static_cast<uint32_t>(f.left);
+  q[22] = static_cast<uint32_t>(f.h);
+  q[23] = static_cast<uint32_t>(re.h);
+  q[24] = static_cast<uint32_t>(re.c);
+  q[25] = re.hit ? 1u : 0u;
+}
+
+__device__ __forceinline__ void far_load(const uint32_t *q, FarWalk &f, RayEnd &re) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    f.tM[a] = __uint_as_float(q[a]);
+    f.tD[a] = __uint_as_float(q[3 + a]);
+    f.e[a] = static_cast<int>(q[6 + a]);
+    f.out[a] = static_cast<int>(q[9 + a]);
+    f.slot[a] = static_cast<int>(q[12 + a]);
+    f.st[a] = static_cast<int>(q[15 + a]);
+    f.off[a] = static_cast<int>(q[18 + a]);
+  }
+  f.left = static_cast<int>(q[21]);
+  f.h = static_cast<int>(q[22]);
+  f.line = -1;
+  re.h = static_cast<int>(q[23]);
+  re.c = static_cast<int>(q[24]);
+  re.hit = q[25] != 0u;
+}
+
+// One walk item (at most kRefillRays rays) in the two phases above.  Ends
+// with a CTA barrier.
+template <int S>
+__device__ __forceinline__ void walk_item_refill(const MapDesc &md, const WalkItem &item,
+                                                 uint32_t *cube, uint32_t *fq, int *s_q) {
+  constexpr int kCube = S * S * S;
+  const RayParams p = md.ray;
+  const int clo[3] = {md.clo[0], md.clo[1], md.clo[2]};
+  for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
+    reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
+  if (threadIdx.x == 0) s_q[0] = s_q[1] = 0;  // queued, taken
+  __syncthreads();
+  uint32_t rays = 0, incs = 0, hits = 0;
+  for (int i = item.start + threadIdx.x; i < item.start + item.count; i += blockDim.x) {
+    const size_t k = static_cast<size_t>(i) * p.stride;
+    RayWalk w;
+    if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;
+    ++rays;
+    const RayEnd re = ray_end_of<S>(p, w, clo);
+    FarWalk f;
+    if (walk_near<S>(p, cube, clo, w, f, incs)) {
+      apply_end<S>(p, cube, re, incs, hits);
+    } else {
+      const int slot = atomicAdd(&s_q[0], 1);
+      far_store(fq + slot * kFarWords, f, re);
+    }
+  }
+  __syncthreads();
+  const int queued = s_q[0];
+  FarWalk f;
+  RayEnd re;
+  bool alive = false;
+  for (;;) {
+    if (!alive) {
+      const int t = atomicAdd(&s_q[1], 1);
+      if (t >= queued) break;
+      far_load(fq + t * kFarWords, f, re);
+      alive = true;
+    }
+    if (walk_far(p, f, kRefillSteps, incs)) {
+      apply_end<S>(p, cube, re, incs, hits);
+      alive = false;
+    }
+  }
+  __syncthreads();
+  flush_cube<S>(p, cube, clo);
+  if (p.stats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      rays += __shfl_down_sync(0xffffffffu, rays, off);
+      incs += __shfl_down_sync(0xffffffffu, incs, off);
+      hits += __shfl_down_sync(0xffffffffu, hits, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(p.stats + 0, static_cast<unsigned long long>(rays));
+      atomicAdd(p.stats + 1, static_cast<unsigned long long>(incs));
+      atomicAdd(p.stats + 2, static_cast<unsigned long long>(hits));
+    }
+  }
+  __syncthreads();
+}
+
+// Persistent refill walk: CTAs take walk items (at most kRefillRays rays
+// each) from counters[0].  Shared memory: the S^3 cube, then the far-state
+// queue.
+template <int S>
+__global__ void __launch_bounds__(512, 1) batch_walk_refill_kernel(const MapDesc *maps,
+                                                                   const WalkItem *items,
+                                                                   int *counters) {
+  extern __shared__ uint32_t smem[];
+  __shared__ int s_item;
+  __shared__ int s_q[2];
+  const int n_items = counters[1];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WalkItem item = items[it];
+    walk_item_refill<S>(maps[item.map], item, smem, smem + S * S * S, s_q);
+  }
+}
+
 __device__ __forceinline__ FoldView fold_view(const MapDesc &m) {
   return FoldView{m.occ, m.ray.cnt, m.ray.hit, m.ray.vnum, m.l_hit, m.l_miss, m.l_min, m.l_max,
                   m.l_unknown, m.ray.fp};
@@ -333,12 +467,14 @@ struct Shape {
   int fused;     // 1: one launch, folds overlap later maps' walks
   int min_ctas;  // 2: registers capped for two CTAs per SM (cube <= 16)
   int wq;        // 1: warps take 32-ray items of a CTA's current map (no item barriers)
+  int refill;    // 1: two-phase items, lanes refilled from a far-state queue
 };
 
-const Shape kShapes[] = {{32, 512, 512, 0, 1, 0},  {32, 1024, 1024, 0, 1, 0},
-                         {32, 0, 512, 0, 1, 1},    {32, 0, 1024, 0, 1, 1},
-                         {16, 0, 512, 0, 1, 1},    {16, 1024, 1024, 0, 2, 0},
-                         {32, 1024, 1024, 1, 1, 0}, {16, 512, 512, 1, 1, 0}};
+const Shape kShapes[] = {{32, 512, 512, 0, 1, 0, 0},  {32, 1024, 1024, 0, 1, 0, 0},
+                         {32, 0, 512, 0, 1, 1, 0},    {32, 0, 1024, 0, 1, 1, 0},
+                         {16, 0, 512, 0, 1, 1, 0},    {16, 1024, 1024, 0, 2, 0, 0},
+                         {32, 1024, 1024, 1, 1, 0, 0}, {16, 512, 512, 1, 1, 0, 0},
+                         {32, kRefillRays, 512, 0, 1, 0, 1}, {16, kRefillRays, 512, 0, 1, 0, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 // The tuner's candidates: every launch shape with the default voxel layout
@@ -348,8 +484,9 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 struct Candidate {
   int shape, layout;
 };
-const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320}, {5, 320},
-                                 {6, 320}, {7, 320}, {0, 230}, {0, 221}, {0, 0}};
+const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320},
+                                 {5, 320}, {6, 320}, {7, 320}, {8, 320}, {9, 320},
+                                 {0, 230}, {0, 221}, {0, 0},   {8, 221}, {8, 0}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {
@@ -365,6 +502,7 @@ int sm_count_batch() {
 
 template <int S>
 const void *shape_kernel_s(const Shape &sh) {
+  if (sh.refill) return reinterpret_cast<const void *>(batch_walk_refill_kernel<S>);
   if (sh.fused) return reinterpret_cast<const void *>(batch_fused_kernel<S>);
   if (sh.wq) return reinterpret_cast<const void *>(batch_walk_wq_kernel<S>);
   if constexpr (S < 32) {
@@ -380,7 +518,8 @@ const void *shape_kernel(const Shape &sh) {
 }
 
 size_t shape_smem(const Shape &sh) {
-  return sizeof(uint32_t) * sh.cube * sh.cube * sh.cube;
+  return sizeof(uint32_t) * (sh.cube * sh.cube * sh.cube +
+                             (sh.refill ? kRefillRays * kFarWords : 0));
 }
 
 // CTAs of a shape's persistent launch: resident CTAs per SM x SMs.  Sets

@@ -144,8 +144,10 @@ __device__ __forceinline__ bool far_step(FarWalk &f, const RayParams &p) {
 // the endpoint only after exactly e0 + e1 + e2 steps (an axis it never steps
 // on must already match), and not at all once a counter went negative.
 // Until then only the limits and the window exit end the loop.  Every
-// iteration counts the current voxel, then steps.
-__device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, int budget,
+// iteration counts the current voxel, then steps.  Returns true if the ray's
+// loop is over (window left, endpoint reached or step limit spent), false
+// if only the budget stopped it.
+__device__ __forceinline__ bool walk_far(const RayParams &p, FarWalk &f, int budget,
                                          uint32_t &incs) {
   const int lim = min(budget, f.left);
   bool reachable = true;
@@ -171,7 +173,7 @@ __device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, int bud
       if (gone) {
         f.left -= done;
         incs += static_cast<uint32_t>(done);
-        return;
+        return true;
       }
     }
     // At a limit, or where the endpoint could be: stop if on it, else (a
@@ -181,5 +183,6 @@ __device__ __forceinline__ void walk_far(const RayParams &p, FarWalk &f, int bud
   }
   f.left -= done;
   incs += static_cast<uint32_t>(done);
+  return f.left == 0 || (f.e[0] | f.e[1] | f.e[2]) == 0;
 }
 }  // namespace cublox_b200

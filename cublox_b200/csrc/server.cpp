@@ -81,7 +81,14 @@ struct MapState {
   bool has_lo = false;
   cublox_grid *g = nullptr;  // created at first admission
   bool resident = false;
-  std::vector<float> snapshot;  // stored log-odds while evicted
+  // stored log-odds while evicted (the grid's own layout): a pinned buffer
+  // allocated at the map's first eviction and kept for the next ones, or
+  // pageable memory if pinning failed
+  float *snap_pinned = nullptr;
+  std::vector<float> snap_pageable;
+  const float *snapshot() const {
+    return snap_pinned ? snap_pinned : (snap_pageable.empty() ? nullptr : snap_pageable.data());
+  }
   size_t vox_bytes = 0;  // device bytes of the map's arrays
   int64_t voxels = 0;
   uint64_t last_use = 0;
@@ -241,6 +248,7 @@ void fill_defaults(cublox_server_config *cfg) {
 }
 
 constexpr int kMaxMaps = 4096;
+constexpr double kSwapAgeMs = 25.0;  // a request this old may force a second swap in a tick
 
 size_t used_bytes(cublox_server *s) {
   size_t b = scratch_bytes(s);
@@ -271,19 +279,38 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
         cublox_b200::detail::release_scratch(o.g);
     }
   while (used_bytes(s) + need > s->cfg.hbm_budget_bytes) {
+    // the victim: a resident map outside this tick, preferring maps with no
+    // queued request (their next use is furthest off), least recently used
+    // first
     int victim = -1;
-    for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
-      MapState &o = *s->maps[j];
-      if (j == mi || !o.resident || busy[j] || o.fetching.load()) continue;
-      if (victim < 0 || o.last_use < s->maps[victim]->last_use) victim = j;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      bool victim_idle = false;
+      for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
+        MapState &o = *s->maps[j];
+        if (j == mi || !o.resident || busy[j] || o.fetching.load()) continue;
+        const bool idle = o.queue.empty();
+        if (victim < 0 || (idle && !victim_idle) ||
+            (idle == victim_idle && o.last_use < s->maps[victim]->last_use)) {
+          victim = j;
+          victim_idle = idle;
+        }
+      }
     }
     if (victim < 0) {
       *later = true;
       return fail(CUBLOX_ERR_NOMEM, "server: no map can be evicted");
     }
     MapState &v = *s->maps[victim];
-    v.snapshot.resize(static_cast<size_t>(v.g->nalloc));  // the grid's own layout
-    int rc = cublox_b200::detail::release_device(v.g, v.snapshot.data());
+    const size_t n = static_cast<size_t>(v.g->nalloc);
+    if (!v.snap_pinned && v.snap_pageable.empty() &&
+        cublox_b200::detail::hmalloc(&v.snap_pinned, n * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      v.snap_pinned = nullptr;
+      v.snap_pageable.resize(n);
+    }
+    int rc = cublox_b200::detail::release_device(
+        v.g, v.snap_pinned ? v.snap_pinned : v.snap_pageable.data());
     if (rc) return rc;
     v.resident = false;
     std::lock_guard<std::mutex> lk(s->mu);
@@ -297,9 +324,8 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
     if (m.has_lo)
       cublox_grid_set_log_odds(m.g, m.lo[0], m.lo[1], m.lo[2], m.lo[3], m.lo[4], m.lo[5]);
   } else {
-    rc = cublox_b200::detail::acquire_device(m.g, m.snapshot.empty() ? nullptr : m.snapshot.data());
+    rc = cublox_b200::detail::acquire_device(m.g, m.snapshot());
     if (rc) return rc;
-    std::vector<float>().swap(m.snapshot);
   }
   m.resident = true;
   const size_t used = used_bytes(s);
@@ -310,9 +336,9 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
   return CUBLOX_OK;
 }
 
-// Tick and fetch-order events: the completer thread waits on them, and a
-// blocking-sync event lets it sleep instead of spinning a core.
-constexpr unsigned kEventFlags = cudaEventDisableTiming | cudaEventBlockingSync;
+// Tick and fetch-order events (the completer thread polls them, see
+// completer_loop).
+constexpr unsigned kEventFlags = cudaEventDisableTiming;
 constexpr int kEventPool = 64;  // created with the server
 
 // Caller holds the lock.
@@ -381,14 +407,30 @@ void worker_loop(cublox_server *s) {
       std::unique_lock<std::mutex> lk(s->mu);
       for (;;) {
         if (s->stop) return;
-        // heads of the per-map queues
+        // heads of the per-map queues.  Under memory pressure a map that is
+        // not resident costs a swap (an eviction and a restore): a tick
+        // takes at most one such map, unless a map's oldest request has
+        // waited kSwapAgeMs, so resident maps' backlogs are served between
+        // swaps.
         nm = s->n_maps.load();
         int64_t pts = 0;
+        const auto now = Clock::now();
+        size_t room = s->cfg.hbm_budget_bytes - std::min(s->cfg.hbm_budget_bytes, used_bytes(s));
+        bool swapped = false;
         for (int k = 0; k < nm; ++k) {
           const int mi = (s->rr + k) % nm;
           MapState &m = *s->maps[mi];
           if (m.queue.empty() || m.fetching) continue;
           Request *r = m.queue.front();
+          if (!m.resident) {
+            if (m.vox_bytes <= room) {
+              room -= m.vox_bytes;  // fits without an eviction
+            } else if (swapped && ms_between(r->t_submit, now) < kSwapAgeMs) {
+              continue;
+            } else {
+              swapped = true;
+            }
+          }
           if (r->kind == kFetch) {
             fetches.push_back(r);
             m.queue.pop_front();
@@ -552,7 +594,11 @@ void completer_loop(cublox_server *s) {
       if (s->inflight.empty()) return;  // stop, nothing in flight
       ev = s->inflight.front().done;
     }
-    const cudaError_t e = cudaEventSynchronize(ev);
+    // Poll, yielding the core between queries: a tick takes a fraction of a
+    // millisecond, and a blocking wait's wake-up would add more than that to
+    // every request's latency.
+    cudaError_t e;
+    while ((e = cudaEventQuery(ev)) == cudaErrorNotReady) std::this_thread::yield();
     std::lock_guard<std::mutex> lk(s->mu);
     Tick t = std::move(s->inflight.front());
     s->inflight.pop_front();
@@ -641,8 +687,10 @@ int cublox_server_destroy(cublox_server *s) {
   for (Tick &t : s->inflight) s->free_events.push_back(t.done);
   for (cudaEvent_t e : s->free_events)
     if (e) cudaEventDestroy(e);
-  for (auto &m : s->maps)
+  for (auto &m : s->maps) {
     if (m->g) cublox_grid_destroy(m->g);
+    cublox_b200::detail::hfree(m->snap_pinned);
+  }
   cublox_batch_destroy(s->batch);
   cublox_b200::detail::free_fetch(&s->fscratch);
   s->pinned.release_all();
@@ -833,7 +881,7 @@ int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int orig
     rc = cublox_grid_export(m.g, occ_host);
     if (rc) return rc;
   } else {
-    cublox_b200::detail::layout_to_reference(m.g, m.snapshot.data(), occ_host);
+    cublox_b200::detail::layout_to_reference(m.g, m.snapshot(), occ_host);
   }
   if (origin_index) cublox_grid_origin(m.g, origin_index, nullptr);
   return CUBLOX_OK;

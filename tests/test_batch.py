@@ -86,7 +86,7 @@ def feed_pinned(batch, bg, clouds, sensors):
 
 @pytest.mark.parametrize("graphs", [False, True])
 def test_batch_matches_solo_updates_through_tuning(graphs):
-    w = small_workload(n_steps=24)  # 11 candidates x 2 tuning rounds, then the chosen one
+    w = small_workload(n_steps=32)  # 15 candidates x 2 tuning rounds, then the chosen one
     b = C.Batch()
     b.set_option(C.BATCH_OPT_GRAPHS, int(graphs))
     bg, solo = setup(w, b)
@@ -136,11 +136,11 @@ def test_fused_wait_runs_out_and_the_context_stays_usable():
     b.close()
 
 
-@pytest.mark.parametrize("shape", range(8))
+@pytest.mark.parametrize("shape", range(10))
 def test_every_shape_gives_the_same_maps(shape):
     w = small_workload(n_maps=4, n_steps=3, seed=7)
     b = C.Batch()
-    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 8
+    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 10
     b.set_option(C.BATCH_OPT_SHAPE, shape)
     b.set_option(C.BATCH_OPT_FOLD, shape % 2)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
