@@ -1075,6 +1075,7 @@ def main():
         "gpu_launches": h["launches"],
         "clocks": h["clocks"],
     }
+    import cublox_b200 as C
     red_l2 = C.red_rate(64 << 20, 1 << 30)      # buffer in L2
     red_hbm = C.red_rate(4 << 30, 1 << 30)      # buffer far beyond L2
     ach = float(np.mean(h["incs"]) / (np.mean(h["walk_ms"]) / 1e3))

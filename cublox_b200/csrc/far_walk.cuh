@@ -26,7 +26,7 @@ struct FarWalk {
   float tM[3], tD[3];  // as in RayWalk
   int e[3];     // steps to the endpoint's coordinate on the axis (all 0: at the endpoint)
   int out[3];   // steps the walk can still take on the axis inside the window
-  int slot[3];  // ring-buffer slot of the current voxel on the axis
+  int slot[3];  // ring-buffer slot of the current voxel on the axis, unwrapped
   int st[3];    // step on the axis (-1, 0, 1)
   int off[3];   // the axis's term of the current voxel's address
   int left;     // loop iterations left (max_steps - k)
@@ -113,26 +113,27 @@ __device__ __forceinline__ void to_far(const RayParams &p, const RayWalk &w, int
     f.out[a] = st > 0 ? p.half[a] - w.rel[a] : (st < 0 ? p.half[a] + w.rel[a] : kNever);
     f.slot[a] = w.slot[a];
     f.st[a] = st;
-    f.off[a] = vox_axis(p.lay, a, w.slot[a]);
+    f.off[a] = __ldg(p.tab[a] + w.slot[a]);
   }
   f.left = w.max_steps - k;
   f.h = f.off[0] + f.off[1] + f.off[2];
   f.line = -1;
 }
 
-// One step on axis A (the tie rule picked it): the slot moves with the ring
-// buffer's wrap and the axis's address term follows it.  Returns true if
-// the new voxel is outside the window, which ends the loop: the next
-// iteration would break at its step limit, at the endpoint or as out of the
-// window for good.
+// One step on axis A (the tie rule picked it): the slot moves one step,
+// unwrapped, and the axis's address term is read from the axis's table,
+// which folds the ring buffer's wrap in.  In the far phase the walk takes at
+// most map[A] steps on an axis from a slot in [0, map[A]) before it leaves
+// the window, so the slot stays inside the table's [-map[A], 2 map[A]).
+// Returns true if the new voxel is outside the window, which ends the loop:
+// the next iteration would break at its step limit, at the endpoint or as
+// out of the window for good.
 template <int A>
 __device__ __forceinline__ bool far_step(FarWalk &f, const RayParams &p) {
   f.tM[A] = fadd(f.tM[A], f.tD[A]);
   --f.e[A];
-  int s = f.slot[A] + f.st[A];
-  s = s == p.map[A] ? 0 : (s < 0 ? p.map[A] - 1 : s);
-  f.slot[A] = s;
-  const int o = vox_axis(p.lay, A, s);
+  f.slot[A] += f.st[A];
+  const int o = __ldg(p.tab[A] + f.slot[A]);
   f.h += o - f.off[A];
   f.off[A] = o;
   return f.out[A]-- == 0;

@@ -138,7 +138,7 @@ def test_cpp_dropin_replay_matches_oracle(exe, tmp_path):
 def test_cpp_reference_perf_test_restated(exe):
     r = subprocess.run([exe, "perf", "20"], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "401 x 401 x 201 voxels (32320401 total) at 0.05 m" in r.stdout, r.stdout
+    assert "401 x 401 x 201 voxels (32321001 total) at 0.05 m" in r.stdout, r.stdout
     line = [ln for ln in r.stdout.splitlines() if ln.startswith("steady-state")][0]
     mean = float(line.split("mean=")[1].split(" ms")[0])
     print(r.stdout)
