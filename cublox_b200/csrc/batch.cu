@@ -268,6 +268,59 @@ __device__ __forceinline__ FoldView fold_view(const MapDesc &m) {
                   m.l_unknown, m.ray.fp};
 }
 
+// Persistent fold with the flagged lines staged by the bulk-copy engine
+// (fold.cuh, fold_lines_bulk): CTAs take fold items from counters[2]; each
+// of the CTA's warps folds one contiguous eighth of the item.  A wait that
+// gives up flags kErrWaitTimeout in the map's error word, and the launch
+// skips the remaining folds (counters[4]).
+constexpr int kBulkFoldWarps = 8;
+
+__global__ void __launch_bounds__(32 * kBulkFoldWarps) batch_fold_bulk_kernel(
+    const MapDesc *maps, const FoldItem *items, int *counters) {
+  extern __shared__ __align__(128) unsigned char fsm[];
+  __shared__ int s_item;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  BulkStage *st = reinterpret_cast<BulkStage *>(fsm) + 2 * warp;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(fsm + 2 * kBulkFoldWarps * sizeof(BulkStage)) +
+                  2 * warp;
+  if (lane == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  uint32_t phase = 0;
+  const int n_items = counters[3];
+  for (;;) {
+    if (threadIdx.x == 0)
+      s_item = *reinterpret_cast<volatile int *>(counters + 4) ? n_items
+                                                               : atomicAdd(&counters[2], 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= n_items) break;
+    const FoldItem item = items[it];
+    const MapDesc &m = maps[item.map];
+    const int per = ((item.count + kBulkFoldWarps - 1) / kBulkFoldWarps + 31) & ~31;
+    const int first = item.start + min(item.count, warp * per);
+    const int end = item.start + min(item.count, (warp + 1) * per);
+    bool ok = true;
+    uint32_t touched = fold_lines_bulk(fold_view(m), m.ray.dirty, first, end, st, bar, phase, &ok);
+    if (!ok && lane == 0) {
+      atomicOr(m.ray.err, kErrWaitTimeout);
+      atomicExch(counters + 4, 1);
+    }
+    if (m.ray.stats) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1)
+        touched += __shfl_down_sync(0xffffffffu, touched, off);
+      if (lane == 0 && touched)
+        atomicAdd(m.ray.stats + 3, static_cast<unsigned long long>(touched));
+    }
+  }
+}
+
+
 // One fold item: the flagged lines among [start, start + count), the CTA's
 // warps taking groups of 32 lines in turn.  kAll: fold every line of the
 // item, flagged or not (the reference's full sweep, for comparison).
@@ -569,10 +622,21 @@ cudaError_t launch_walk(const MapDesc *maps, const WalkItem *witems, const FoldI
 cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counters,
                         int variant, cudaStream_t s) {
   const dim3 grid(sm_count_batch() * 8), block(256);
-  if (variant == 1)
+  if (variant == 0) {
+    static bool attr = false;
+    const size_t smem = kBulkFoldWarps * kBulkWarpSmem;
+    if (!attr) {
+      cudaFuncSetAttribute(batch_fold_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem));
+      attr = true;
+    }
+    batch_fold_bulk_kernel<<<sm_count_batch(), 32 * kBulkFoldWarps, smem, s>>>(maps, fitems,
+                                                                             counters);
+  } else if (variant == 1) {
     batch_fold_kernel<true><<<grid, block, 0, s>>>(maps, fitems, counters);
-  else
+  } else {
     batch_fold_kernel<false><<<grid, block, 0, s>>>(maps, fitems, counters);
+  }
   return cudaGetLastError();
 }
 
@@ -828,7 +892,7 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
       b->timed = value != 0;
       return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD:
-      if (value < 0 || value > 1) break;
+      if (value < 0 || value > 2) break;
       b->fold_variant = value;
       drop_graph(b);
       return CUBLOX_OK;

@@ -494,7 +494,7 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
       g->opt_seg = value;
       return CUBLOX_OK;
     case CUBLOX_OPT_FOLD:
-      if (value < 0 || value > 2) break;
+      if (value < 0 || value > 3) break;
       g->opt_fold = value;
       return CUBLOX_OK;
     case CUBLOX_OPT_LAYOUT:
@@ -704,12 +704,13 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   a.variant = g->opt_fold;
   a.dirty = g->d_dirty;
   a.nlines = g->nlines;
+  a.err = g->d_err;
   a.vnum = static_cast<int>(std::min<int64_t>(g->nalloc, std::numeric_limits<int>::max()));
   tmark(g, 1, 0);
   launch_apply(a, g->stream);
   CK_LAUNCH();
   // the full sweeps leave the line flags set: clear them
-  if (a.variant != 2)
+  if (a.variant < 2)
     CK(cudaMemsetAsync(g->d_dirty, 0, static_cast<size_t>(g->nlines), g->stream));
   tmark(g, 1, 1);
   return CUBLOX_OK;

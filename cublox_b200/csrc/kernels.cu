@@ -175,6 +175,41 @@ __global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
   }
 }
 
+// Fold of the flagged lines, staged in shared memory by the bulk-copy
+// engine (fold_lines_bulk): 8 warps per CTA, each folding one contiguous
+// run of lines (a multiple of 32).
+constexpr int kBulkFoldWarps = 8;
+
+template <bool kStats>
+__global__ void __launch_bounds__(32 * kBulkFoldWarps) fold_bulk_kernel(const ApplyParams p) {
+  extern __shared__ __align__(128) unsigned char fsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  BulkStage *st = reinterpret_cast<BulkStage *>(fsm) + 2 * warp;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(fsm + 2 * kBulkFoldWarps * sizeof(BulkStage)) +
+                  2 * warp;
+  if (lane == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  const FoldView v = fold_view(p);
+  const int warps = gridDim.x * kBulkFoldWarps;
+  const int gw = blockIdx.x * kBulkFoldWarps + warp;
+  const int per = (((p.nlines + warps - 1) / warps) + 31) & ~31;
+  const int first = min(p.nlines, gw * per), end = min(p.nlines, first + per);
+  uint32_t phase = 0;
+  bool ok = true;
+  uint32_t touched = fold_lines_bulk(v, p.dirty, first, end, st, bar, phase, &ok);
+  if (!ok && lane == 0 && p.err) atomicOr(p.err, kErrWaitTimeout);
+  if (kStats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      touched += __shfl_down_sync(0xffffffffu, touched, off);
+    if (lane == 0 && touched) atomicAdd(p.stats + 3, static_cast<unsigned long long>(touched));
+  }
+}
+
 // Union-of-slabs clear.  One block per x slot: a marked x slab is one
 // contiguous run of ny*nz floats; otherwise every (x, y) column clears its
 // whole run if y is marked, else the marked z slots.
@@ -591,6 +626,27 @@ void launch_step_count(const RayParams &p, cudaStream_t s) {
 
 void launch_apply(const ApplyParams &p, cudaStream_t s) {
   if (p.variant == 2) {
+    if (p.nlines <= 0) return;
+    static bool attr = false;
+    const size_t smem = kBulkFoldWarps * kBulkWarpSmem;
+    if (!attr) {
+      cudaFuncSetAttribute(fold_bulk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem));
+      cudaFuncSetAttribute(fold_bulk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem));
+      attr = true;
+    }
+    const int groups = (p.nlines + 31) / 32;
+    int grid = (groups + kBulkFoldWarps * 16 - 1) / (kBulkFoldWarps * 16);  // >= 16 groups a warp
+    if (grid > sm_count()) grid = sm_count();
+    if (grid < 1) grid = 1;
+    if (p.stats)
+      fold_bulk_kernel<true><<<grid, 32 * kBulkFoldWarps, smem, s>>>(p);
+    else
+      fold_bulk_kernel<false><<<grid, 32 * kBulkFoldWarps, smem, s>>>(p);
+    return;
+  }
+  if (p.variant == 3) {
     if (p.nlines <= 0) return;
     const int groups = (p.nlines + 31) / 32;  // one warp per group of 32 lines
     int grid = (groups + 7) / 8;

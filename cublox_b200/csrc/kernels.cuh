@@ -82,9 +82,11 @@ struct ApplyParams {
   float l_hit, l_miss, l_min, l_max, l_unknown;
   unsigned fp;
   unsigned long long *stats;  // [3] += touched
-  int variant;                // 0 scalar sweep, 1 vector sweep, 2 dirty lines
-  uint8_t *dirty;             // variant 2: line flags (cleared as folded)
-  int nlines;                 // variant 2: lines
+  int variant;                // 0 scalar sweep, 1 vector sweep, 2 flagged lines
+                              // (bulk-copy gather), 3 flagged lines (registers)
+  uint8_t *dirty;             // variants 2, 3: line flags (cleared as folded)
+  int nlines;                 // variants 2, 3: lines
+  uint32_t *err;              // error word (a bounded wait that gave up)
 };
 
 struct ClearParams {

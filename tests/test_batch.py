@@ -142,7 +142,7 @@ def test_every_shape_gives_the_same_maps(shape):
     b = C.Batch()
     assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 10
     b.set_option(C.BATCH_OPT_SHAPE, shape)
-    b.set_option(C.BATCH_OPT_FOLD, shape % 2)
+    b.set_option(C.BATCH_OPT_FOLD, shape % 3)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
     bg, solo = setup(w, b)
     run_and_compare(w, b, bg, solo, feed_lists)
@@ -195,6 +195,6 @@ def test_batch_rejects_bad_calls():
     with pytest.raises(C.CubloxError):
         b.set_option(C.BATCH_OPT_SHAPE, 99)
     with pytest.raises(C.CubloxError):
-        b.set_option(C.BATCH_OPT_FOLD, 4)
+        b.set_option(C.BATCH_OPT_FOLD, 3)
     b.update([], [], np.zeros((0, 3), np.float32))
     b.close()
