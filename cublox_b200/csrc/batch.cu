@@ -69,13 +69,13 @@ constexpr int kWaitIters = 1 << 23;
 // Near phase of the two-phase walk (far_walk.cuh), from the ray's start.
 // Returns true if the ray's loop ended in it; false once the walk is inside
 // the window and outside the cube (f then holds it).
-template <int S>
+template <int S, int SZ = S>
 __device__ __forceinline__ bool walk_near(const RayParams &p, uint32_t *cube, const int clo[3],
                                           RayWalk &w, FarWalk &f, uint32_t &incs) {
   for (int k = 0;; ++k) {
     if (k >= w.max_steps || at_end(w)) return true;
     if (in_window(w, p)) {
-      const int c = cube_cell<S>(w.id[0], w.id[1], w.id[2], clo);
+      const int c = cube_cell<S, SZ>(w.id[0], w.id[1], w.id[2], clo);
       if (c < 0) {
         to_far(p, w, k, f);
         return false;
@@ -91,10 +91,10 @@ __device__ __forceinline__ bool walk_near(const RayParams &p, uint32_t *cube, co
 
 // One walk item: zero the cube, walk the item's rays (one thread per ray),
 // flush the cube into the map's counters.  Ends with a CTA barrier.
-template <int S>
+template <int S, int SZ = S>
 __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &item,
                                           uint32_t *cube) {
-  constexpr int kCube = S * S * S;
+  constexpr int kCube = S * S * SZ;
   const RayParams p = md.ray;
   const int clo[3] = {md.clo[0], md.clo[1], md.clo[2]};
   for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
@@ -106,13 +106,13 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
     RayWalk w;
     if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;
     ++rays;
-    const RayEnd re = ray_end_of<S>(p, w, clo);
+    const RayEnd re = ray_end_of<S, SZ>(p, w, clo);
     FarWalk f;
-    if (!walk_near<S>(p, cube, clo, w, f, incs)) walk_far(p, f, f.left, incs);
+    if (!walk_near<S, SZ>(p, cube, clo, w, f, incs)) walk_far(p, f, f.left, incs);
     apply_end<S>(p, cube, re, incs, hits);
   }
   __syncthreads();
-  flush_cube<S>(p, cube, clo);
+  flush_cube<S, SZ>(p, cube, clo);
   if (p.stats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -358,6 +358,28 @@ __global__ void __launch_bounds__(1024, kMinCtas) batch_walk_kernel(const MapDes
   }
 }
 
+// The same with a flat S x S x S/2 cube (64 KB at S = 32) and 512-thread
+// CTAs capped at 64 registers, so that two CTAs share an SM: twice the
+// resident warps of the 32^3 cube.  LiDAR beams within +-22.5 degrees stay
+// within +-0.66 m of the sensor's height inside the cube's +-1.6 m, so the
+// flat cube holds the same near field.
+template <int S>
+__global__ void __launch_bounds__(512, 2) batch_walk_flat_kernel(const MapDesc *maps,
+                                                                 const WalkItem *items,
+                                                                 int *counters) {
+  extern __shared__ uint32_t cube[];
+  __shared__ int s_item;
+  const int n_items = counters[1];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WalkItem item = items[it];
+    walk_item<S, S / 2>(maps[item.map], item, cube);
+  }
+}
+
 // Persistent walk without per-item barriers.  A CTA adopts one map at a
 // time (starting at blockIdx % maps, then the next map with rays left): it
 // zeroes its cube around that map's sensor, and its warps take 32-ray items
@@ -521,13 +543,15 @@ struct Shape {
   int min_ctas;  // 2: registers capped for two CTAs per SM (cube <= 16)
   int wq;        // 1: warps take 32-ray items of a CTA's current map (no item barriers)
   int refill;    // 1: two-phase items, lanes refilled from a far-state queue
+  int flat;      // 1: S x S x S/2 cube, two 512-thread CTAs per SM
 };
 
 const Shape kShapes[] = {{32, 512, 512, 0, 1, 0, 0},  {32, 1024, 1024, 0, 1, 0, 0},
                          {32, 0, 512, 0, 1, 1, 0},    {32, 0, 1024, 0, 1, 1, 0},
                          {16, 0, 512, 0, 1, 1, 0},    {16, 1024, 1024, 0, 2, 0, 0},
                          {32, 1024, 1024, 1, 1, 0, 0}, {16, 512, 512, 1, 1, 0, 0},
-                         {32, kRefillRays, 512, 0, 1, 0, 1}, {16, kRefillRays, 512, 0, 1, 0, 1}};
+                         {32, kRefillRays, 512, 0, 1, 0, 1}, {16, kRefillRays, 512, 0, 1, 0, 1},
+                         {32, 512, 512, 0, 2, 0, 0, 1},     {32, 256, 512, 0, 2, 0, 0, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 // The tuner's candidates: every launch shape with the default voxel layout
@@ -539,7 +563,7 @@ struct Candidate {
 };
 const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320},
                                  {5, 320}, {6, 320}, {7, 320}, {8, 320}, {9, 320},
-                                 {0, 230}, {0, 221}, {0, 0},   {8, 221}, {8, 0}};
+                                 {10, 320}, {11, 320}, {0, 230}, {0, 221}, {0, 0}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {
@@ -555,6 +579,7 @@ int sm_count_batch() {
 
 template <int S>
 const void *shape_kernel_s(const Shape &sh) {
+  if (sh.flat) return reinterpret_cast<const void *>(batch_walk_flat_kernel<S>);
   if (sh.refill) return reinterpret_cast<const void *>(batch_walk_refill_kernel<S>);
   if (sh.fused) return reinterpret_cast<const void *>(batch_fused_kernel<S>);
   if (sh.wq) return reinterpret_cast<const void *>(batch_walk_wq_kernel<S>);
@@ -571,7 +596,7 @@ const void *shape_kernel(const Shape &sh) {
 }
 
 size_t shape_smem(const Shape &sh) {
-  return sizeof(uint32_t) * (sh.cube * sh.cube * sh.cube +
+  return sizeof(uint32_t) * (sh.cube * sh.cube * (sh.flat ? sh.cube / 2 : sh.cube) +
                              (sh.refill ? kRefillRays * kFarWords : 0));
 }
 
@@ -1007,7 +1032,8 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     md.l_max = g->l_max;
     md.l_unknown = g->l_unknown;
     for (int a = 0; a < 3; ++a)
-      md.clo[a] = pos_to_global_dev(sensors[3 * i + a], g->res_inv, g->ctr, g->fp) - sh.cube / 2;
+      md.clo[a] = pos_to_global_dev(sensors[3 * i + a], g->res_inv, g->ctr, g->fp) -
+                  (a == 2 && sh.flat ? sh.cube / 4 : sh.cube / 2);
     md.n_walk = 0;
     for (int s0 = 0; s0 < c; s0 += rays_per_item, ++md.n_walk)
       b->h_witems[w++] = WalkItem{d, s0, std::min(rays_per_item, c - s0), 0};

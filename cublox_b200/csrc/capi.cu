@@ -142,7 +142,6 @@ int cublox_binary_version(int *binary_version) {
 
 static void free_all(cublox_grid *g) {
   cublox_b200::detail::dfree(g->d_dirty);
-  cublox_b200::detail::dfree(g->d_offtab);
   cublox_b200::detail::dfree(g->d_occ);
   cublox_b200::detail::dfree(g->d_cnt);
   cublox_b200::detail::dfree(g->d_hit);
@@ -263,31 +262,6 @@ void cublox_b200::detail::layout_to_reference(const cublox_grid *g, const float 
   }
 }
 
-// The far walk's address tables for the grid's layout (RayParams::tab),
-// enqueued on the grid's stream after the work that used the old ones.
-static int upload_offtab(cublox_grid *g) {
-  const size_t total = 3 * static_cast<size_t>(g->map[0] + g->map[1] + g->map[2]);
-  g->h_offtab.resize(total);
-  size_t at = 0;
-  for (int a = 0; a < 3; ++a) {
-    const int m = g->map[a];
-    for (int s = -m; s < 2 * m; ++s) g->h_offtab[at++] = vox_axis(g->lay, a, ((s % m) + m) % m);
-  }
-  CK(cudaMemcpyAsync(g->d_offtab, g->h_offtab.data(), total * sizeof(int),
-                     cudaMemcpyHostToDevice, g->stream));
-  // the host copy is the source of an asynchronous copy: keep it until done
-  CK(cudaStreamSynchronize(g->stream));
-  return CUBLOX_OK;
-}
-
-static void set_tables(const cublox_grid *g, RayParams &p) {
-  const int *t = g->d_offtab;
-  for (int a = 0; a < 3; ++a) {
-    p.tab[a] = t + g->map[a];
-    t += 3 * g->map[a];
-  }
-}
-
 int cublox_b200::detail::set_layout(cublox_grid *g, int code) {
   if (!layout_valid(code)) return fail(CUBLOX_ERR_INVALID, "layout: bricks must hold 32 voxels");
   if (code == g->lay_code) return CUBLOX_OK;
@@ -308,7 +282,7 @@ int cublox_b200::detail::set_layout(cublox_grid *g, int code) {
   g->lay = nl;
   g->lay_code = code;
   for (int a = 0; a < 3; ++a) g->nbr[a] = nbr[a];
-  return upload_offtab(g);
+  return CUBLOX_OK;
 }
 
 extern "C" {
@@ -394,8 +368,6 @@ int cublox_grid_create(const int half_map_size[3], float resolution,
   const size_t n = static_cast<size_t>(g->nalloc);
   if ((e = cublox_b200::detail::dmalloc(&g->d_dirty, static_cast<size_t>(g->nlines))) != cudaSuccess) return bail(e, "cudaMalloc line flags");
   if ((e = cudaMemsetAsync(g->d_dirty, 0, static_cast<size_t>(g->nlines), g->stream)) != cudaSuccess) return bail(e, "memset line flags");
-  if ((e = cublox_b200::detail::dmalloc(&g->d_offtab, 3 * sizeof(int) * static_cast<size_t>(g->map[0] + g->map[1] + g->map[2]))) != cudaSuccess) return bail(e, "cudaMalloc address tables");
-  if (upload_offtab(g) != CUBLOX_OK) return bail(cudaGetLastError(), "address tables");
   if ((e = cublox_b200::detail::dmalloc(&g->d_occ, n * sizeof(float))) != cudaSuccess) return bail(e, "cudaMalloc occ");
   if ((e = cublox_b200::detail::dmalloc(&g->d_cnt, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc cnt");
   if ((e = cublox_b200::detail::dmalloc(&g->d_hit, n * sizeof(uint32_t))) != cudaSuccess) return bail(e, "cudaMalloc hit");
@@ -617,7 +589,6 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
   p.err = g->d_err;
   p.lay = g->lay;
   p.dirty = g->d_dirty;
-  set_tables(g, p);
   if ((g->opt_raycast == 1 || (g->opt_raycast == 2 && g->opt_sort)) && n > g->bin_cap) {
     CK(cudaStreamSynchronize(g->stream));
     cublox_b200::detail::dfree(g->d_bins);
@@ -753,7 +724,6 @@ RayParams cublox_b200::detail::ray_params(const cublox_grid *g, const float *x,
   p.err = g->d_err;
   p.lay = g->lay;
   p.dirty = g->d_dirty;
-  set_tables(g, p);
   return p;
 }
 

@@ -26,7 +26,7 @@ struct FarWalk {
   float tM[3], tD[3];  // as in RayWalk
   int e[3];     // steps to the endpoint's coordinate on the axis (all 0: at the endpoint)
   int out[3];   // steps the walk can still take on the axis inside the window
-  int slot[3];  // ring-buffer slot of the current voxel on the axis, unwrapped
+  int slot[3];  // ring-buffer slot of the current voxel on the axis
   int st[3];    // step on the axis (-1, 0, 1)
   int off[3];   // the axis's term of the current voxel's address
   int left;     // loop iterations left (max_steps - k)
@@ -44,22 +44,24 @@ struct RayEnd {
 
 constexpr int kNever = 0x7fffffff;  // counters of an axis the ray never steps on
 
-template <int S>
+// Cell of a global voxel in the S x S x SZ shared-memory cube with corner
+// clo (z fastest), or -1 outside it.
+template <int S, int SZ = S>
 __device__ __forceinline__ int cube_cell(int g0, int g1, int g2, const int clo[3]) {
   const int c0 = g0 - clo[0], c1 = g1 - clo[1], c2 = g2 - clo[2];
   if (S > 0 && static_cast<unsigned>(c0) < static_cast<unsigned>(S) &&
       static_cast<unsigned>(c1) < static_cast<unsigned>(S) &&
-      static_cast<unsigned>(c2) < static_cast<unsigned>(S))
-    return (c0 * S + c1) * S + c2;
+      static_cast<unsigned>(c2) < static_cast<unsigned>(SZ))
+    return (c0 * S + c1) * SZ + c2;
   return -1;
 }
 
-template <int S>
+template <int S, int SZ = S>
 __device__ __forceinline__ RayEnd ray_end_of(const RayParams &p, const RayWalk &w,
                                              const int clo[3]) {
   RayEnd r;
   r.h = end_hash(w, p);
-  r.c = r.h >= 0 ? cube_cell<S>(w.en[0], w.en[1], w.en[2], clo) : -1;
+  r.c = r.h >= 0 ? cube_cell<S, SZ>(w.en[0], w.en[1], w.en[2], clo) : -1;
   r.hit = !w.clipped;
   return r;
 }
@@ -86,14 +88,15 @@ __device__ __forceinline__ void apply_end(const RayParams &p, uint32_t *cube, co
 // Add an S^3 shared-memory cube of counts (corner clo, global voxel index)
 // into the map's counters and flag their lines.  Only in-window voxels reach
 // the cube, so every non-zero cell has an address in the map.
-template <int S>
+template <int S, int SZ = S>
 __device__ __forceinline__ void flush_cube(const RayParams &p, const uint32_t *cube,
                                            const int clo[3]) {
   if constexpr (S > 0) {
-    for (int q = threadIdx.x; q < S * S * S; q += blockDim.x) {
+    for (int q = threadIdx.x; q < S * S * SZ; q += blockDim.x) {
       const uint32_t v = cube[q];
       if (!v) continue;
-      const int h = global_addr(p, clo[0] + q / (S * S), clo[1] + (q / S) % S, clo[2] + q % S);
+      const int h =
+          global_addr(p, clo[0] + q / (S * SZ), clo[1] + (q / SZ) % S, clo[2] + q % SZ);
       atomicAdd(p.cnt + h, v);
       if (p.dirty) p.dirty[h >> kLineShift] = 1;
     }
@@ -113,18 +116,16 @@ __device__ __forceinline__ void to_far(const RayParams &p, const RayWalk &w, int
     f.out[a] = st > 0 ? p.half[a] - w.rel[a] : (st < 0 ? p.half[a] + w.rel[a] : kNever);
     f.slot[a] = w.slot[a];
     f.st[a] = st;
-    f.off[a] = __ldg(p.tab[a] + w.slot[a]);
+    f.off[a] = vox_axis(p.lay, a, w.slot[a]);
   }
   f.left = w.max_steps - k;
   f.h = f.off[0] + f.off[1] + f.off[2];
   f.line = -1;
 }
 
-// One step on axis A (the tie rule picked it): the slot moves one step,
-// unwrapped, and the axis's address term is read from the axis's table,
-// which folds the ring buffer's wrap in.  In the far phase the walk takes at
-// most map[A] steps on an axis from a slot in [0, map[A]) before it leaves
-// the window, so the slot stays inside the table's [-map[A], 2 map[A]).
+// One step on axis A (the tie rule picked it): the slot moves with the ring
+// buffer's wrap and the axis's address term follows it (a few integer
+// operations, no memory access on the way to the next atomic's address).
 // Returns true if the new voxel is outside the window, which ends the loop:
 // the next iteration would break at its step limit, at the endpoint or as
 // out of the window for good.
@@ -132,8 +133,10 @@ template <int A>
 __device__ __forceinline__ bool far_step(FarWalk &f, const RayParams &p) {
   f.tM[A] = fadd(f.tM[A], f.tD[A]);
   --f.e[A];
-  f.slot[A] += f.st[A];
-  const int o = __ldg(p.tab[A] + f.slot[A]);
+  int s = f.slot[A] + f.st[A];
+  s = s == p.map[A] ? 0 : (s < 0 ? p.map[A] - 1 : s);
+  f.slot[A] = s;
+  const int o = vox_axis(p.lay, A, s);
   f.h += o - f.off[A];
   f.off[A] = o;
   return f.out[A]-- == 0;

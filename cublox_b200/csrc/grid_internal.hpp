@@ -77,8 +77,6 @@ struct cublox_grid {
   int64_t nalloc = 0;
   int nlines = 0;       // nalloc / 32
   uint8_t *d_dirty = nullptr;  // line flags (kernels.cuh)
-  int *d_offtab = nullptr;     // the far walk's per-axis address tables (RayParams::tab)
-  std::vector<int> h_offtab;   // their host copy (the source of the last upload)
   int nbr[3] = {0, 0, 0};      // bricks per axis in the current layout
 
   float *d_occ = nullptr;

@@ -68,10 +68,6 @@ struct RayParams {
   uint32_t *err;
   VoxLayout lay;
   uint8_t *dirty;  // line flags to set, or null (the fold sweeps every line)
-  // per axis a: tab[a][s] = vox_axis(lay, a, s mod map[a]) for s in
-  // [-map[a], 2 map[a]): the far walk's address terms with the ring
-  // buffer's wrap folded in (null where no far walk runs)
-  const int *tab[3];
 };
 
 struct ApplyParams {
