@@ -268,48 +268,31 @@ __device__ __forceinline__ FoldView fold_view(const MapDesc &m) {
                   m.l_unknown, m.ray.fp};
 }
 
-// Persistent fold with the flagged lines staged by the bulk-copy engine
-// (fold.cuh, fold_lines_bulk): CTAs take fold items from counters[2]; each
-// of the CTA's warps folds one contiguous eighth of the item.  A wait that
-// gives up flags kErrWaitTimeout in the map's error word, and the launch
-// skips the remaining folds (counters[4]).
-constexpr int kBulkFoldWarps = 8;
+// Persistent fold with the flagged lines staged in shared memory by
+// asynchronous copies (fold.cuh, fold_lines_staged): CTAs take fold items
+// from counters[2]; each of the CTA's warps folds one contiguous eighth of
+// the item.
+constexpr int kStagedFoldWarps = 8;
 
-__global__ void __launch_bounds__(32 * kBulkFoldWarps) batch_fold_bulk_kernel(
+__global__ void __launch_bounds__(32 * kStagedFoldWarps) batch_fold_staged_kernel(
     const MapDesc *maps, const FoldItem *items, int *counters) {
   extern __shared__ __align__(128) unsigned char fsm[];
   __shared__ int s_item;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  BulkStage *st = reinterpret_cast<BulkStage *>(fsm) + 2 * warp;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(fsm + 2 * kBulkFoldWarps * sizeof(BulkStage)) +
-                  2 * warp;
-  if (lane == 0) {
-    mbar_init(&bar[0]);
-    mbar_init(&bar[1]);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncwarp();
-  uint32_t phase = 0;
+  LineStage *st = reinterpret_cast<LineStage *>(fsm) + 2 * warp;
   const int n_items = counters[3];
   for (;;) {
-    if (threadIdx.x == 0)
-      s_item = *reinterpret_cast<volatile int *>(counters + 4) ? n_items
-                                                               : atomicAdd(&counters[2], 1);
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[2], 1);
     __syncthreads();
     const int it = s_item;
     __syncthreads();
     if (it >= n_items) break;
     const FoldItem item = items[it];
     const MapDesc &m = maps[item.map];
-    const int per = ((item.count + kBulkFoldWarps - 1) / kBulkFoldWarps + 31) & ~31;
+    const int per = ((item.count + kStagedFoldWarps - 1) / kStagedFoldWarps + 31) & ~31;
     const int first = item.start + min(item.count, warp * per);
     const int end = item.start + min(item.count, (warp + 1) * per);
-    bool ok = true;
-    uint32_t touched = fold_lines_bulk(fold_view(m), m.ray.dirty, first, end, st, bar, phase, &ok);
-    if (!ok && lane == 0) {
-      atomicOr(m.ray.err, kErrWaitTimeout);
-      atomicExch(counters + 4, 1);
-    }
+    uint32_t touched = fold_lines_staged(fold_view(m), m.ray.dirty, first, end, st);
     if (m.ray.stats) {
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1)
@@ -319,7 +302,6 @@ __global__ void __launch_bounds__(32 * kBulkFoldWarps) batch_fold_bulk_kernel(
     }
   }
 }
-
 
 // One fold item: the flagged lines among [start, start + count), the CTA's
 // warps taking groups of 32 lines in turn.  kAll: fold every line of the
@@ -555,15 +537,15 @@ const Shape kShapes[] = {{32, 512, 512, 0, 1, 0, 0},  {32, 1024, 1024, 0, 1, 0, 
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 // The tuner's candidates: every launch shape with the default voxel layout
-// (8 x 4 x 1 bricks), then the first shape with the other layouts (4 x 8 x
-// 1 and 4 x 4 x 2 bricks, the reference's hash order).  A candidate with
+// (8 x 4 x 1 bricks), then the flat-cube shape with the other layouts (4 x
+// 8 x 1 and 4 x 4 x 2 bricks, the reference's hash order).  A candidate with
 // another layout moves every grid of the update to it first.
 struct Candidate {
   int shape, layout;
 };
 const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320},
                                  {5, 320}, {6, 320}, {7, 320}, {8, 320}, {9, 320},
-                                 {10, 320}, {11, 320}, {0, 230}, {0, 221}, {0, 0}};
+                                 {10, 320}, {11, 320}, {10, 230}, {10, 221}, {10, 0}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {
@@ -649,14 +631,14 @@ cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counte
   const dim3 grid(sm_count_batch() * 8), block(256);
   if (variant == 0) {
     static bool attr = false;
-    const size_t smem = kBulkFoldWarps * kBulkWarpSmem;
+    const size_t smem = kStagedFoldWarps * kStageWarpSmem;
     if (!attr) {
-      cudaFuncSetAttribute(batch_fold_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(batch_fold_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem));
       attr = true;
     }
-    batch_fold_bulk_kernel<<<sm_count_batch(), 32 * kBulkFoldWarps, smem, s>>>(maps, fitems,
-                                                                             counters);
+    batch_fold_staged_kernel<<<sm_count_batch(), 32 * kStagedFoldWarps, smem, s>>>(maps, fitems,
+                                                                                  counters);
   } else if (variant == 1) {
     batch_fold_kernel<true><<<grid, block, 0, s>>>(maps, fitems, counters);
   } else {

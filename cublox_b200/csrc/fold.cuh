@@ -136,62 +136,30 @@ __device__ __forceinline__ uint32_t fold_lines(const FoldView &v, uint8_t *dirty
   return touched;
 }
 
-// ---- flagged lines gathered by the bulk-copy engine -------------------------
+// ---- flagged lines gathered into shared memory by asynchronous copies ----
 // The register fold above keeps at most kLines lines in flight per warp, and
 // the fold is bound by how many scattered 128-byte lines are in flight.
-// Here each warp stages its flagged lines in shared memory with
-// cp.async.bulk (the copy engine needs no registers): for a group of 32
-// line flags, the lanes of flagged lines each issue two 128-byte copies
-// (counters, stored values) completing on the stage's mbarrier, while the
-// warp folds the previous group out of the other stage.  Waits are bounded:
-// one that gives up flags kErrWaitTimeout and the warp stops folding (after
-// a bounded wait for its own copies).
+// Here each warp stages up to 32 flagged lines at a time in shared memory
+// with cp.async (16 bytes a lane, the data never passes through registers):
+// a stage of 32 lines x (counters, values) is 16 instructions for the warp,
+// and the next stage's copies are in flight while the warp folds the
+// current one out of shared memory.  (One cp.async.bulk per 128-byte line,
+// tried first, ran at half the speed: the copy engine's per-copy cost
+// dominates at this size.)
 
-constexpr int kBulkWaitSpin = 1 << 22;  // try_wait polls before a wait gives up
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(
+                   __cvta_generic_to_shared(smem_dst))),
+               "l"(gmem_src)
                : "memory");
 }
 
-__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes,
-                                          uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int i = 0; i < kBulkWaitSpin; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
 // Shared memory of one warp: two stages of 32 lines x (counters, values).
-struct BulkStage {
+struct LineStage {
   uint32_t cnt[32][32];
   float occ[32][32];
 };
-constexpr size_t kBulkWarpSmem = 2 * sizeof(BulkStage) + 2 * sizeof(uint64_t);
+constexpr size_t kStageWarpSmem = 2 * sizeof(LineStage);
 
 // A warp's position in its line range: the next flag group to read and the
 // flagged lines of the current group not taken yet.
@@ -234,51 +202,45 @@ __device__ __forceinline__ int collect_lines(uint8_t *dirty, int end, LineCursor
   return n;
 }
 
-// Copies of the n lines held by the lanes (my_line) into stage `st`: lane 0
-// arms the barrier with their bytes, then each lane with a line copies its
-// counters and values into its own slot.
-__device__ __forceinline__ void bulk_issue(const FoldView &v, int n, int my_line, BulkStage *st,
-                                           uint64_t *bar) {
+// Copies of the n lines held by the lanes (my_line, slots 0..n-1) into
+// stage `st`, as one commit group: 256 16-byte chunks per array, chunk
+// k * 32 + lane being part (lane & 7) of slot 4 k + (lane >> 3).
+__device__ __forceinline__ void stage_issue(const FoldView &v, int n, int my_line,
+                                            LineStage *st) {
   const int lane = threadIdx.x & 31;
-  if (lane == 0) mbar_expect(bar, 256u * static_cast<uint32_t>(n));
-  __syncwarp();
-  if (my_line >= 0) {
-    const size_t at = static_cast<size_t>(my_line) << kLineShift;
-    bulk_copy(st->cnt[lane], v.cnt + at, 128u, bar);
-    bulk_copy(st->occ[lane], v.occ + at, 128u, bar);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int slot = 4 * k + (lane >> 3), part = lane & 7;
+    const int line = __shfl_sync(0xffffffffu, my_line, slot);
+    if (slot < n) {
+      const size_t at = (static_cast<size_t>(line) << kLineShift) + 4 * part;
+      cp_async16(&st->cnt[slot][4 * part], v.cnt + at);
+      cp_async16(&st->occ[slot][4 * part], v.occ + at);
+    }
   }
+  asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-// The flagged lines of [first, end) by one warp with its two stages `st`
-// and barriers `bar` (initialised; `phase` their parities, kept across
-// calls).  Stages hold up to 32 lines each, collected across flag groups,
-// so a warp keeps up to 64 lines (16 KB) in flight whatever the density.
-// Returns the voxels folded; *ok = false if a wait gave up.
-__device__ __forceinline__ uint32_t fold_lines_bulk(const FoldView &v, uint8_t *dirty, int first,
-                                                    int end, BulkStage *st, uint64_t *bar,
-                                                    uint32_t &phase, bool *ok) {
+// The flagged lines of [first, end) by one warp with its two stages `st`.
+// Returns the voxels folded.
+__device__ __forceinline__ uint32_t fold_lines_staged(const FoldView &v, uint8_t *dirty,
+                                                      int first, int end, LineStage *st) {
   const int lane = threadIdx.x & 31;
   uint32_t touched = 0;
   LineCursor c{first, 0u, false};
   int cur = 0, line = -1;
   int n = collect_lines(dirty, end, c, line);
-  if (n) bulk_issue(v, n, line, &st[cur], &bar[cur]);
+  if (n) stage_issue(v, n, line, &st[cur]);
   while (n) {
     int nline = -1;
     const int nn = collect_lines(dirty, end, c, nline);
     if (nn) {
-      // the other stage was last read by this warp's generic loads
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      bulk_issue(v, nn, nline, &st[cur ^ 1], &bar[cur ^ 1]);
+      stage_issue(v, nn, nline, &st[cur ^ 1]);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
-    if (!mbar_wait(&bar[cur], (phase >> cur) & 1u)) {
-      *ok = false;
-      // bounded waits for this warp's copies still in flight, then stop
-      mbar_wait(&bar[cur], (phase >> cur) & 1u);
-      if (nn) mbar_wait(&bar[cur ^ 1], (phase >> (cur ^ 1)) & 1u);
-      return touched;
-    }
-    phase ^= 1u << cur;
+    __syncwarp();
     for (int j = 0; j < n; ++j) {
       const int at = (__shfl_sync(0xffffffffu, line, j) << kLineShift) + lane;
       const uint32_t cv = st[cur].cnt[j][lane];

@@ -175,33 +175,22 @@ __global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
   }
 }
 
-// Fold of the flagged lines, staged in shared memory by the bulk-copy
-// engine (fold_lines_bulk): 8 warps per CTA, each folding one contiguous
-// run of lines (a multiple of 32).
-constexpr int kBulkFoldWarps = 8;
+// Fold of the flagged lines, staged in shared memory by asynchronous copies
+// (fold_lines_staged): 8 warps per CTA, each folding one contiguous run of
+// lines (a multiple of 32).
+constexpr int kStagedFoldWarps = 8;
 
 template <bool kStats>
-__global__ void __launch_bounds__(32 * kBulkFoldWarps) fold_bulk_kernel(const ApplyParams p) {
+__global__ void __launch_bounds__(32 * kStagedFoldWarps) fold_staged_kernel(const ApplyParams p) {
   extern __shared__ __align__(128) unsigned char fsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  BulkStage *st = reinterpret_cast<BulkStage *>(fsm) + 2 * warp;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(fsm + 2 * kBulkFoldWarps * sizeof(BulkStage)) +
-                  2 * warp;
-  if (lane == 0) {
-    mbar_init(&bar[0]);
-    mbar_init(&bar[1]);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncwarp();
+  LineStage *st = reinterpret_cast<LineStage *>(fsm) + 2 * warp;
   const FoldView v = fold_view(p);
-  const int warps = gridDim.x * kBulkFoldWarps;
-  const int gw = blockIdx.x * kBulkFoldWarps + warp;
+  const int warps = gridDim.x * kStagedFoldWarps;
+  const int gw = blockIdx.x * kStagedFoldWarps + warp;
   const int per = (((p.nlines + warps - 1) / warps) + 31) & ~31;
   const int first = min(p.nlines, gw * per), end = min(p.nlines, first + per);
-  uint32_t phase = 0;
-  bool ok = true;
-  uint32_t touched = fold_lines_bulk(v, p.dirty, first, end, st, bar, phase, &ok);
-  if (!ok && lane == 0 && p.err) atomicOr(p.err, kErrWaitTimeout);
+  uint32_t touched = fold_lines_staged(v, p.dirty, first, end, st);
   if (kStats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
@@ -628,22 +617,22 @@ void launch_apply(const ApplyParams &p, cudaStream_t s) {
   if (p.variant == 2) {
     if (p.nlines <= 0) return;
     static bool attr = false;
-    const size_t smem = kBulkFoldWarps * kBulkWarpSmem;
+    const size_t smem = kStagedFoldWarps * kStageWarpSmem;
     if (!attr) {
-      cudaFuncSetAttribute(fold_bulk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(fold_staged_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem));
-      cudaFuncSetAttribute(fold_bulk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(fold_staged_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem));
       attr = true;
     }
     const int groups = (p.nlines + 31) / 32;
-    int grid = (groups + kBulkFoldWarps * 16 - 1) / (kBulkFoldWarps * 16);  // >= 16 groups a warp
+    int grid = (groups + kStagedFoldWarps * 16 - 1) / (kStagedFoldWarps * 16);  // >= 16 groups a warp
     if (grid > sm_count()) grid = sm_count();
     if (grid < 1) grid = 1;
     if (p.stats)
-      fold_bulk_kernel<true><<<grid, 32 * kBulkFoldWarps, smem, s>>>(p);
+      fold_staged_kernel<true><<<grid, 32 * kStagedFoldWarps, smem, s>>>(p);
     else
-      fold_bulk_kernel<false><<<grid, 32 * kBulkFoldWarps, smem, s>>>(p);
+      fold_staged_kernel<false><<<grid, 32 * kStagedFoldWarps, smem, s>>>(p);
     return;
   }
   if (p.variant == 3) {

@@ -113,9 +113,9 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 #define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (64)   */
 #define CUBLOX_OPT_FOLD 6    /* fold: 0 scalar sweep of every counter, 1
                                 16-byte sweep; only the 32-voxel lines the
-                                scan flagged: 2 (default) gathered into
-                                shared memory by the bulk-copy engine, 3
-                                through registers                          */
+                                scan flagged: 2 (default) staged in shared
+                                memory by asynchronous copies, 3 through
+                                registers                                  */
 #define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
 #define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
                                    consecutive segments (default 0: all
@@ -290,14 +290,15 @@ typedef struct cublox_batch cublox_batch;
                                          voxel layout over the first
                                          updates (default 1): each candidate
                                          (every shape with 8 x 4 x 1
-                                         bricks, the first shape with the
-                                         other layouts) is timed twice      */
+                                         bricks, the flat-cube shape with
+                                         the other layouts) is timed twice  */
 #define CUBLOX_BATCH_OPT_SHAPE 3      /* fix the launch shape (0 .. n-1)    */
 #define CUBLOX_BATCH_OPT_TIMING 4     /* record walk/fold device times      */
 #define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
 #define CUBLOX_BATCH_OPT_FOLD 6       /* fold: 0 (default) the 32-voxel
-                                         lines the walk flagged, gathered by
-                                         the bulk-copy engine; 1 every line
+                                         lines the walk flagged, staged in
+                                         shared memory by asynchronous
+                                         copies; 1 every line
                                          (the reference's full sweep, for
                                          comparison); 2 the flagged lines
                                          through registers                  */
