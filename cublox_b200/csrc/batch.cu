@@ -310,7 +310,7 @@ template <bool kL2, bool kAll = false>
 __device__ __forceinline__ uint32_t fold_item(const MapDesc &m, const FoldItem &item) {
   const FoldView v = fold_view(m);
   const int warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  return fold_lines<4, kL2, kAll>(v, m.ray.dirty, item.start + 32 * warp, item.start + item.count,
+  return fold_lines<8, kL2, kAll>(v, m.ray.dirty, item.start + 32 * warp, item.start + item.count,
                                   32 * warps);
 }
 
@@ -629,7 +629,7 @@ cudaError_t launch_walk(const MapDesc *maps, const WalkItem *witems, const FoldI
 cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counters,
                         int variant, cudaStream_t s) {
   const dim3 grid(sm_count_batch() * 8), block(256);
-  if (variant == 0) {
+  if (variant == 2) {
     static bool attr = false;
     const size_t smem = kStagedFoldWarps * kStageWarpSmem;
     if (!attr) {

@@ -98,11 +98,16 @@ __device__ __forceinline__ uint32_t fold_lines(const FoldView &v, uint8_t *dirty
                                                int end, int stride) {
   const int lane = threadIdx.x & 31;
   uint32_t touched = 0;
+  auto flag = [&](int l) -> bool {
+    return l < end && (kAll || (kL2 ? __ldcg(dirty + l) : dirty[l]) != 0);
+  };
+  bool next = flag(first + lane);  // the group's flags are read a group ahead
   for (int base = first; base < end; base += stride) {
     const int l = base + lane;
-    const bool d = l < end && (kAll || (kL2 ? __ldcg(dirty + l) : dirty[l]) != 0);
+    const bool d = next;
     uint32_t mask = __ballot_sync(0xffffffffu, d);
     if (d) dirty[l] = 0;
+    next = flag(base + stride + lane);
     while (mask) {
       int at[kLines];
 #pragma unroll

@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
   const FoldView v = fold_view(p);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  uint32_t touched = fold_lines<4, false>(v, p.dirty, warp * 32, p.nlines, warps * 32);
+  uint32_t touched = fold_lines<8, false>(v, p.dirty, warp * 32, p.nlines, warps * 32);
   if (kStats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
@@ -614,7 +614,7 @@ void launch_step_count(const RayParams &p, cudaStream_t s) {
 }
 
 void launch_apply(const ApplyParams &p, cudaStream_t s) {
-  if (p.variant == 2) {
+  if (p.variant == 3) {
     if (p.nlines <= 0) return;
     static bool attr = false;
     const size_t smem = kStagedFoldWarps * kStageWarpSmem;
@@ -635,7 +635,7 @@ void launch_apply(const ApplyParams &p, cudaStream_t s) {
       fold_staged_kernel<false><<<grid, 32 * kStagedFoldWarps, smem, s>>>(p);
     return;
   }
-  if (p.variant == 3) {
+  if (p.variant == 2) {
     if (p.nlines <= 0) return;
     const int groups = (p.nlines + 31) / 32;  // one warp per group of 32 lines
     int grid = (groups + 7) / 8;

@@ -339,6 +339,23 @@ def test_readme_scale_scan_exact():
     assert same_bits(occ, o.occ())
 
 
+@pytest.mark.parametrize("fold", [0, 1, 2, 3])
+def test_fold_variants_exact(small, fold):
+    """Every fold (full sweeps, flagged lines through registers or staged in
+    shared memory) gives the oracle's map over scans that move the sensor,
+    and leaves no line flagged behind."""
+    w, pts, s = small
+    g, o = pair(w.half, w.resolution, max_range=w.sensor.max_range)
+    g.set_option(C.OPT_FOLD, fold)
+    assert g.get_option(C.OPT_FOLD) == fold
+    for k in range(3):
+        so = (s + np.float32([1.7 * k, -0.9 * k, 0.1 * k])).astype(np.float32)
+        g.update(pts, so)
+        o.update(pts, so)
+        assert same_bits(g.export(), o.occ()), k
+    assert g.check() == 0
+
+
 VARIANTS = [dict(raycast=0), dict(raycast=1, cube=32, match=1, sort=1),
             dict(raycast=1, cube=16, match=0, sort=1), dict(raycast=1, cube=0, match=1, sort=0),
             dict(raycast=2, cube=32, seg=48), dict(raycast=2, cube=0, seg=4, sort=0),
