@@ -61,6 +61,7 @@ struct FoldItem {
 // its waits and folds), [5] the fused launch's wait limit (sleep rounds)
 constexpr int kCounters = 6;
 constexpr int kFoldItemLines = 1 << 12;  // 32-voxel lines per fold item
+static_assert(kFoldItemLines == kListLines, "a fold item is one CTA's line list");
 // Fused launch: how long a fold item waits for its map's walk items
 // (rounds of a ~256 ns sleep, about 2 s) before it gives up and flags
 // kErrWaitTimeout in the map's error word (CUBLOX_BATCH_OPT_WAIT_LIMIT).
@@ -268,41 +269,6 @@ __device__ __forceinline__ FoldView fold_view(const MapDesc &m) {
                   m.l_unknown, m.ray.fp};
 }
 
-// Persistent fold with the flagged lines staged in shared memory by
-// asynchronous copies (fold.cuh, fold_lines_staged): CTAs take fold items
-// from counters[2]; each of the CTA's warps folds one contiguous eighth of
-// the item.
-constexpr int kStagedFoldWarps = 8;
-
-__global__ void __launch_bounds__(32 * kStagedFoldWarps) batch_fold_staged_kernel(
-    const MapDesc *maps, const FoldItem *items, int *counters) {
-  extern __shared__ __align__(128) unsigned char fsm[];
-  __shared__ int s_item;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  LineStage *st = reinterpret_cast<LineStage *>(fsm) + 2 * warp;
-  const int n_items = counters[3];
-  for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(&counters[2], 1);
-    __syncthreads();
-    const int it = s_item;
-    __syncthreads();
-    if (it >= n_items) break;
-    const FoldItem item = items[it];
-    const MapDesc &m = maps[item.map];
-    const int per = ((item.count + kStagedFoldWarps - 1) / kStagedFoldWarps + 31) & ~31;
-    const int first = item.start + min(item.count, warp * per);
-    const int end = item.start + min(item.count, (warp + 1) * per);
-    uint32_t touched = fold_lines_staged(fold_view(m), m.ray.dirty, first, end, st);
-    if (m.ray.stats) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1)
-        touched += __shfl_down_sync(0xffffffffu, touched, off);
-      if (lane == 0 && touched)
-        atomicAdd(m.ray.stats + 3, static_cast<unsigned long long>(touched));
-    }
-  }
-}
-
 // One fold item: the flagged lines among [start, start + count), the CTA's
 // warps taking groups of 32 lines in turn.  kAll: fold every line of the
 // item, flagged or not (the reference's full sweep, for comparison).
@@ -454,6 +420,40 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
     const FoldItem item = items[it];
     const MapDesc &m = maps[item.map];
     add_touched(m, fold_item<false, kAll>(m, item));
+  }
+}
+
+// Persistent fold over per-item lists of the flagged lines (fold.cuh,
+// build_line_list / fold_line_list): CTAs take fold items from counters[2]
+// and load the next item's flags before folding the current list.
+__global__ void __launch_bounds__(kListThreads, 3) batch_fold_list_kernel(const MapDesc *maps,
+                                                                          const FoldItem *items,
+                                                                          int *counters) {
+  __shared__ LineList L;
+  __shared__ int s_item;
+  const int n_items = counters[3];
+  if (threadIdx.x == 0) s_item = atomicAdd(&counters[2], 1);
+  __syncthreads();
+  int it = s_item;
+  uint4 f = make_uint4(0u, 0u, 0u, 0u);
+  if (it < n_items) {
+    const FoldItem fi = items[it];
+    f = load_line_flags(maps[fi.map].ray.dirty, fi.start, fi.count);
+  }
+  while (it < n_items) {
+    const FoldItem item = items[it];
+    const MapDesc &m = maps[item.map];
+    const int n = build_line_list(line_flag_bits(f), L, m.ray.dirty, item.start, item.count);
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[2], 1);
+    __syncthreads();
+    const int next = s_item;
+    if (next < n_items) {
+      const FoldItem fi = items[next];
+      f = load_line_flags(maps[fi.map].ray.dirty, fi.start, fi.count);
+    }
+    add_touched(m, fold_line_list<4, false>(fold_view(m), L, n, item.start));
+    __syncthreads();  // the list and s_item are rewritten next
+    it = next;
   }
 }
 
@@ -629,16 +629,8 @@ cudaError_t launch_walk(const MapDesc *maps, const WalkItem *witems, const FoldI
 cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counters,
                         int variant, cudaStream_t s) {
   const dim3 grid(sm_count_batch() * 8), block(256);
-  if (variant == 2) {
-    static bool attr = false;
-    const size_t smem = kStagedFoldWarps * kStageWarpSmem;
-    if (!attr) {
-      cudaFuncSetAttribute(batch_fold_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
-      attr = true;
-    }
-    batch_fold_staged_kernel<<<sm_count_batch(), 32 * kStagedFoldWarps, smem, s>>>(maps, fitems,
-                                                                                  counters);
+  if (variant == 0) {
+    batch_fold_list_kernel<<<sm_count_batch() * 3, kListThreads, 0, s>>>(maps, fitems, counters);
   } else if (variant == 1) {
     batch_fold_kernel<true><<<grid, block, 0, s>>>(maps, fitems, counters);
   } else {

@@ -141,126 +141,127 @@ __device__ __forceinline__ uint32_t fold_lines(const FoldView &v, uint8_t *dirty
   return touched;
 }
 
-// ---- flagged lines gathered into shared memory by asynchronous copies ----
-// The register fold above keeps at most kLines lines in flight per warp, and
-// the fold is bound by how many scattered 128-byte lines are in flight.
-// Here each warp stages up to 32 flagged lines at a time in shared memory
-// with cp.async (16 bytes a lane, the data never passes through registers):
-// a stage of 32 lines x (counters, values) is 16 instructions for the warp,
-// and the next stage's copies are in flight while the warp folds the
-// current one out of shared memory.  (One cp.async.bulk per 128-byte line,
-// tried first, ran at half the speed: the copy engine's per-copy cost
-// dominates at this size.)
+// ---- flagged lines compacted into a list per CTA ----
+// The per-warp fold above reads 32 flags, then folds only the flagged ones
+// among them: about 9 of 32 lines at README scale, so a warp rarely has more
+// than one batch of lines in flight and waits a full memory latency on every
+// flag group.  Here a 256-thread CTA takes 4096 lines at a time: one 16-byte
+// flag load per thread, a CTA-wide prefix sum turns the flagged lines into a
+// dense list in shared memory (flags cleared on the way), and the warps then
+// fold the list four lines per warp access (8 lanes x 16 bytes a line) with
+// kQuads accesses in flight per warp, so every warp has 4 kQuads lines in
+// flight until the list runs out.  The next item's flags are loaded before
+// the current list is folded.
 
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(
-                   __cvta_generic_to_shared(smem_dst))),
-               "l"(gmem_src)
-               : "memory");
-}
+constexpr int kListThreads = 256;
+constexpr int kListLines = 16 * kListThreads;  // lines per item: 16 flags per thread
+constexpr int kListWarps = kListThreads / 32;
 
-// Shared memory of one warp: two stages of 32 lines x (counters, values).
-struct LineStage {
-  uint32_t cnt[32][32];
-  float occ[32][32];
-};
-constexpr size_t kStageWarpSmem = 2 * sizeof(LineStage);
-
-// A warp's position in its line range: the next flag group to read and the
-// flagged lines of the current group not taken yet.
-struct LineCursor {
-  int base;       // first line of the current group of 32
-  uint32_t pend;  // bit j: line base + j is flagged and not taken yet
-  bool read;      // pend holds the current group's flags
+struct LineList {
+  uint16_t line[kListLines];  // flagged lines, relative to the item's first line
+  int warp_sum[kListWarps];
 };
 
-// Up to 32 flagged lines from [cursor, end): lane j of the warp gets the
-// j-th line (or -1), flags are cleared as their groups are read.  Returns
-// how many lines were taken.
-__device__ __forceinline__ int collect_lines(uint8_t *dirty, int end, LineCursor &c,
-                                             int &my_line) {
-  const int lane = threadIdx.x & 31;
-  int n = 0;
-  my_line = -1;
-  while (n < 32) {
-    if (!c.read) {
-      if (c.base >= end) break;
-      const int l = c.base + lane;
-      const bool d = l < end && dirty[l] != 0;
-      c.pend = __ballot_sync(0xffffffffu, d);
-      if (d) dirty[l] = 0;
-      c.read = true;
-    }
-    if (c.pend) {
-      const int take = min(__popc(c.pend), 32 - n);
-      const int r = lane - n;
-      if (r >= 0 && r < take) my_line = c.base + static_cast<int>(__fns(c.pend, 0, r + 1));
-      const int last = static_cast<int>(__fns(c.pend, 0, take));  // bit of the take-th line
-      c.pend &= ~((2u << last) - 1u);
-      n += take;
-    }
-    if (!c.pend) {
-      c.base += 32;
-      c.read = false;
-    }
-  }
-  return n;
+// The raw flags of this thread's lines start + 16 t .. + 15 (bytes of lines
+// at or beyond `count` read as zero); `dirty + start` is 16-byte aligned.
+// The value is used only by line_flag_bits, so the load can stay in flight
+// across other work.
+__device__ __forceinline__ uint4 load_line_flags(const uint8_t *dirty, int start, int count) {
+  const int i = 16 * static_cast<int>(threadIdx.x);
+  if (i + 16 <= count) return *reinterpret_cast<const uint4 *>(dirty + start + i);
+  uint32_t w[4] = {0u, 0u, 0u, 0u};
+  for (int j = 0; i + j < count && j < 16; ++j)
+    w[j >> 2] |= static_cast<uint32_t>(dirty[start + i + j] != 0) << (8 * (j & 3));
+  return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// Copies of the n lines held by the lanes (my_line, slots 0..n-1) into
-// stage `st`, as one commit group: 256 16-byte chunks per array, chunk
-// k * 32 + lane being part (lane & 7) of slot 4 k + (lane >> 3).
-__device__ __forceinline__ void stage_issue(const FoldView &v, int n, int my_line,
-                                            LineStage *st) {
-  const int lane = threadIdx.x & 31;
+// One bit per non-zero flag byte: bit j for byte j of the 16.
+__device__ __forceinline__ uint32_t line_flag_bits(const uint4 &f) {
+  const uint32_t w[4] = {f.x, f.y, f.z, f.w};
+  uint32_t m = 0;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int slot = 4 * k + (lane >> 3), part = lane & 7;
-    const int line = __shfl_sync(0xffffffffu, my_line, slot);
-    if (slot < n) {
-      const size_t at = (static_cast<size_t>(line) << kLineShift) + 4 * part;
-      cp_async16(&st->cnt[slot][4 * part], v.cnt + at);
-      cp_async16(&st->occ[slot][4 * part], v.occ + at);
-    }
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t nz = __vcmpne4(w[k], 0u) & 0x01010101u;  // bits 0, 8, 16, 24
+    m |= ((nz | (nz >> 7) | (nz >> 14) | (nz >> 21)) & 0xfu) << (4 * k);
   }
-  asm volatile("cp.async.commit_group;" ::: "memory");
+  return m;
 }
 
-// The flagged lines of [first, end) by one warp with its two stages `st`.
-// Returns the voxels folded.
-__device__ __forceinline__ uint32_t fold_lines_staged(const FoldView &v, uint8_t *dirty,
-                                                      int first, int end, LineStage *st) {
-  const int lane = threadIdx.x & 31;
+// The CTA's list from every thread's flag bits `m` (item of `count` lines
+// from line `start`); clears the flags it found.  Returns the list's
+// length.  Contains two CTA barriers, the last at the end.
+__device__ __forceinline__ int build_line_list(uint32_t m, LineList &L, uint8_t *dirty, int start,
+                                               int count) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = __popc(m);
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) L.warp_sum[warp] = incl;
+  __syncthreads();
+  int pos = incl - c, total = 0;
+#pragma unroll
+  for (int w = 0; w < kListWarps; ++w) {
+    const int s = L.warp_sum[w];
+    pos += w < warp ? s : 0;
+    total += s;
+  }
+  const int i = 16 * static_cast<int>(threadIdx.x);
+  for (uint32_t r = m; r; r &= r - 1) L.line[pos++] = static_cast<uint16_t>(i + __ffs(r) - 1);
+  if (m) {
+    if (i + 16 <= count)  // the thread's 16 flags are one aligned 16-byte word
+      *reinterpret_cast<uint4 *>(dirty + start + i) = make_uint4(0u, 0u, 0u, 0u);
+    else
+      for (uint32_t r = m; r; r &= r - 1) dirty[start + i + __ffs(r) - 1] = 0;
+  }
+  __syncthreads();
+  return total;
+}
+
+// Fold of the CTA's list of n lines (item's first line `start`).  Warp w
+// takes line quads w, w + kListWarps, ...; lane (q, s) = (lane / 8, lane % 8)
+// handles 16-byte piece s of the quad's line q.  A piece whose counters are
+// all zero is left as it is (its values do not change, its counters are
+// zero already).  kL2: counters are read at L2.  Returns the voxels folded.
+template <int kQuads, bool kL2>
+__device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const LineList &L, int n,
+                                                   int start) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q = lane >> 3, sub = lane & 7;
+  const uint4 *c4r = reinterpret_cast<const uint4 *>(v.cnt);
+  uint4 *c4 = reinterpret_cast<uint4 *>(v.cnt);
+  float4 *o4 = reinterpret_cast<float4 *>(v.occ);
   uint32_t touched = 0;
-  LineCursor c{first, 0u, false};
-  int cur = 0, line = -1;
-  int n = collect_lines(dirty, end, c, line);
-  if (n) stage_issue(v, n, line, &st[cur]);
-  while (n) {
-    int nline = -1;
-    const int nn = collect_lines(dirty, end, c, nline);
-    if (nn) {
-      stage_issue(v, nn, nline, &st[cur ^ 1]);
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
+  const int quads = (n + 3) >> 2;
+  for (int i0 = warp; i0 < quads; i0 += kQuads * kListWarps) {
+    int at[kQuads];
+#pragma unroll
+    for (int u = 0; u < kQuads; ++u) {
+      const int k = 4 * (i0 + u * kListWarps) + q;
+      at[u] = k < n ? ((start + L.line[k]) << 3) + sub : -1;  // index of the 16-byte piece
     }
-    __syncwarp();
-    for (int j = 0; j < n; ++j) {
-      const int at = (__shfl_sync(0xffffffffu, line, j) << kLineShift) + lane;
-      const uint32_t cv = st[cur].cnt[j][lane];
-      float o = st[cur].occ[j][lane];
-      if (cv) {
-        o = fold_counter(v, at, cv, o);
-        ++touched;
-      }
-      v.occ[at] = o;
-      v.cnt[at] = 0u;
+    uint4 c[kQuads];
+    float4 o[kQuads];
+#pragma unroll
+    for (int u = 0; u < kQuads; ++u)
+      if (at[u] >= 0) c[u] = kL2 ? __ldcg(c4r + at[u]) : c4r[at[u]];
+#pragma unroll
+    for (int u = 0; u < kQuads; ++u)
+      if (at[u] >= 0) o[u] = o4[at[u]];
+#pragma unroll
+    for (int u = 0; u < kQuads; ++u) {
+      if (at[u] < 0 || !any_set(c[u])) continue;
+      const int h = at[u] << 2;
+      if (c[u].x) { o[u].x = fold_counter(v, h + 0, c[u].x, o[u].x); ++touched; }
+      if (c[u].y) { o[u].y = fold_counter(v, h + 1, c[u].y, o[u].y); ++touched; }
+      if (c[u].z) { o[u].z = fold_counter(v, h + 2, c[u].z, o[u].z); ++touched; }
+      if (c[u].w) { o[u].w = fold_counter(v, h + 3, c[u].w, o[u].w); ++touched; }
+      o4[at[u]] = o[u];
+      c4[at[u]] = make_uint4(0u, 0u, 0u, 0u);
     }
-    __syncwarp();
-    cur ^= 1;
-    n = nn;
-    line = nline;
   }
   return touched;
 }

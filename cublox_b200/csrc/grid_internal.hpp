@@ -46,7 +46,7 @@ struct cublox_grid {
   // kernel options (cublox_grid_set_option)
   int opt_raycast = 2;  // 0 thread per ray, 1 binned warp walk, 2 split walk
   int opt_seg = 64;     // split walk: target in-window steps per lane
-  int opt_fold = 2;     // 0 scalar sweep, 1 vector sweep, 2 flagged lines (registers), 3 staged
+  int opt_fold = 2;     // 0 scalar sweep, 1 vector sweep, flagged lines: 2 lists, 3 per warp
   int opt_block = 512;  // split walk CTA size
   int opt_contig = 0;   // split walk: contiguous segment runs per CTA
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)

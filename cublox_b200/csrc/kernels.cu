@@ -175,27 +175,34 @@ __global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
   }
 }
 
-// Fold of the flagged lines, staged in shared memory by asynchronous copies
-// (fold_lines_staged): 8 warps per CTA, each folding one contiguous run of
-// lines (a multiple of 32).
-constexpr int kStagedFoldWarps = 8;
-
+// Fold of the flagged lines through per-CTA line lists (fold.cuh,
+// build_line_list / fold_line_list): CTA b takes items of kListLines lines
+// b, b + grid, ... and loads the next item's flags before folding the
+// current list.
 template <bool kStats>
-__global__ void __launch_bounds__(32 * kStagedFoldWarps) fold_staged_kernel(const ApplyParams p) {
-  extern __shared__ __align__(128) unsigned char fsm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  LineStage *st = reinterpret_cast<LineStage *>(fsm) + 2 * warp;
+__global__ void __launch_bounds__(kListThreads, 4) fold_list_kernel(const ApplyParams p) {
+  __shared__ LineList L;
   const FoldView v = fold_view(p);
-  const int warps = gridDim.x * kStagedFoldWarps;
-  const int gw = blockIdx.x * kStagedFoldWarps + warp;
-  const int per = (((p.nlines + warps - 1) / warps) + 31) & ~31;
-  const int first = min(p.nlines, gw * per), end = min(p.nlines, first + per);
-  uint32_t touched = fold_lines_staged(v, p.dirty, first, end, st);
+  const int items = (p.nlines + kListLines - 1) / kListLines;
+  auto count_of = [&](int it) { return min(kListLines, p.nlines - it * kListLines); };
+  int it = blockIdx.x;
+  uint4 f = make_uint4(0u, 0u, 0u, 0u);
+  if (it < items) f = load_line_flags(p.dirty, it * kListLines, count_of(it));
+  uint32_t touched = 0;
+  for (; it < items; it += gridDim.x) {
+    const int start = it * kListLines;
+    const int n = build_line_list(line_flag_bits(f), L, p.dirty, start, count_of(it));
+    const int next = it + gridDim.x;
+    if (next < items) f = load_line_flags(p.dirty, next * kListLines, count_of(next));
+    touched += fold_line_list<4, false>(v, L, n, start);
+    __syncthreads();  // the list is rewritten next
+  }
   if (kStats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
       touched += __shfl_down_sync(0xffffffffu, touched, off);
-    if (lane == 0 && touched) atomicAdd(p.stats + 3, static_cast<unsigned long long>(touched));
+    if ((threadIdx.x & 31) == 0 && touched)
+      atomicAdd(p.stats + 3, static_cast<unsigned long long>(touched));
   }
 }
 
@@ -614,28 +621,18 @@ void launch_step_count(const RayParams &p, cudaStream_t s) {
 }
 
 void launch_apply(const ApplyParams &p, cudaStream_t s) {
-  if (p.variant == 3) {
+  if (p.variant == 2) {
     if (p.nlines <= 0) return;
-    static bool attr = false;
-    const size_t smem = kStagedFoldWarps * kStageWarpSmem;
-    if (!attr) {
-      cudaFuncSetAttribute(fold_staged_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
-      cudaFuncSetAttribute(fold_staged_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
-      attr = true;
-    }
-    const int groups = (p.nlines + 31) / 32;
-    int grid = (groups + kStagedFoldWarps * 16 - 1) / (kStagedFoldWarps * 16);  // >= 16 groups a warp
-    if (grid > sm_count()) grid = sm_count();
-    if (grid < 1) grid = 1;
+    int grid = (p.nlines + kListLines - 1) / kListLines;
+    const int cap = sm_count() * 4;
+    if (grid > cap) grid = cap;
     if (p.stats)
-      fold_staged_kernel<true><<<grid, 32 * kStagedFoldWarps, smem, s>>>(p);
+      fold_list_kernel<true><<<grid, kListThreads, 0, s>>>(p);
     else
-      fold_staged_kernel<false><<<grid, 32 * kStagedFoldWarps, smem, s>>>(p);
+      fold_list_kernel<false><<<grid, kListThreads, 0, s>>>(p);
     return;
   }
-  if (p.variant == 2) {
+  if (p.variant == 3) {
     if (p.nlines <= 0) return;
     const int groups = (p.nlines + 31) / 32;  // one warp per group of 32 lines
     int grid = (groups + 7) / 8;

@@ -79,7 +79,7 @@ struct ApplyParams {
   unsigned fp;
   unsigned long long *stats;  // [3] += touched
   int variant;                // 0 scalar sweep, 1 vector sweep, 2 flagged lines
-                              // (bulk-copy gather), 3 flagged lines (registers)
+                              // (per-CTA line lists), 3 flagged lines (per warp)
   uint8_t *dirty;             // variants 2, 3: line flags (cleared as folded)
   int nlines;                 // variants 2, 3: lines
   uint32_t *err;              // error word (a bounded wait that gave up)

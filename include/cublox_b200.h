@@ -113,9 +113,9 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 #define CUBLOX_OPT_SEGMENT 5 /* split walk: in-window steps per lane (64)   */
 #define CUBLOX_OPT_FOLD 6    /* fold: 0 scalar sweep of every counter, 1
                                 16-byte sweep; only the 32-voxel lines the
-                                scan flagged: 2 (default) through registers
-                                (8 lines in flight per warp), 3 staged in
-                                shared memory by asynchronous copies       */
+                                scan flagged: 2 (default) compacted into a
+                                list per 4096 lines, 3 read 32 flags at a
+                                time per warp                              */
 #define CUBLOX_OPT_BLOCK 7   /* split walk CTA size: 256, 512, 1024         */
 #define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
                                    consecutive segments (default 0: all
@@ -296,12 +296,12 @@ typedef struct cublox_batch cublox_batch;
 #define CUBLOX_BATCH_OPT_TIMING 4     /* record walk/fold device times      */
 #define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
 #define CUBLOX_BATCH_OPT_FOLD 6       /* fold: 0 (default) the 32-voxel
-                                         lines the walk flagged, through
-                                         registers; 1 every line
-                                         (the reference's full sweep, for
-                                         comparison); 2 the flagged lines
-                                         staged in shared memory by
-                                         asynchronous copies                */
+                                         lines the walk flagged, compacted
+                                         into a list per 4096 lines; 1 every
+                                         line (the reference's full sweep,
+                                         for comparison); 2 the flagged
+                                         lines, 32 flags at a time per
+                                         warp                               */
 #define CUBLOX_BATCH_OPT_LAYOUT 8     /* voxel layout the batch keeps its
                                          grids in (CUBLOX_OPT_LAYOUT codes;
                                          default 320); setting it stops
