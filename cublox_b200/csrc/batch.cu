@@ -457,6 +457,30 @@ __global__ void __launch_bounds__(kListThreads, 3) batch_fold_list_kernel(const 
   }
 }
 
+// Thread 0 of a CTA about to fold map m: waits until all of m's walk items
+// have finished (*done == n_walk), at most counters[5] sleep rounds.  Once
+// one wait of the launch gave up (counters[4]), the rest do not wait; a wait
+// that gives up sets the map's error word.  Returns 1 if the walks finished.
+__device__ __forceinline__ int wait_walks(const MapDesc &m, const int *done, int *counters) {
+  volatile const int *vd = done;
+  volatile int *gave_up = counters + 4;
+  int ok = 0;
+  const int limit = counters[5];
+  for (int k = 0; k < limit && !*gave_up; ++k) {
+    if (*vd >= m.n_walk) {
+      ok = 1;
+      break;
+    }
+    __nanosleep(256);
+  }
+  __threadfence();
+  if (!ok) {
+    *gave_up = 1;
+    atomicOr(m.ray.err, kErrWaitTimeout);
+  }
+  return ok;
+}
+
 // Walk and fold in one persistent launch.  Items come from one queue, in
 // the order the host wrote them: map 0's walk items, map 1's walk items,
 // map 0's fold items, map 2's walk items, map 1's fold items, ... (a fold
@@ -491,27 +515,49 @@ __global__ void __launch_bounds__(1024) batch_fused_kernel(const MapDesc *maps,
     } else {
       const FoldItem item{~raw.map, raw.start, raw.count, raw.pad};
       const MapDesc &m = maps[item.map];
-      if (threadIdx.x == 0) {
-        volatile int *vd = done + item.map;
-        volatile int *gave_up = counters + 4;
-        int ok = 0;
-        const int limit = counters[5];
-        for (int k = 0; k < limit && !*gave_up; ++k) {
-          if (*vd >= m.n_walk) {
-            ok = 1;
-            break;
-          }
-          __nanosleep(256);
-        }
-        __threadfence();
-        if (!ok) {
-          *gave_up = 1;
-          atomicOr(m.ray.err, kErrWaitTimeout);
-        }
-        s_ok = ok;
-      }
+      if (threadIdx.x == 0) s_ok = wait_walks(m, done + item.map, counters);
       __syncthreads();
       if (s_ok) add_touched(m, fold_item<true>(m, item));
+      __syncthreads();
+    }
+  }
+}
+
+// The fused launch with the flat cube: 512-thread CTAs, two per SM (as the
+// flat walk), folding through per-item line lists.  Items come in the order
+// the host wrote them, a map's fold items `lag` maps after its walk items
+// (the shape's `fused` value), and wait (bounded) as in batch_fused_kernel.
+template <int S>
+__global__ void __launch_bounds__(512, 2) batch_fused_flat_kernel(const MapDesc *maps,
+                                                                  const WalkItem *items,
+                                                                  const FoldItem * /*fold items*/,
+                                                                  int *counters, int *done) {
+  extern __shared__ uint32_t cube[];
+  __shared__ LineList L;
+  __shared__ int s_item, s_ok;
+  const int n_all = counters[1];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_all) break;
+    const WalkItem raw = items[it];
+    if (raw.map >= 0) {
+      walk_item<S, S / 2>(maps[raw.map], raw, cube);  // ends with a barrier
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(done + raw.map, 1);
+      }
+    } else {
+      const FoldItem item{~raw.map, raw.start, raw.count, raw.pad};
+      const MapDesc &m = maps[item.map];
+      if (threadIdx.x == 0) s_ok = wait_walks(m, done + item.map, counters);
+      __syncthreads();
+      if (s_ok) {
+        const uint4 f = load_line_flags<true>(m.ray.dirty, item.start, item.count);
+        const int n = build_line_list(line_flag_bits(f), L, m.ray.dirty, item.start, item.count);
+        add_touched(m, fold_line_list<2, true>(fold_view(m), L, n, item.start));
+      }
       __syncthreads();
     }
   }
@@ -521,7 +567,7 @@ struct Shape {
   int cube;      // 0, 16, 32
   int rays;      // rays per walk item; 0: about two items per resident CTA
   int block;     // walk (or fused) CTA size
-  int fused;     // 1: one launch, folds overlap later maps' walks
+  int fused;     // >= 1: one launch, a map's folds queued `fused` maps after its walks
   int min_ctas;  // 2: registers capped for two CTAs per SM (cube <= 16)
   int wq;        // 1: warps take 32-ray items of a CTA's current map (no item barriers)
   int refill;    // 1: two-phase items, lanes refilled from a far-state queue
@@ -533,7 +579,8 @@ const Shape kShapes[] = {{32, 512, 512, 0, 1, 0, 0},  {32, 1024, 1024, 0, 1, 0, 
                          {16, 0, 512, 0, 1, 1, 0},    {16, 1024, 1024, 0, 2, 0, 0},
                          {32, 1024, 1024, 1, 1, 0, 0}, {16, 512, 512, 1, 1, 0, 0},
                          {32, kRefillRays, 512, 0, 1, 0, 1}, {16, kRefillRays, 512, 0, 1, 0, 1},
-                         {32, 512, 512, 0, 2, 0, 0, 1},     {32, 256, 512, 0, 2, 0, 0, 1}};
+                         {32, 512, 512, 0, 2, 0, 0, 1},     {32, 256, 512, 0, 2, 0, 0, 1},
+                         {32, 512, 512, 2, 2, 0, 0, 1},     {32, 512, 512, 1, 2, 0, 0, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 // The tuner's candidates: every launch shape with the default voxel layout
@@ -545,7 +592,8 @@ struct Candidate {
 };
 const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320},
                                  {5, 320}, {6, 320}, {7, 320}, {8, 320}, {9, 320},
-                                 {10, 320}, {11, 320}, {10, 230}, {10, 221}, {10, 0}};
+                                 {10, 320}, {11, 320}, {12, 320}, {13, 320}, {10, 230},
+                                 {10, 221}, {10, 0}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {
@@ -561,6 +609,7 @@ int sm_count_batch() {
 
 template <int S>
 const void *shape_kernel_s(const Shape &sh) {
+  if (sh.flat && sh.fused) return reinterpret_cast<const void *>(batch_fused_flat_kernel<S>);
   if (sh.flat) return reinterpret_cast<const void *>(batch_walk_flat_kernel<S>);
   if (sh.refill) return reinterpret_cast<const void *>(batch_walk_refill_kernel<S>);
   if (sh.fused) return reinterpret_cast<const void *>(batch_fused_kernel<S>);
@@ -673,6 +722,7 @@ struct cublox_batch {
   int tune_step = 0;
   int tune_rounds = 2;
   std::vector<float> tune_ms;
+  std::vector<WalkItem> order;  // fused launch: the queue in launch order (capacity kept)
   bool graphs = false;
   int fold_variant = 0;
   cudaGraphExec_t graph = nullptr;
@@ -1022,28 +1072,25 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
     ++d;
   }
   if (sh.fused) {
-    // walk(0) walk(1) fold(0) walk(2) fold(1) ... fold(d-1), written after
-    // the walk items, then moved to the front
-    const int n_walk = w;
+    // with lag L = sh.fused: walk(0) .. walk(L) fold(0) walk(L + 1) fold(1)
+    // ... walk(d - 1) fold(d - 1 - L) .. fold(d - 1)
+    const int lag = sh.fused;
+    auto &order = b->order;
+    order.clear();
+    auto put_walk = [&](int map) {
+      for (int i = map ? w_end[map - 1] : 0; i < w_end[map]; ++i) order.push_back(b->h_witems[i]);
+    };
     auto put_fold = [&](int map) {
       for (int i = map ? f_end[map - 1] : 0; i < f_end[map]; ++i) {
         const FoldItem &fi = b->h_fitems[i];
-        b->h_witems[w++] = WalkItem{~fi.map, fi.start, fi.count, fi.pad};
+        order.push_back(WalkItem{~fi.map, fi.start, fi.count, fi.pad});
       }
     };
-    std::vector<WalkItem> order;
-    order.reserve(static_cast<size_t>(n_walk + f));
     for (int map = 0; map < d; ++map) {
-      for (int i = map ? w_end[map - 1] : 0; i < w_end[map]; ++i) order.push_back(b->h_witems[i]);
-      if (map >= 1) {
-        w = n_walk;
-        put_fold(map - 1);
-        order.insert(order.end(), b->h_witems + n_walk, b->h_witems + w);
-      }
+      put_walk(map);
+      if (map >= lag) put_fold(map - lag);
     }
-    w = n_walk;
-    put_fold(d - 1);
-    order.insert(order.end(), b->h_witems + n_walk, b->h_witems + w);
+    for (int map = std::max(0, d - lag); map < d; ++map) put_fold(map);
     std::copy(order.begin(), order.end(), b->h_witems);
     w = static_cast<int>(order.size());
     f = 0;

@@ -145,33 +145,40 @@ __device__ __forceinline__ uint32_t fold_lines(const FoldView &v, uint8_t *dirty
 // The per-warp fold above reads 32 flags, then folds only the flagged ones
 // among them: about 9 of 32 lines at README scale, so a warp rarely has more
 // than one batch of lines in flight and waits a full memory latency on every
-// flag group.  Here a 256-thread CTA takes 4096 lines at a time: one 16-byte
-// flag load per thread, a CTA-wide prefix sum turns the flagged lines into a
+// flag group.  Here a CTA (256 threads or more) takes up to 4096 lines at a
+// time: one 16-byte flag load for each of its first 256 threads, a CTA-wide
+// prefix sum turns the flagged lines into a
 // dense list in shared memory (flags cleared on the way), and the warps then
 // fold the list four lines per warp access (8 lanes x 16 bytes a line) with
 // kQuads accesses in flight per warp, so every warp has 4 kQuads lines in
 // flight until the list runs out.  The next item's flags are loaded before
 // the current list is folded.
 
-constexpr int kListThreads = 256;
+constexpr int kListThreads = 256;              // CTA size of the fold-only kernels
 constexpr int kListLines = 16 * kListThreads;  // lines per item: 16 flags per thread
-constexpr int kListWarps = kListThreads / 32;
 
 struct LineList {
   uint16_t line[kListLines];  // flagged lines, relative to the item's first line
-  int warp_sum[kListWarps];
+  int warp_sum[32];
 };
 
 // The raw flags of this thread's lines start + 16 t .. + 15 (bytes of lines
 // at or beyond `count` read as zero); `dirty + start` is 16-byte aligned.
 // The value is used only by line_flag_bits, so the load can stay in flight
-// across other work.
+// across other work.  kL2: read at L2 (ld.global.cg), as flags that other
+// CTAs of the same launch wrote need.
+template <bool kL2 = false>
 __device__ __forceinline__ uint4 load_line_flags(const uint8_t *dirty, int start, int count) {
   const int i = 16 * static_cast<int>(threadIdx.x);
-  if (i + 16 <= count) return *reinterpret_cast<const uint4 *>(dirty + start + i);
+  if (i + 16 <= count) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(dirty + start + i);
+    return kL2 ? __ldcg(q) : *q;
+  }
   uint32_t w[4] = {0u, 0u, 0u, 0u};
-  for (int j = 0; i + j < count && j < 16; ++j)
-    w[j >> 2] |= static_cast<uint32_t>(dirty[start + i + j] != 0) << (8 * (j & 3));
+  for (int j = 0; i + j < count && j < 16; ++j) {
+    const uint8_t d = kL2 ? __ldcg(dirty + start + i + j) : dirty[start + i + j];
+    w[j >> 2] |= static_cast<uint32_t>(d != 0) << (8 * (j & 3));
+  }
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
@@ -203,8 +210,8 @@ __device__ __forceinline__ int build_line_list(uint32_t m, LineList &L, uint8_t 
   if (lane == 31) L.warp_sum[warp] = incl;
   __syncthreads();
   int pos = incl - c, total = 0;
-#pragma unroll
-  for (int w = 0; w < kListWarps; ++w) {
+  const int warps = blockDim.x >> 5;
+  for (int w = 0; w < warps; ++w) {
     const int s = L.warp_sum[w];
     pos += w < warp ? s : 0;
     total += s;
@@ -222,25 +229,25 @@ __device__ __forceinline__ int build_line_list(uint32_t m, LineList &L, uint8_t 
 }
 
 // Fold of the CTA's list of n lines (item's first line `start`).  Warp w
-// takes line quads w, w + kListWarps, ...; lane (q, s) = (lane / 8, lane % 8)
+// of W takes line quads w, w + W, ...; lane (q, s) = (lane / 8, lane % 8)
 // handles 16-byte piece s of the quad's line q.  A piece whose counters are
 // all zero is left as it is (its values do not change, its counters are
 // zero already).  kL2: counters are read at L2.  Returns the voxels folded.
 template <int kQuads, bool kL2>
 __device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const LineList &L, int n,
                                                    int start) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   const int q = lane >> 3, sub = lane & 7;
   const uint4 *c4r = reinterpret_cast<const uint4 *>(v.cnt);
   uint4 *c4 = reinterpret_cast<uint4 *>(v.cnt);
   float4 *o4 = reinterpret_cast<float4 *>(v.occ);
   uint32_t touched = 0;
   const int quads = (n + 3) >> 2;
-  for (int i0 = warp; i0 < quads; i0 += kQuads * kListWarps) {
+  for (int i0 = warp; i0 < quads; i0 += kQuads * warps) {
     int at[kQuads];
 #pragma unroll
     for (int u = 0; u < kQuads; ++u) {
-      const int k = 4 * (i0 + u * kListWarps) + q;
+      const int k = 4 * (i0 + u * warps) + q;
       at[u] = k < n ? ((start + L.line[k]) << 3) + sub : -1;  // index of the 16-byte piece
     }
     uint4 c[kQuads];

@@ -102,7 +102,7 @@ def test_batch_matches_solo_updates_through_tuning(graphs):
 def test_every_layout_gives_the_same_maps(layout):
     w = small_workload(n_maps=4, n_steps=4, seed=8)
     b = C.Batch()
-    b.set_option(C.BATCH_OPT_SHAPE, 6)  # fused: folds read flags other CTAs wrote
+    b.set_option(C.BATCH_OPT_SHAPE, 12)  # fused: folds read flags other CTAs wrote
     b.set_option(C.BATCH_OPT_LAYOUT, layout)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
     bg, solo = setup(w, b)
@@ -111,7 +111,8 @@ def test_every_layout_gives_the_same_maps(layout):
     b.close()
 
 
-def test_fused_wait_runs_out_and_the_context_stays_usable():
+@pytest.mark.parametrize("shape", [6, 12])
+def test_fused_wait_runs_out_and_the_context_stays_usable(shape):
     """A fused launch whose first map's folds wait for a walk item that
     does not exist (the test hook): the bounded wait (shortened here to
     about a millisecond) gives up, the launch ends, the map's error word
@@ -119,7 +120,7 @@ def test_fused_wait_runs_out_and_the_context_stays_usable():
     reset, integrates correctly again."""
     w = small_workload(n_maps=3, n_steps=3, seed=10)
     b = C.Batch()
-    b.set_option(C.BATCH_OPT_SHAPE, 6)
+    b.set_option(C.BATCH_OPT_SHAPE, shape)
     b.set_option(C.BATCH_OPT_WAIT_LIMIT, 4000)
     b.set_option(C.BATCH_OPT_INJECT_MISSING_WALK, 1)
     bg, solo = setup(w, b)
@@ -136,11 +137,11 @@ def test_fused_wait_runs_out_and_the_context_stays_usable():
     b.close()
 
 
-@pytest.mark.parametrize("shape", range(12))
+@pytest.mark.parametrize("shape", range(14))
 def test_every_shape_gives_the_same_maps(shape):
     w = small_workload(n_maps=4, n_steps=3, seed=7)
     b = C.Batch()
-    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 12
+    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 14
     b.set_option(C.BATCH_OPT_SHAPE, shape)
     b.set_option(C.BATCH_OPT_FOLD, shape % 3)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
