@@ -592,8 +592,7 @@ struct Candidate {
 };
 const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320},
                                  {5, 320}, {6, 320}, {7, 320}, {8, 320}, {9, 320},
-                                 {10, 320}, {11, 320}, {12, 320}, {13, 320}, {10, 230},
-                                 {10, 221}, {10, 0}};
+                                 {10, 320}, {11, 320}, {10, 230}, {10, 221}, {10, 0}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {
