@@ -90,8 +90,9 @@ __device__ __forceinline__ bool walk_near(const RayParams &p, uint32_t *cube, co
   }
 }
 
-// One walk item: zero the cube, walk the item's rays (one thread per ray),
-// flush the cube into the map's counters.  Ends with a CTA barrier.
+// One walk item: zero the cube, walk the item's rays (one thread per ray,
+// in order of their estimated length when the item fits the CTA), flush the
+// cube into the map's counters.  Ends with a CTA barrier.
 template <int S, int SZ = S>
 __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &item,
                                           uint32_t *cube) {
@@ -100,9 +101,15 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
   const int clo[3] = {md.clo[0], md.clo[1], md.clo[2]};
   for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
     reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
-  __syncthreads();
+  __shared__ RayOrder order;
+  const bool ordered = item.count <= static_cast<int>(blockDim.x) && item.count <= kOrderCap;
+  if (ordered)
+    order_rays(p, item.start, item.count, order);  // ends with a barrier
+  else
+    __syncthreads();
   uint32_t rays = 0, incs = 0, hits = 0;
-  for (int i = item.start + threadIdx.x; i < item.start + item.count; i += blockDim.x) {
+  for (int j = threadIdx.x; j < item.count; j += blockDim.x) {
+    const int i = item.start + (ordered ? order.idx[j] : j);
     const size_t k = static_cast<size_t>(i) * p.stride;
     RayWalk w;
     if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;

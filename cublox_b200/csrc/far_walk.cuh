@@ -189,4 +189,71 @@ __device__ __forceinline__ bool walk_far(const RayParams &p, FarWalk &f, int bud
   incs += static_cast<uint32_t>(done);
   return f.left == 0 || (f.e[0] | f.e[1] | f.e[2]) == 0;
 }
+// ---- rays of an item ordered by length ----
+// A warp runs until its longest ray ends, and rays of one azimuth column of
+// a spinning LiDAR differ several-fold in how far they walk (beams that
+// hit the ground near the sensor, beams that leave the window's top, beams
+// clipped at max range).  A CTA therefore walks its item's rays in order of
+// an estimate of their loop length (a counting sort on kOrderBins bins of
+// kOrderStep iterations), so that the lanes of a warp end at about the same
+// time.  Counts are sums of integer increments, so the order changes no
+// result; the estimate only has to be cheap.
+
+constexpr int kOrderBins = 32;
+constexpr int kOrderStep = 32;   // loop iterations per bin
+constexpr int kOrderCap = 1024;  // rays per item the CTA orders
+
+struct RayOrder {
+  uint16_t idx[kOrderCap];  // the item's rays, shortest estimate first
+  int base[kOrderBins];
+};
+
+// Estimated loop iterations of the ray to (x, y, z): the L1 length in voxels
+// of its segment, clipped at max range and at the window's box.
+__device__ __forceinline__ int ray_len_estimate(const RayParams &p, float x, float y, float z) {
+  const float d[3] = {x - p.o[0], y - p.o[1], z - p.o[2]};
+  const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  if (!(r2 < 1e30f)) return 0;  // non-finite: the walk drops the ray at once
+  float t = 1.0f;
+  if (r2 > p.max_range * p.max_range) t = p.max_range * rsqrtf(r2);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = static_cast<float>(p.win[a] - p.half[a]) * p.res;
+    const float hi = static_cast<float>(p.win[a] + p.half[a] + 1) * p.res;
+    if (d[a] > 0.0f) t = fminf(t, fmaxf(0.0f, (hi - p.o[a]) / d[a]));
+    if (d[a] < 0.0f) t = fminf(t, fmaxf(0.0f, (lo - p.o[a]) / d[a]));
+  }
+  const float l1 = (fabsf(d[0]) + fabsf(d[1]) + fabsf(d[2])) * t * p.inv;
+  return l1 < 1e9f ? static_cast<int>(l1) : 1 << 30;
+}
+
+// Fills `o` with the order of the item's rays start .. start + count - 1
+// (count <= min(blockDim.x, kOrderCap)): thread j's ray is o.idx[j].
+// Contains CTA barriers; every thread of the CTA calls it.
+__device__ __forceinline__ void order_rays(const RayParams &p, int start, int count, RayOrder &o) {
+  const int t = threadIdx.x;
+  if (t < kOrderBins) o.base[t] = 0;
+  __syncthreads();
+  int bin = 0, slot = 0;
+  if (t < count) {
+    const size_t k = static_cast<size_t>(start + t) * p.stride;
+    bin = min(kOrderBins - 1, ray_len_estimate(p, p.x[k], p.y[k], p.z[k]) / kOrderStep);
+    slot = atomicAdd(&o.base[bin], 1);
+  }
+  __syncthreads();
+  if (t < 32) {  // exclusive prefix sum of the bin sizes
+    const int c = o.base[t];
+    int incl = c;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, s);
+      if (t >= s) incl += v;
+    }
+    o.base[t] = incl - c;
+  }
+  __syncthreads();
+  if (t < count) o.idx[o.base[bin] + slot] = static_cast<uint16_t>(t);
+  __syncthreads();
+}
+
 }  // namespace cublox_b200
