@@ -90,9 +90,10 @@ __device__ __forceinline__ bool walk_near(const RayParams &p, uint32_t *cube, co
   }
 }
 
-// One walk item: zero the cube, walk the item's rays (one thread per ray,
-// in order of their estimated length when the item fits the CTA), flush the
-// cube into the map's counters.  Ends with a CTA barrier.
+// One walk item: zero the cube, walk the item's rays (in order of their
+// estimated length when the item has at most twice as many rays as the CTA
+// has threads), flush the cube into the map's counters.  Ends with a CTA
+// barrier.
 template <int S, int SZ = S>
 __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &item,
                                           uint32_t *cube) {
@@ -102,22 +103,31 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
   for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
     reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
   __shared__ RayOrder order;
-  const bool ordered = item.count <= static_cast<int>(blockDim.x) && item.count <= kOrderCap;
+  const int t = threadIdx.x, nt = blockDim.x;
+  const bool ordered = item.count <= 2 * nt && item.count <= kOrderCap;
   if (ordered)
     order_rays(p, item.start, item.count, order);  // ends with a barrier
   else
     __syncthreads();
   uint32_t rays = 0, incs = 0, hits = 0;
-  for (int j = threadIdx.x; j < item.count; j += blockDim.x) {
-    const int i = item.start + (ordered ? order.idx[j] : j);
+  auto walk_ray = [&](int i) {
     const size_t k = static_cast<size_t>(i) * p.stride;
     RayWalk w;
-    if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) continue;
+    if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) return;
     ++rays;
     const RayEnd re = ray_end_of<S, SZ>(p, w, clo);
     FarWalk f;
     if (!walk_near<S, SZ>(p, cube, clo, w, f, incs)) walk_far(p, f, f.left, incs);
     apply_end<S>(p, cube, re, incs, hits);
+  };
+  if (ordered) {
+    // thread t walks the t-th shortest ray, then (items of more rays than
+    // threads) the t-th longest: every thread gets about the same work
+    if (t < item.count) walk_ray(item.start + order.idx[t]);
+    const int j = item.count - 1 - t;
+    if (j >= nt) walk_ray(item.start + order.idx[j]);
+  } else {
+    for (int j = t; j < item.count; j += nt) walk_ray(item.start + j);
   }
   __syncthreads();
   flush_cube<S, SZ>(p, cube, clo);
@@ -433,9 +443,9 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const MapDesc *maps,
 // Persistent fold over per-item lists of the flagged lines (fold.cuh,
 // build_line_list / fold_line_list): CTAs take fold items from counters[2]
 // and load the next item's flags before folding the current list.
-__global__ void __launch_bounds__(kListThreads, 3) batch_fold_list_kernel(const MapDesc *maps,
-                                                                          const FoldItem *items,
-                                                                          int *counters) {
+template <int kQuads, int kMinCtas>
+__global__ void __launch_bounds__(kListThreads, kMinCtas) batch_fold_list_kernel(
+    const MapDesc *maps, const FoldItem *items, int *counters) {
   __shared__ LineList L;
   __shared__ int s_item;
   const int n_items = counters[3];
@@ -458,7 +468,7 @@ __global__ void __launch_bounds__(kListThreads, 3) batch_fold_list_kernel(const 
       const FoldItem fi = items[next];
       f = load_line_flags(maps[fi.map].ray.dirty, fi.start, fi.count);
     }
-    add_touched(m, fold_line_list<4, false>(fold_view(m), L, n, item.start));
+    add_touched(m, fold_line_list<kQuads, false>(fold_view(m), L, n, item.start));
     __syncthreads();  // the list and s_item are rewritten next
     it = next;
   }
@@ -587,7 +597,8 @@ const Shape kShapes[] = {{32, 512, 512, 0, 1, 0, 0},  {32, 1024, 1024, 0, 1, 0, 
                          {32, 1024, 1024, 1, 1, 0, 0}, {16, 512, 512, 1, 1, 0, 0},
                          {32, kRefillRays, 512, 0, 1, 0, 1}, {16, kRefillRays, 512, 0, 1, 0, 1},
                          {32, 512, 512, 0, 2, 0, 0, 1},     {32, 256, 512, 0, 2, 0, 0, 1},
-                         {32, 512, 512, 2, 2, 0, 0, 1},     {32, 512, 512, 1, 2, 0, 0, 1}};
+                         {32, 512, 512, 2, 2, 0, 0, 1},     {32, 512, 512, 1, 2, 0, 0, 1},
+                         {32, 1024, 512, 0, 2, 0, 0, 1},    {32, 768, 512, 0, 2, 0, 0, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 // The tuner's candidates: every launch shape with the default voxel layout
@@ -685,7 +696,13 @@ cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counte
                         int variant, cudaStream_t s) {
   const dim3 grid(sm_count_batch() * 8), block(256);
   if (variant == 0) {
-    batch_fold_list_kernel<<<sm_count_batch() * 3, kListThreads, 0, s>>>(maps, fitems, counters);
+    batch_fold_list_kernel<4, 3><<<sm_count_batch() * 3, kListThreads, 0, s>>>(maps, fitems, counters);
+  } else if (variant == 3) {
+    batch_fold_list_kernel<2, 4><<<sm_count_batch() * 4, kListThreads, 0, s>>>(maps, fitems, counters);
+  } else if (variant == 4) {
+    batch_fold_list_kernel<8, 2><<<sm_count_batch() * 2, kListThreads, 0, s>>>(maps, fitems, counters);
+  } else if (variant == 5) {
+    batch_fold_list_kernel<4, 4><<<sm_count_batch() * 4, kListThreads, 0, s>>>(maps, fitems, counters);
   } else if (variant == 1) {
     batch_fold_kernel<true><<<grid, block, 0, s>>>(maps, fitems, counters);
   } else {
@@ -947,7 +964,7 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
       b->timed = value != 0;
       return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD:
-      if (value < 0 || value > 2) break;
+      if (value < 0 || value > 5) break;
       b->fold_variant = value;
       drop_graph(b);
       return CUBLOX_OK;

@@ -228,17 +228,21 @@ __device__ __forceinline__ int ray_len_estimate(const RayParams &p, float x, flo
 }
 
 // Fills `o` with the order of the item's rays start .. start + count - 1
-// (count <= min(blockDim.x, kOrderCap)): thread j's ray is o.idx[j].
+// (count <= min(2 blockDim.x, kOrderCap)): o.idx[j] is the j-th shortest.
 // Contains CTA barriers; every thread of the CTA calls it.
 __device__ __forceinline__ void order_rays(const RayParams &p, int start, int count, RayOrder &o) {
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, nt = blockDim.x;
   if (t < kOrderBins) o.base[t] = 0;
   __syncthreads();
-  int bin = 0, slot = 0;
-  if (t < count) {
-    const size_t k = static_cast<size_t>(start + t) * p.stride;
-    bin = min(kOrderBins - 1, ray_len_estimate(p, p.x[k], p.y[k], p.z[k]) / kOrderStep);
-    slot = atomicAdd(&o.base[bin], 1);
+  int bin[2] = {0, 0}, slot[2] = {0, 0};
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int j = t + r * nt;
+    if (j < count) {
+      const size_t k = static_cast<size_t>(start + j) * p.stride;
+      bin[r] = min(kOrderBins - 1, ray_len_estimate(p, p.x[k], p.y[k], p.z[k]) / kOrderStep);
+      slot[r] = atomicAdd(&o.base[bin[r]], 1);
+    }
   }
   __syncthreads();
   if (t < 32) {  // exclusive prefix sum of the bin sizes
@@ -252,7 +256,11 @@ __device__ __forceinline__ void order_rays(const RayParams &p, int start, int co
     o.base[t] = incl - c;
   }
   __syncthreads();
-  if (t < count) o.idx[o.base[bin] + slot] = static_cast<uint16_t>(t);
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int j = t + r * nt;
+    if (j < count) o.idx[o.base[bin[r]] + slot[r]] = static_cast<uint16_t>(j);
+  }
   __syncthreads();
 }
 

@@ -137,11 +137,11 @@ def test_fused_wait_runs_out_and_the_context_stays_usable(shape):
     b.close()
 
 
-@pytest.mark.parametrize("shape", range(14))
+@pytest.mark.parametrize("shape", range(16))
 def test_every_shape_gives_the_same_maps(shape):
     w = small_workload(n_maps=4, n_steps=3, seed=7)
     b = C.Batch()
-    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 14
+    assert b.get_option(C.BATCH_OPT_NUM_SHAPES) == 16
     b.set_option(C.BATCH_OPT_SHAPE, shape)
     b.set_option(C.BATCH_OPT_FOLD, shape % 3)
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
