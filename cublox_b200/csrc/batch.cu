@@ -110,24 +110,41 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
   else
     __syncthreads();
   uint32_t rays = 0, incs = 0, hits = 0;
-  auto walk_ray = [&](int i) {
-    const size_t k = static_cast<size_t>(i) * p.stride;
-    RayWalk w;
-    if (!ray_begin(p, p.x[k], p.y[k], p.z[k], w)) return;
-    ++rays;
-    const RayEnd re = ray_end_of<S, SZ>(p, w, clo);
+  // Ordered: thread t walks the t-th shortest ray, then (items of more rays
+  // than threads) the t-th longest, so every thread gets about the same
+  // work.  Every lane runs every round (live or not) and the warp meets
+  // after the near phase, so that its lanes walk their far phases together
+  // rather than in groups that entered the far loop at different times.
+  const int rounds = ordered ? (item.count > nt ? 2 : 1) : (item.count + nt - 1) / nt;
+#pragma unroll 1
+  for (int r = 0; r < rounds; ++r) {
+    int j;
+    bool live;
+    if (ordered) {
+      j = r ? item.count - 1 - t : t;
+      live = r ? j >= nt : j < item.count;
+      j = live ? order.idx[j] : 0;
+    } else {
+      j = r * nt + t;
+      live = j < item.count;
+    }
     FarWalk f;
-    if (!walk_near<S, SZ>(p, cube, clo, w, f, incs)) walk_far(p, f, f.left, incs);
-    apply_end<S>(p, cube, re, incs, hits);
-  };
-  if (ordered) {
-    // thread t walks the t-th shortest ray, then (items of more rays than
-    // threads) the t-th longest: every thread gets about the same work
-    if (t < item.count) walk_ray(item.start + order.idx[t]);
-    const int j = item.count - 1 - t;
-    if (j >= nt) walk_ray(item.start + order.idx[j]);
-  } else {
-    for (int j = t; j < item.count; j += nt) walk_ray(item.start + j);
+    RayEnd re{-1, -1, false};
+    bool far = false;
+    if (live) {
+      const size_t k = static_cast<size_t>(item.start + j) * p.stride;
+      RayWalk w;
+      if (ray_begin(p, p.x[k], p.y[k], p.z[k], w)) {
+        ++rays;
+        re = ray_end_of<S, SZ>(p, w, clo);
+        far = !walk_near<S, SZ>(p, cube, clo, w, f, incs);
+      } else {
+        live = false;
+      }
+    }
+    __syncwarp();
+    if (far) walk_far(p, f, f.left, incs);
+    if (live) apply_end<S>(p, cube, re, incs, hits);
   }
   __syncthreads();
   flush_cube<S, SZ>(p, cube, clo);
