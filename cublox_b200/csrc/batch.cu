@@ -464,9 +464,13 @@ template <int kQuads, int kMinCtas>
 __global__ void __launch_bounds__(kListThreads, kMinCtas) batch_fold_list_kernel(
     const MapDesc *maps, const FoldItem *items, int *counters) {
   __shared__ LineList L;
+  __shared__ HitQueue hq;
   __shared__ int s_item;
   const int n_items = counters[3];
-  if (threadIdx.x == 0) s_item = atomicAdd(&counters[2], 1);
+  if (threadIdx.x == 0) {
+    s_item = atomicAdd(&counters[2], 1);
+    hq.n = 0;
+  }
   __syncthreads();
   int it = s_item;
   uint4 f = make_uint4(0u, 0u, 0u, 0u);
@@ -485,8 +489,10 @@ __global__ void __launch_bounds__(kListThreads, kMinCtas) batch_fold_list_kernel
       const FoldItem fi = items[next];
       f = load_line_flags(maps[fi.map].ray.dirty, fi.start, fi.count);
     }
-    add_touched(m, fold_line_list<kQuads, false>(fold_view(m), L, n, item.start));
-    __syncthreads();  // the list and s_item are rewritten next
+    const FoldView v = fold_view(m);
+    add_touched(m, fold_line_list<kQuads, false>(v, L, n, item.start, &hq));
+    __syncthreads();
+    fold_hit_queue(v, hq);  // ends with a barrier: the list and s_item are rewritten next
     it = next;
   }
 }
@@ -568,7 +574,9 @@ __global__ void __launch_bounds__(512, 2) batch_fused_flat_kernel(const MapDesc 
                                                                   int *counters, int *done) {
   extern __shared__ uint32_t cube[];
   __shared__ LineList L;
+  __shared__ HitQueue hq;
   __shared__ int s_item, s_ok;
+  if (threadIdx.x == 0) hq.n = 0;
   const int n_all = counters[1];
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1);
@@ -590,7 +598,10 @@ __global__ void __launch_bounds__(512, 2) batch_fused_flat_kernel(const MapDesc 
       if (s_ok) {
         const uint4 f = load_line_flags<true>(m.ray.dirty, item.start, item.count);
         const int n = build_line_list(line_flag_bits(f), L, m.ray.dirty, item.start, item.count);
-        add_touched(m, fold_line_list<2, true>(fold_view(m), L, n, item.start));
+        const FoldView v = fold_view(m);
+        add_touched(m, fold_line_list<2, true>(v, L, n, item.start, &hq));
+        __syncthreads();
+        fold_hit_queue(v, hq);
       }
       __syncthreads();
     }
@@ -618,16 +629,18 @@ const Shape kShapes[] = {{32, 512, 512, 0, 1, 0, 0},  {32, 1024, 1024, 0, 1, 0, 
                          {32, 1024, 512, 0, 2, 0, 0, 1},    {32, 768, 512, 0, 2, 0, 0, 1}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
-// The tuner's candidates: every launch shape with the default voxel layout
-// (8 x 4 x 1 bricks), then the flat-cube shape with the other layouts (4 x
-// 8 x 1 and 4 x 4 x 2 bricks, the reference's hash order).  A candidate with
-// another layout moves every grid of the update to it first.
+// The tuner's candidates: the launch shapes that have been fastest on some
+// workload, with the default voxel layout (8 x 4 x 1 bricks), then the two
+// fastest walk shapes with the other layouts (4 x 8 x 1 and 4 x 4 x 2
+// bricks, the reference's hash order).  Shapes 3, 4, 5, 8, 9 and 13 stay
+// selectable.  A candidate with another layout moves every grid of the
+// update to it first.
 struct Candidate {
   int shape, layout;
 };
-const Candidate kCandidates[] = {{0, 320}, {1, 320}, {2, 320}, {3, 320}, {4, 320},
-                                 {5, 320}, {6, 320}, {7, 320}, {8, 320}, {9, 320},
-                                 {10, 320}, {11, 320}, {10, 230}, {10, 221}, {10, 0}};
+const Candidate kCandidates[] = {{0, 320},  {1, 320},  {2, 320},  {6, 320},  {7, 320},
+                                 {10, 320}, {11, 320}, {12, 320}, {14, 320}, {15, 320},
+                                 {1, 230},  {10, 230}, {1, 221},  {10, 221}, {1, 0}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 int sm_count_batch() {

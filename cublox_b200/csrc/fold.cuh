@@ -228,14 +228,46 @@ __device__ __forceinline__ int build_line_list(uint32_t m, LineList &L, uint8_t 
   return total;
 }
 
+// Voxels with a hit whose fold waits for the end of the item.  Their hit
+// count lives in a second array; loaded where the voxel is met, it would
+// stall the warp's whole batch of lines for one more memory round trip
+// (most batches hold a hit voxel), so they are queued in shared memory
+// and folded together once the list is done, every hit load in flight at
+// once.  A full queue folds further hits where they are met.
+constexpr int kHitCap = 1024;
+
+struct HitQueue {
+  int n;                 // voxels queued (may pass kHitCap: the rest were folded in place)
+  int h[kHitCap];        // address
+  uint32_t c[kHitCap];   // counter word
+};
+
+// Folds voxel h (counter word c, stored value o) now, or queues it if it has
+// a hit and the queue has room (its stored value is then written back
+// unchanged by the caller and replaced by fold_hit_queue).
+__device__ __forceinline__ float fold_or_queue(const FoldView &v, HitQueue *hq, int h, uint32_t c,
+                                               float o) {
+  if (hq && (c & kHitFlag)) {
+    const int slot = atomicAdd(&hq->n, 1);
+    if (slot < kHitCap) {
+      hq->h[slot] = h;
+      hq->c[slot] = c;
+      return o;
+    }
+  }
+  return fold_counter(v, h, c, o);
+}
+
 // Fold of the CTA's list of n lines (item's first line `start`).  Warp w
 // of W takes line quads w, w + W, ...; lane (q, s) = (lane / 8, lane % 8)
 // handles 16-byte piece s of the quad's line q.  A piece whose counters are
 // all zero is left as it is (its values do not change, its counters are
-// zero already).  kL2: counters are read at L2.  Returns the voxels folded.
+// zero already).  Hit voxels go to `hq` when it is given (fold_hit_queue
+// folds them after a CTA barrier).  kL2: counters are read at L2.  Returns
+// the voxels folded or queued.
 template <int kQuads, bool kL2>
 __device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const LineList &L, int n,
-                                                   int start) {
+                                                   int start, HitQueue *hq = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   const int q = lane >> 3, sub = lane & 7;
   const uint4 *c4r = reinterpret_cast<const uint4 *>(v.cnt);
@@ -262,15 +294,28 @@ __device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const Line
     for (int u = 0; u < kQuads; ++u) {
       if (at[u] < 0 || !any_set(c[u])) continue;
       const int h = at[u] << 2;
-      if (c[u].x) { o[u].x = fold_counter(v, h + 0, c[u].x, o[u].x); ++touched; }
-      if (c[u].y) { o[u].y = fold_counter(v, h + 1, c[u].y, o[u].y); ++touched; }
-      if (c[u].z) { o[u].z = fold_counter(v, h + 2, c[u].z, o[u].z); ++touched; }
-      if (c[u].w) { o[u].w = fold_counter(v, h + 3, c[u].w, o[u].w); ++touched; }
+      if (c[u].x) { o[u].x = fold_or_queue(v, hq, h + 0, c[u].x, o[u].x); ++touched; }
+      if (c[u].y) { o[u].y = fold_or_queue(v, hq, h + 1, c[u].y, o[u].y); ++touched; }
+      if (c[u].z) { o[u].z = fold_or_queue(v, hq, h + 2, c[u].z, o[u].z); ++touched; }
+      if (c[u].w) { o[u].w = fold_or_queue(v, hq, h + 3, c[u].w, o[u].w); ++touched; }
       o4[at[u]] = o[u];
       c4[at[u]] = make_uint4(0u, 0u, 0u, 0u);
     }
   }
   return touched;
+}
+
+// Folds the queued hit voxels (after a CTA barrier that follows every
+// fold_line_list of the item) and empties the queue; ends with a CTA
+// barrier.  The stored value is read back: the list fold wrote it unchanged.
+__device__ __forceinline__ void fold_hit_queue(const FoldView &v, HitQueue &hq) {
+  const int n = min(hq.n, kHitCap);
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int h = hq.h[e];
+    v.occ[h] = fold_counter(v, h, hq.c[e], v.occ[h]);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) hq.n = 0;
 }
 
 // The vnum % 4 voxels after the last whole group, one per thread 0..2.

@@ -182,6 +182,8 @@ __global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
 template <bool kStats>
 __global__ void __launch_bounds__(kListThreads, 4) fold_list_kernel(const ApplyParams p) {
   __shared__ LineList L;
+  __shared__ HitQueue hq;
+  if (threadIdx.x == 0) hq.n = 0;  // the first read follows build_line_list's barriers
   const FoldView v = fold_view(p);
   const int items = (p.nlines + kListLines - 1) / kListLines;
   auto count_of = [&](int it) { return min(kListLines, p.nlines - it * kListLines); };
@@ -194,8 +196,9 @@ __global__ void __launch_bounds__(kListThreads, 4) fold_list_kernel(const ApplyP
     const int n = build_line_list(line_flag_bits(f), L, p.dirty, start, count_of(it));
     const int next = it + gridDim.x;
     if (next < items) f = load_line_flags(p.dirty, next * kListLines, count_of(next));
-    touched += fold_line_list<4, false>(v, L, n, start);
-    __syncthreads();  // the list is rewritten next
+    touched += fold_line_list<4, false>(v, L, n, start, &hq);
+    __syncthreads();
+    fold_hit_queue(v, hq);  // ends with a barrier: the list is rewritten next
   }
   if (kStats) {
 #pragma unroll
