@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(kListThreads, kMinCtas) batch_fold_list_kernel
       f = load_line_flags(maps[fi.map].ray.dirty, fi.start, fi.count);
     }
     const FoldView v = fold_view(m);
-    add_touched(m, fold_line_list<kQuads, false>(v, L, n, item.start, &hq));
+    add_touched(m, fold_line_list<kQuads, false>(v, L.line, n, item.start, &hq));
     __syncthreads();
     fold_hit_queue(v, hq);  // ends with a barrier: the list and s_item are rewritten next
     it = next;
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(512, 2) batch_fused_flat_kernel(const MapDesc 
         const uint4 f = load_line_flags<true>(m.ray.dirty, item.start, item.count);
         const int n = build_line_list(line_flag_bits(f), L, m.ray.dirty, item.start, item.count);
         const FoldView v = fold_view(m);
-        add_touched(m, fold_line_list<2, true>(v, L, n, item.start, &hq));
+        add_touched(m, fold_line_list<2, true>(v, L.line, n, item.start, &hq));
         __syncthreads();
         fold_hit_queue(v, hq);
       }
@@ -726,12 +726,6 @@ cudaError_t launch_fold(const MapDesc *maps, const FoldItem *fitems, int *counte
                         int variant, cudaStream_t s) {
   const dim3 grid(sm_count_batch() * 8), block(256);
   if (variant == 0) {
-    batch_fold_list_kernel<4, 3><<<sm_count_batch() * 3, kListThreads, 0, s>>>(maps, fitems, counters);
-  } else if (variant == 3) {
-    batch_fold_list_kernel<2, 4><<<sm_count_batch() * 4, kListThreads, 0, s>>>(maps, fitems, counters);
-  } else if (variant == 4) {
-    batch_fold_list_kernel<8, 2><<<sm_count_batch() * 2, kListThreads, 0, s>>>(maps, fitems, counters);
-  } else if (variant == 5) {
     batch_fold_list_kernel<4, 4><<<sm_count_batch() * 4, kListThreads, 0, s>>>(maps, fitems, counters);
   } else if (variant == 1) {
     batch_fold_kernel<true><<<grid, block, 0, s>>>(maps, fitems, counters);
@@ -994,7 +988,7 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
       b->timed = value != 0;
       return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD:
-      if (value < 0 || value > 5) break;
+      if (value < 0 || value > 2) break;
       b->fold_variant = value;
       drop_graph(b);
       return CUBLOX_OK;

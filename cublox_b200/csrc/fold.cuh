@@ -258,15 +258,15 @@ __device__ __forceinline__ float fold_or_queue(const FoldView &v, HitQueue *hq, 
   return fold_counter(v, h, c, o);
 }
 
-// Fold of the CTA's list of n lines (item's first line `start`).  Warp w
-// of W takes line quads w, w + W, ...; lane (q, s) = (lane / 8, lane % 8)
+// Fold of the CTA's list of n lines (relative to line `start`).  Warp w of
+// W takes line quads w, w + W, ...; lane (q, s) = (lane / 8, lane % 8)
 // handles 16-byte piece s of the quad's line q.  A piece whose counters are
 // all zero is left as it is (its values do not change, its counters are
 // zero already).  Hit voxels go to `hq` when it is given (fold_hit_queue
 // folds them after a CTA barrier).  kL2: counters are read at L2.  Returns
 // the voxels folded or queued.
 template <int kQuads, bool kL2>
-__device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const LineList &L, int n,
+__device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const uint16_t *list, int n,
                                                    int start, HitQueue *hq = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   const int q = lane >> 3, sub = lane & 7;
@@ -280,7 +280,7 @@ __device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const Line
 #pragma unroll
     for (int u = 0; u < kQuads; ++u) {
       const int k = 4 * (i0 + u * warps) + q;
-      at[u] = k < n ? ((start + L.line[k]) << 3) + sub : -1;  // index of the 16-byte piece
+      at[u] = k < n ? ((start + list[k]) << 3) + sub : -1;  // index of the 16-byte piece
     }
     uint4 c[kQuads];
     float4 o[kQuads];

@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kListThreads, 4) fold_list_kernel(const ApplyP
     const int n = build_line_list(line_flag_bits(f), L, p.dirty, start, count_of(it));
     const int next = it + gridDim.x;
     if (next < items) f = load_line_flags(p.dirty, next * kListLines, count_of(next));
-    touched += fold_line_list<4, false>(v, L, n, start, &hq);
+    touched += fold_line_list<4, false>(v, L.line, n, start, &hq);
     __syncthreads();
     fold_hit_queue(v, hq);  // ends with a barrier: the list is rewritten next
   }

@@ -196,6 +196,6 @@ def test_batch_rejects_bad_calls():
     with pytest.raises(C.CubloxError):
         b.set_option(C.BATCH_OPT_SHAPE, 99)
     with pytest.raises(C.CubloxError):
-        b.set_option(C.BATCH_OPT_FOLD, 6)
+        b.set_option(C.BATCH_OPT_FOLD, 99)
     b.update([], [], np.zeros((0, 3), np.float32))
     b.close()
