@@ -584,6 +584,7 @@ BATCH_OPT_FOLD = 6
 BATCH_OPT_TUNING = 7
 BATCH_OPT_LAYOUT = 8
 BATCH_OPT_WAIT_LIMIT, BATCH_OPT_INJECT_MISSING_WALK = 9, 10
+BATCH_OPT_HOST_READ = 11
 DEVICE_WAIT_TIMEOUT = 1 << 3
 
 

@@ -120,21 +120,32 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
   for (int r = 0; r < rounds; ++r) {
     int j;
     bool live;
+    float x = 0.0f, y = 0.0f, z = 0.0f;
     if (ordered) {
       j = r ? item.count - 1 - t : t;
       live = r ? j >= nt : j < item.count;
-      j = live ? order.idx[j] : 0;
+      if (live) {
+        j = order.idx[j];
+        x = order.x[j];
+        y = order.y[j];
+        z = order.z[j];
+      }
     } else {
       j = r * nt + t;
       live = j < item.count;
+      if (live) {
+        const size_t k = static_cast<size_t>(item.start + j) * p.stride;
+        x = p.x[k];
+        y = p.y[k];
+        z = p.z[k];
+      }
     }
     FarWalk f;
     RayEnd re{-1, -1, false};
     bool far = false;
     if (live) {
-      const size_t k = static_cast<size_t>(item.start + j) * p.stride;
       RayWalk w;
-      if (ray_begin(p, p.x[k], p.y[k], p.z[k], w)) {
+      if (ray_begin(p, x, y, z, w)) {
         ++rays;
         re = ray_end_of<S, SZ>(p, w, clo);
         far = !walk_near<S, SZ>(p, cube, clo, w, f, incs);
@@ -760,6 +771,7 @@ struct cublox_batch {
   float *h_points = nullptr;
   size_t h_points_cap = 0;
   cudaEvent_t staged = nullptr;  // host staging free again
+  cudaEvent_t points_read = nullptr;  // the walk is done with points it read from h_points
   // shape choice
   int shape = 0;
   int layout = detail::kDefaultLayout;  // voxel layout of the batch's grids
@@ -770,7 +782,9 @@ struct cublox_batch {
   int tune_rounds = 2;
   std::vector<float> tune_ms;
   std::vector<WalkItem> order;  // fused launch: the queue in launch order (capacity kept)
+  std::vector<int> w_end, f_end;  // per map of an update: end of its walk / fold items
   bool graphs = false;
+  bool host_read = true;  // the walk reads host points in place (CUBLOX_BATCH_OPT_HOST_READ)
   int fold_variant = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_shape = -1;
@@ -842,6 +856,7 @@ int reserve_points(cublox_batch *b, size_t floats) {
   }
   if (floats > b->h_points_cap) {
     floats = std::max(floats, 2 * b->h_points_cap);
+    cudaStreamSynchronize(b->stream);  // a walk may be reading the old buffer in place
     if ((rc = ensure_pinned(reinterpret_cast<void **>(&b->h_points), floats * sizeof(float))))
       return rc;
     b->h_points_cap = floats;
@@ -910,7 +925,8 @@ int cublox_batch_create(void *stream, cublox_batch **out) {
   }
   if (cublox_b200::detail::dmalloc(&b->d_counters, sizeof(int) * kCounters) != cudaSuccess ||
       cublox_b200::detail::hmalloc(&b->h_counters, sizeof(int) * kCounters) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->points_read, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     delete b;
     return fail(CUBLOX_ERR_NOMEM, "batch_create: allocation failed");
@@ -938,6 +954,7 @@ int cublox_batch_destroy(cublox_batch *b) {
   if (b->h_counters) cublox_b200::detail::hfree(b->h_counters);
   if (b->h_points) cublox_b200::detail::hfree(b->h_points);
   if (b->staged) cudaEventDestroy(b->staged);
+  if (b->points_read) cudaEventDestroy(b->points_read);
   for (int i = 0; i < 4; ++i)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   if (b->own_stream) cudaStreamDestroy(b->stream);
@@ -987,6 +1004,9 @@ int cublox_batch_set_option(cublox_batch *b, int key, int value) {
     case CUBLOX_BATCH_OPT_TIMING:
       b->timed = value != 0;
       return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_HOST_READ:
+      b->host_read = value != 0;
+      return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD:
       if (value < 0 || value > 2) break;
       b->fold_variant = value;
@@ -1008,6 +1028,7 @@ int cublox_batch_get_option(const cublox_batch *b, int key, int *value) {
     case CUBLOX_BATCH_OPT_WAIT_LIMIT: *value = b->wait_limit; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_INJECT_MISSING_WALK: *value = b->inject_missing_walk; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_TIMING: *value = b->timed; return CUBLOX_OK;
+    case CUBLOX_BATCH_OPT_HOST_READ: *value = b->host_read; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_NUM_SHAPES: *value = kNumShapes; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_FOLD: *value = b->fold_variant; return CUBLOX_OK;
     case CUBLOX_BATCH_OPT_TUNING:
@@ -1059,7 +1080,7 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   // points: one concatenated x0 y0 z0 ... buffer, host or device
   cudaPointerAttributes pa;
   const float *base = xyz + 3 * offsets[0];
-  bool on_device = false;
+  bool on_device = false, staged_read = false;
   if (cudaPointerGetAttributes(&pa, xyz) == cudaSuccess)
     on_device = pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged;
   else
@@ -1069,23 +1090,37 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
   if (cudaEventSynchronize(b->staged) != cudaSuccess) cudaGetLastError();
   if (!on_device && total > 0) {
     const size_t floats = 3 * static_cast<size_t>(total);
-    if ((rc = reserve_points(b, floats))) return rc;
-    if (pa.type != cudaMemoryTypeHost) {
-      std::memcpy(b->h_points, base, floats * sizeof(float));
-      cudaError_t e = cudaMemcpyAsync(b->d_points, b->h_points, floats * sizeof(float),
-                                      cudaMemcpyHostToDevice, b->stream);
-      if (e != cudaSuccess) return cuda_fail(e, "batch points copy", __LINE__);
+    const bool pinned = pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr;
+    if (b->host_read && pinned) {
+      // the walk reads the caller's pinned points over the bus, each once,
+      // while it runs: no copy ahead of the launch
+      base = static_cast<const float *>(pa.devicePointer) + 3 * offsets[0];
     } else {
-      cudaError_t e = cudaMemcpyAsync(b->d_points, base, floats * sizeof(float),
-                                      cudaMemcpyHostToDevice, b->stream);
-      if (e != cudaSuccess) return cuda_fail(e, "batch points copy", __LINE__);
+      if ((rc = reserve_points(b, floats))) return rc;
+      const float *src = base;
+      if (!pinned) {
+        // a walk that read the staged points in place must be done with them
+        if (cudaEventSynchronize(b->points_read) != cudaSuccess) cudaGetLastError();
+        std::memcpy(b->h_points, base, floats * sizeof(float));
+        src = b->h_points;
+      }
+      if (b->host_read) {
+        base = b->h_points;  // staged in pinned memory, read in place by the walk
+        staged_read = true;
+      } else {
+        cudaError_t e = cudaMemcpyAsync(b->d_points, src, floats * sizeof(float),
+                                        cudaMemcpyHostToDevice, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "batch points copy", __LINE__);
+        base = b->d_points;
+      }
     }
-    base = b->d_points;
   }
   // descriptors and items; an empty scan leaves its grid untouched, as
   // cublox_grid_update does (OccupancyGrid.cpp:183-190)
   int w = 0, f = 0, d = 0;
-  std::vector<int> w_end, f_end;  // per map: end of its walk / fold items
+  auto &w_end = b->w_end, &f_end = b->f_end;  // per map: end of its walk / fold items
+  w_end.clear();
+  f_end.clear();
   for (int i = 0; i < n; ++i) {
     cublox_grid *g = grids[i];
     const int64_t off = offsets[i] - offsets[0];
@@ -1188,6 +1223,8 @@ int cublox_batch_update(cublox_batch *b, int n, cublox_grid *const *grids, const
                            "): " + what).c_str(), __LINE__);
   }
   b->timed = timed_before;
+  if (staged_read && (e = cudaEventRecord(b->points_read, b->stream)) != cudaSuccess)
+    return cuda_fail(e, "batch staging event", __LINE__);
   if (tuning) {
     float ms = 0.0f;  // walk + fold
     cudaEventSynchronize(b->ev[2]);

@@ -204,6 +204,7 @@ constexpr int kOrderStep = 32;   // loop iterations per bin
 constexpr int kOrderCap = 1024;  // rays per item the CTA orders
 
 struct RayOrder {
+  float x[kOrderCap], y[kOrderCap], z[kOrderCap];  // the item's points, in input order
   uint16_t idx[kOrderCap];  // the item's rays, shortest estimate first
   int base[kOrderBins];
 };
@@ -227,9 +228,11 @@ __device__ __forceinline__ int ray_len_estimate(const RayParams &p, float x, flo
   return l1 < 1e9f ? static_cast<int>(l1) : 1 << 30;
 }
 
-// Fills `o` with the order of the item's rays start .. start + count - 1
-// (count <= min(2 blockDim.x, kOrderCap)): o.idx[j] is the j-th shortest.
-// Contains CTA barriers; every thread of the CTA calls it.
+// Fills `o` with the item's points start .. start + count - 1 and their
+// order (count <= min(2 blockDim.x, kOrderCap)): o.idx[j] is the j-th
+// shortest.  Each point is read once, here (the points may sit in host
+// memory and be read over the bus).  Contains CTA barriers; every thread of
+// the CTA calls it.
 __device__ __forceinline__ void order_rays(const RayParams &p, int start, int count, RayOrder &o) {
   const int t = threadIdx.x, nt = blockDim.x;
   if (t < kOrderBins) o.base[t] = 0;
@@ -240,7 +243,11 @@ __device__ __forceinline__ void order_rays(const RayParams &p, int start, int co
     const int j = t + r * nt;
     if (j < count) {
       const size_t k = static_cast<size_t>(start + j) * p.stride;
-      bin[r] = min(kOrderBins - 1, ray_len_estimate(p, p.x[k], p.y[k], p.z[k]) / kOrderStep);
+      const float x = p.x[k], y = p.y[k], z = p.z[k];
+      o.x[j] = x;
+      o.y[j] = y;
+      o.z[j] = z;
+      bin[r] = min(kOrderBins - 1, ray_len_estimate(p, x, y, z) / kOrderStep);
       slot[r] = atomicAdd(&o.base[bin[r]], 1);
     }
   }

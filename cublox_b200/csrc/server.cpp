@@ -494,9 +494,10 @@ void worker_loop(cublox_server *s) {
       std::vector<float> sensors;
       size_t floats = 0;
       for (Request *r : ok) floats += pts_floats(r);
-      // One scan (the usual tick) is passed in place — from its pinned block
-      // the batch copies it to the device directly; several are
-      // concatenated into an uninitialised buffer, which the batch stages.
+      // One scan (the usual tick) is passed in place — the batch's walk reads
+      // it from its pinned block, which goes back to the pool only when the
+      // tick has completed; several are concatenated into an uninitialised
+      // buffer, which the batch stages in its own pinned buffer.
       std::unique_ptr<float[]> joined;
       const float *xyz = ok.size() == 1 ? pts_data(ok[0]) : nullptr;
       if (!xyz) {

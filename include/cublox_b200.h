@@ -319,6 +319,12 @@ typedef struct cublox_batch cublox_batch;
                                          exist, so the wait runs out; the
                                          maps are then left unfolded and
                                          must be reset                      */
+#define CUBLOX_BATCH_OPT_HOST_READ 11 /* host points (pinned, or staged in
+                                         the batch's pinned buffer): 1
+                                         (default) the walk reads them in
+                                         place over the bus, each point once,
+                                         while it runs; 0 copy them to the
+                                         device before the walk             */
 #define CUBLOX_BATCH_OPT_TUNING 7     /* read only: 1 while the tuner is
                                          still timing candidate shapes (the
                                          updates until it reads 0 run

@@ -81,7 +81,7 @@ def feed_pinned(batch, bg, clouds, sensors):
     off[1:] = np.cumsum([c.shape[0] for c in clouds])
     host = torch.from_numpy(np.concatenate(clouds, axis=0)).pin_memory()
     batch.update(bg, host.numpy(), sensors, offsets=off)
-    batch.synchronize()  # the pinned buffer is read by the device copy
+    batch.synchronize()  # the walk (or the copy ahead of it) reads the pinned buffer
 
 
 @pytest.mark.parametrize("graphs", [False, True])
@@ -150,11 +150,18 @@ def test_every_shape_gives_the_same_maps(shape):
     b.close()
 
 
-@pytest.mark.parametrize("feed", [feed_device, feed_pinned], ids=["device", "pinned"])
-def test_batch_inputs_device_and_pinned(feed):
+@pytest.mark.parametrize("host_read", [1, 0], ids=["read-in-place", "copied"])
+@pytest.mark.parametrize("feed", [feed_device, feed_pinned, feed_lists],
+                         ids=["device", "pinned", "pageable"])
+def test_batch_inputs_device_pinned_pageable(feed, host_read):
+    """Device points are walked where they are; host points are read in
+    place by the walk (pinned, or staged in the batch's pinned buffer) or
+    copied to the device first: the maps are the same."""
     w = small_workload(n_maps=5, n_steps=3, seed=9)
     b = C.Batch()
     b.set_option(C.BATCH_OPT_GRAPHS, 1)
+    b.set_option(C.BATCH_OPT_HOST_READ, host_read)
+    assert b.get_option(C.BATCH_OPT_HOST_READ) == host_read
     bg, solo = setup(w, b)
     run_and_compare(w, b, bg, solo, feed)
     b.close()
