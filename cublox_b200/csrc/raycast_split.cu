@@ -361,36 +361,47 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
     if (lane == 0) b = contiguous ? lo + atomicAdd(&cta_next, 32) : atomicAdd(work, 32);
     b = __shfl_sync(0xffffffffu, b, 0);
     if (b >= hi) break;
+    // Every lane runs the round, live or not, and the warp meets after the
+    // near phase, so that its far phases run together rather than in groups
+    // that entered the far loop at different times.
     const int g = b + lane;
-    if (g >= hi) continue;
-    const SegRec sr = segs[g];
-    if (sr.ray < 0) continue;
-    const RayRec rr = rays[sr.ray];
-    const int j_sum = sr.ax[0].j + sr.ax[1].j + sr.ax[2].j;
-    const int i0 = min(j_sum, rr.max_steps);
-    int budget = sr.ax[0].nj < 0
-                     ? 0x7fffffff
-                     : min(j_sum + sr.ax[0].nj + sr.ax[1].nj + sr.ax[2].nj, rr.max_steps) - i0;
+    bool live = g < hi;
+    SegRec sr;
+    if (live) {
+      sr = segs[g];
+      live = sr.ray >= 0;
+    }
     RayWalk w;
+    FarWalk f;
+    bool far = false;
+    int budget = 0;
+    if (live) {
+      const RayRec rr = rays[sr.ray];
+      const int j_sum = sr.ax[0].j + sr.ax[1].j + sr.ax[2].j;
+      const int i0 = min(j_sum, rr.max_steps);
+      budget = sr.ax[0].nj < 0
+                   ? 0x7fffffff
+                   : min(j_sum + sr.ax[0].nj + sr.ax[1].nj + sr.ax[2].nj, rr.max_steps) - i0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      w.id[a] = sr.ax[a].id;
-      w.en[a] = rr.en[a];
-      w.st[a] = rr.st[a];
-      w.tD[a] = rr.tD[a];
-      w.tM[a] = sr.ax[a].tM;
-      w.rel[a] = w.id[a] - p.win[a];
-      w.slot[a] = global_to_local(w.id[a], p.map[a], p.half[a]) + p.half[a];
+      for (int a = 0; a < 3; ++a) {
+        w.id[a] = sr.ax[a].id;
+        w.en[a] = rr.en[a];
+        w.st[a] = rr.st[a];
+        w.tD[a] = rr.tD[a];
+        w.tM[a] = sr.ax[a].tM;
+        w.rel[a] = w.id[a] - p.win[a];
+        w.slot[a] = global_to_local(w.id[a], p.map[a], p.half[a]) + p.half[a];
+      }
+      w.max_steps = rr.max_steps;
+      w.clipped = (rr.flags & kFlagClipped) != 0;
+      // A ray whose state L1 is the end voxel stops there: segments past it
+      // have nothing to walk.
+      if (!((rr.flags & kFlagEndsAtL1) && i0 > rr.L1))
+        far = !seg_near<S>(p, cube, clo, w, i0, budget, f, incs);
     }
-    w.max_steps = rr.max_steps;
-    w.clipped = (rr.flags & kFlagClipped) != 0;
-    // A ray whose state L1 is the end voxel stops there: segments past it
-    // have nothing to walk.
-    if (!((rr.flags & kFlagEndsAtL1) && i0 > rr.L1)) {
-      FarWalk f;
-      if (!seg_near<S>(p, cube, clo, w, i0, budget, f, incs)) walk_far(p, f, budget, incs);
-    }
-    if (sr.k == 0) {
+    __syncwarp();
+    if (far) walk_far(p, f, budget, incs);
+    if (live && sr.k == 0) {
       // Endpoint (kernels.cu:139-151).
       ++nrays;
       apply_end<S>(p, cube, ray_end_of<S>(p, w, clo), incs, hits);
