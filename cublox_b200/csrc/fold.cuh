@@ -24,16 +24,10 @@ struct FoldView {
 
 // One voxel: miss = op - hit (never negative), stored value shifted by
 // l_unknown, miss then hit added (fused or not as the pinned contraction
-// says), clamped, shifted back (kernels.cu:179-200).  The hit count is read
-// at L2 (ld.global.cg): in a fused launch other CTAs of the same kernel
-// wrote it.
-__device__ __forceinline__ float fold_counter(const FoldView &v, int h, uint32_t c, float s0) {
-  const int op = static_cast<int>(c & kOpMask);
-  int hit = 0;
-  if (c & kHitFlag) {
-    hit = static_cast<int>(__ldcg(v.hit + h));
-    v.hit[h] = 0u;
-  }
+// says), clamped, shifted back (kernels.cu:179-200).  fold_counter reads the
+// hit count of a flagged voxel at L2 (ld.global.cg): in a fused launch other
+// CTAs of the same kernel wrote it.
+__device__ __forceinline__ float fold_value(const FoldView &v, int op, int hit, float s0) {
   const int miss = op > hit ? op - hit : 0;
   float l = fadd(s0, v.l_unknown);
   l = (v.fp & kFpMissFma) ? ffma(v.l_miss, static_cast<float>(miss), l)
@@ -43,6 +37,15 @@ __device__ __forceinline__ float fold_counter(const FoldView &v, int h, uint32_t
   if (l < v.l_min) l = v.l_min;
   if (l > v.l_max) l = v.l_max;
   return fsub(l, v.l_unknown);
+}
+
+__device__ __forceinline__ float fold_counter(const FoldView &v, int h, uint32_t c, float s0) {
+  int hit = 0;
+  if (c & kHitFlag) {
+    hit = static_cast<int>(__ldcg(v.hit + h));
+    v.hit[h] = 0u;
+  }
+  return fold_value(v, static_cast<int>(c & kOpMask), hit, s0);
 }
 
 __device__ __forceinline__ bool any_set(const uint4 &c) { return (c.x | c.y | c.z | c.w) != 0u; }
@@ -294,11 +297,20 @@ __device__ __forceinline__ uint32_t fold_line_list(const FoldView &v, const uint
     for (int u = 0; u < kQuads; ++u) {
       if (at[u] < 0 || !any_set(c[u])) continue;
       const int h = at[u] << 2;
-      if (c[u].x) { o[u].x = fold_or_queue(v, hq, h + 0, c[u].x, o[u].x); ++touched; }
-      if (c[u].y) { o[u].y = fold_or_queue(v, hq, h + 1, c[u].y, o[u].y); ++touched; }
-      if (c[u].z) { o[u].z = fold_or_queue(v, hq, h + 2, c[u].z, o[u].z); ++touched; }
-      if (c[u].w) { o[u].w = fold_or_queue(v, hq, h + 3, c[u].w, o[u].w); ++touched; }
-      o4[at[u]] = o[u];
+      const uint32_t cc[4] = {c[u].x, c[u].y, c[u].z, c[u].w};
+      float oo[4] = {o[u].x, o[u].y, o[u].z, o[u].w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        touched += cc[e] != 0u;
+        if (cc[e] & kHitFlag) {  // rare: queued, or folded here with its hit count
+          oo[e] = fold_or_queue(v, hq, h + e, cc[e], oo[e]);
+        } else {
+          // no hit: the same arithmetic for every lane, kept where counted
+          const float f = fold_value(v, static_cast<int>(cc[e]), 0, oo[e]);
+          oo[e] = cc[e] ? f : oo[e];
+        }
+      }
+      o4[at[u]] = make_float4(oo[0], oo[1], oo[2], oo[3]);
       c4[at[u]] = make_uint4(0u, 0u, 0u, 0u);
     }
   }

@@ -180,22 +180,23 @@ __global__ void __launch_bounds__(256) fold_lines_kernel(const ApplyParams p) {
 // b, b + grid, ... and loads the next item's flags before folding the
 // current list.
 template <bool kStats>
-__global__ void __launch_bounds__(kListThreads, 4) fold_list_kernel(const ApplyParams p) {
+__global__ void __launch_bounds__(kListThreads, 4) fold_list_kernel(const ApplyParams p,
+                                                                     int item_lines) {
   __shared__ LineList L;
   __shared__ HitQueue hq;
   if (threadIdx.x == 0) hq.n = 0;  // the first read follows build_line_list's barriers
   const FoldView v = fold_view(p);
-  const int items = (p.nlines + kListLines - 1) / kListLines;
-  auto count_of = [&](int it) { return min(kListLines, p.nlines - it * kListLines); };
+  const int items = (p.nlines + item_lines - 1) / item_lines;
+  auto count_of = [&](int it) { return min(item_lines, p.nlines - it * item_lines); };
   int it = blockIdx.x;
   uint4 f = make_uint4(0u, 0u, 0u, 0u);
-  if (it < items) f = load_line_flags(p.dirty, it * kListLines, count_of(it));
+  if (it < items) f = load_line_flags(p.dirty, it * item_lines, count_of(it));
   uint32_t touched = 0;
   for (; it < items; it += gridDim.x) {
-    const int start = it * kListLines;
+    const int start = it * item_lines;
     const int n = build_line_list(line_flag_bits(f), L, p.dirty, start, count_of(it));
     const int next = it + gridDim.x;
-    if (next < items) f = load_line_flags(p.dirty, next * kListLines, count_of(next));
+    if (next < items) f = load_line_flags(p.dirty, next * item_lines, count_of(next));
     touched += fold_line_list<4, false>(v, L.line, n, start, &hq);
     __syncthreads();
     fold_hit_queue(v, hq);  // ends with a barrier: the list is rewritten next
@@ -626,13 +627,18 @@ void launch_step_count(const RayParams &p, cudaStream_t s) {
 void launch_apply(const ApplyParams &p, cudaStream_t s) {
   if (p.variant == 2) {
     if (p.nlines <= 0) return;
-    int grid = (p.nlines + kListLines - 1) / kListLines;
+    // items of up to 4,096 lines, smaller for small maps so that every SM
+    // gets some (a multiple of 16 lines keeps the 16-byte flag loads aligned)
     const int cap = sm_count() * 4;
+    int item_lines = (p.nlines + cap - 1) / cap;
+    item_lines = ((item_lines + 255) / 256) * 256;
+    if (item_lines > kListLines) item_lines = kListLines;
+    int grid = (p.nlines + item_lines - 1) / item_lines;
     if (grid > cap) grid = cap;
     if (p.stats)
-      fold_list_kernel<true><<<grid, kListThreads, 0, s>>>(p);
+      fold_list_kernel<true><<<grid, kListThreads, 0, s>>>(p, item_lines);
     else
-      fold_list_kernel<false><<<grid, kListThreads, 0, s>>>(p);
+      fold_list_kernel<false><<<grid, kListThreads, 0, s>>>(p, item_lines);
     return;
   }
   if (p.variant == 3) {
