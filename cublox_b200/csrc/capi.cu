@@ -222,7 +222,7 @@ static int64_t make_layout(const int map[3], int code, VoxLayout *L, int nbr[3])
   return n;
 }
 
-size_t cublox_b200::detail::voxel_bytes_for(const int half[3]) {
+int64_t cublox_b200::detail::nalloc_for(const int half[3]) {
   int map[3];
   for (int a = 0; a < 3; ++a) map[a] = 2 * half[a] + 1;
   int64_t nalloc = 0;
@@ -232,6 +232,11 @@ size_t cublox_b200::detail::voxel_bytes_for(const int half[3]) {
     const int64_t n = make_layout(map, code, &l, nb);
     if (n <= (int64_t(1) << 31)) nalloc = std::max(nalloc, n);
   }
+  return nalloc;
+}
+
+size_t cublox_b200::detail::voxel_bytes_for(const int half[3]) {
+  const int64_t nalloc = nalloc_for(half);
   return 12 * static_cast<size_t>(nalloc) + static_cast<size_t>(nalloc >> kLineShift);
 }
 
@@ -798,6 +803,39 @@ int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host) {
     e = cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "acquire_device", __LINE__);
+  return CUBLOX_OK;
+}
+
+int cublox_b200::detail::detach_voxels(cublox_grid *g, float *occ_host, VoxelBuffers *out) {
+  if (!g->d_occ) return fail(CUBLOX_ERR_INVALID, "detach_voxels: grid holds no voxel buffers");
+  if (occ_host) {
+    const cudaError_t e = cudaMemcpyAsync(occ_host, g->d_occ,
+                                          sizeof(float) * static_cast<size_t>(g->nalloc),
+                                          cudaMemcpyDeviceToHost, g->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "detach_voxels", __LINE__);
+  }
+  out->nalloc = g->nalloc;
+  out->occ = g->d_occ;
+  out->cnt = g->d_cnt;
+  out->hit = g->d_hit;
+  g->d_occ = nullptr;
+  g->d_cnt = g->d_hit = nullptr;
+  return CUBLOX_OK;
+}
+
+int cublox_b200::detail::attach_voxels(cublox_grid *g, VoxelBuffers *in, const float *occ_host) {
+  if (g->d_occ || in->nalloc != g->nalloc || !in->occ)
+    return fail(CUBLOX_ERR_INVALID, "attach_voxels: buffers of another size, or grid not empty");
+  const size_t n = static_cast<size_t>(g->nalloc);
+  const cudaError_t e =
+      occ_host ? cudaMemcpyAsync(in->occ, occ_host, n * sizeof(float), cudaMemcpyHostToDevice,
+                                 g->stream)
+               : cudaMemsetAsync(in->occ, 0, n * sizeof(float), g->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "attach_voxels", __LINE__);
+  g->d_occ = in->occ;
+  g->d_cnt = in->cnt;
+  g->d_hit = in->hit;
+  *in = VoxelBuffers{};
   return CUBLOX_OK;
 }
 

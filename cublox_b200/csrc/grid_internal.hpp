@@ -168,6 +168,25 @@ int release_scratch(cublox_grid *g);
 // Allocate the voxel buffers again, stored log-odds from occ_host (all
 // unknown if null), counters zero.
 int acquire_device(cublox_grid *g, const float *occ_host);
+// A grid's voxel buffers (stored log-odds, traversal and hit counters)
+// detached from it, to be handed to another grid of the same allocation
+// size without freeing and allocating.  The counters are zero (they are
+// between scans).
+struct VoxelBuffers {
+  int64_t nalloc = 0;
+  float *occ = nullptr;
+  uint32_t *cnt = nullptr, *hit = nullptr;
+  size_t bytes() const { return 12 * static_cast<size_t>(nalloc); }
+};
+// Voxels the arrays of a grid with these half sizes hold (padding included).
+int64_t nalloc_for(const int half[3]);
+// Detach g's voxel buffers into *out after enqueueing, on g's stream, the
+// copy of its stored log-odds to occ_host (pinned for the copy to be
+// asynchronous).  No sync, no free.  g must not be used until attach_voxels.
+int detach_voxels(cublox_grid *g, float *occ_host, VoxelBuffers *out);
+// Give g the buffers *in (same nalloc) and enqueue, on g's stream, the copy
+// of its stored log-odds from occ_host (all unknown if null).
+int attach_voxels(cublox_grid *g, VoxelBuffers *in, const float *occ_host);
 // fetch_batch on stream st (ordered after the grid's work by the caller),
 // outputs sized to the samples found, in the scratch `sc` (the grid's own if
 // null).

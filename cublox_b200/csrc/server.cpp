@@ -82,14 +82,15 @@ struct MapState {
   cublox_grid *g = nullptr;  // created at first admission
   bool resident = false;
   // stored log-odds while evicted (the grid's own layout): a pinned buffer
-  // allocated at the map's first eviction and kept for the next ones, or
-  // pageable memory if pinning failed
+  // allocated when the maps outgrow the budget (cublox_server_add_map) or at
+  // the map's first eviction, and kept; pageable memory if pinning failed
   float *snap_pinned = nullptr;
   std::vector<float> snap_pageable;
   const float *snapshot() const {
     return snap_pinned ? snap_pinned : (snap_pageable.empty() ? nullptr : snap_pageable.data());
   }
   size_t vox_bytes = 0;  // device bytes of the map's arrays
+  int64_t nalloc = 0;    // voxels each array holds (padding included)
   int64_t voxels = 0;
   uint64_t last_use = 0;
   std::deque<Request *> queue;  // pending requests, arrival order
@@ -187,6 +188,9 @@ struct cublox_server {
   std::condition_variable cv_inflight;  // a tick left the device
   std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
   std::vector<std::unique_ptr<MapState>> maps;  // reserved: never reallocated
+  // voxel buffers of evicted maps, kept for the next map of the same size
+  // (worker thread only)
+  std::vector<cublox_b200::detail::VoxelBuffers> spare;
   std::atomic<int> n_maps{0};                    // maps[0, n_maps) are published
   std::deque<Tick> inflight;
   std::deque<FetchJob> fetch_jobs;
@@ -255,7 +259,38 @@ size_t used_bytes(cublox_server *s) {
   const int nm = s->n_maps.load();
   for (int j = 0; j < nm; ++j)
     if (s->maps[j]->resident) b += cublox_b200::detail::device_bytes(s->maps[j]->g);
+  for (const auto &v : s->spare) b += v.bytes();
   return b;
+}
+
+// Hand map m a spare set of voxel buffers of its size, if there is one: its
+// stored log-odds are copied in on the server stream (no allocation, no
+// sync).  Returns 1 if it did, 0 if no spare fits, <0 on error.
+int take_spare(cublox_server *s, MapState &m) {
+  for (size_t i = 0; i < s->spare.size(); ++i) {
+    if (s->spare[i].nalloc != m.nalloc) continue;
+    const int rc = cublox_b200::detail::attach_voxels(m.g, &s->spare[i], m.snapshot());
+    if (rc) return rc;
+    s->spare.erase(s->spare.begin() + static_cast<std::ptrdiff_t>(i));
+    return 1;
+  }
+  return 0;
+}
+
+// Free spare buffer sets (largest first) until `need` more bytes fit the
+// budget.  cudaFree waits for the device: only a map's first admission, or
+// one whose size no spare has, comes here.
+void free_spares(cublox_server *s, size_t need) {
+  while (!s->spare.empty() && used_bytes(s) + need > s->cfg.hbm_budget_bytes) {
+    size_t big = 0;
+    for (size_t i = 1; i < s->spare.size(); ++i)
+      if (s->spare[i].nalloc > s->spare[big].nalloc) big = i;
+    auto &v = s->spare[big];
+    cublox_b200::detail::dfree(v.occ);
+    cublox_b200::detail::dfree(v.cnt);
+    cublox_b200::detail::dfree(v.hit);
+    s->spare.erase(s->spare.begin() + static_cast<std::ptrdiff_t>(big));
+  }
 }
 
 // Make map `mi` resident, evicting least recently used maps not in `busy`
@@ -267,33 +302,55 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
   MapState &m = *s->maps[mi];
   m.last_use = ++s->clock;
   if (m.resident) return CUBLOX_OK;
-  const size_t need = m.vox_bytes;
+  size_t need = m.vox_bytes;
   if (need + scratch_bytes(s) > s->cfg.hbm_budget_bytes)
     return fail(CUBLOX_ERR_NOMEM, "server: map needs " + std::to_string(need) +
                                       " bytes, more than the budget allows");
-  // First give back the per-call scratch (fetch outputs) of idle maps.
+  // First give back the per-call scratch (fetch outputs) of idle maps that
+  // hold some (release_scratch waits for the server stream).
   if (used_bytes(s) + need > s->cfg.hbm_budget_bytes)
     for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
       MapState &o = *s->maps[j];
-      if (j != mi && o.resident && !busy[j] && !o.fetching.load())
+      if (j != mi && o.resident && !busy[j] && !o.fetching.load() &&
+          cublox_b200::detail::device_bytes(o.g) > o.vox_bytes)
         cublox_b200::detail::release_scratch(o.g);
     }
-  while (used_bytes(s) + need > s->cfg.hbm_budget_bytes) {
+  // A map that was resident before takes a spare set of its size, if any
+  // (an eviction earlier left one), without allocating.  Otherwise maps are
+  // evicted (their buffers become spare sets) until one of them fits, or
+  // until freeing spare sets of other sizes makes room.
+  for (;;) {
+    if (m.g) {
+      const int rc = take_spare(s, m);
+      if (rc < 0) return rc;
+      if (rc == 1) {
+        need = 0;
+        break;
+      }
+    }
+    size_t spare = 0;
+    for (const auto &v : s->spare) spare += v.bytes();
+    if (used_bytes(s) - spare + need <= s->cfg.hbm_budget_bytes) break;
     // the victim: a resident map outside this tick, preferring maps with no
-    // queued request (their next use is furthest off), least recently used
+    // queued request (their next use is furthest off), then maps of this
+    // map's size (their buffers can be handed over), least recently used
     // first
     int victim = -1;
     {
       std::lock_guard<std::mutex> lk(s->mu);
-      bool victim_idle = false;
+      bool victim_idle = false, victim_same = false;
       for (int j = 0; j < static_cast<int>(busy.size()); ++j) {
         MapState &o = *s->maps[j];
         if (j == mi || !o.resident || busy[j] || o.fetching.load()) continue;
-        const bool idle = o.queue.empty();
-        if (victim < 0 || (idle && !victim_idle) ||
-            (idle == victim_idle && o.last_use < s->maps[victim]->last_use)) {
+        const bool idle = o.queue.empty(), same = o.nalloc == m.nalloc;
+        const bool better =
+            victim < 0 || (idle && !victim_idle) ||
+            (idle == victim_idle && same && !victim_same) ||
+            (idle == victim_idle && same == victim_same && o.last_use < s->maps[victim]->last_use);
+        if (better) {
           victim = j;
           victim_idle = idle;
+          victim_same = same;
         }
       }
     }
@@ -302,28 +359,34 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
       return fail(CUBLOX_ERR_NOMEM, "server: no map can be evicted");
     }
     MapState &v = *s->maps[victim];
-    const size_t n = static_cast<size_t>(v.g->nalloc);
+    const size_t n = static_cast<size_t>(v.nalloc);
     if (!v.snap_pinned && v.snap_pageable.empty() &&
         cublox_b200::detail::hmalloc(&v.snap_pinned, n * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       v.snap_pinned = nullptr;
       v.snap_pageable.resize(n);
     }
-    int rc = cublox_b200::detail::release_device(
-        v.g, v.snap_pinned ? v.snap_pinned : v.snap_pageable.data());
+    // The stored log-odds go to the snapshot on the server stream, ordered
+    // before any later use of the buffers; the buffers become a spare set.
+    cublox_b200::detail::VoxelBuffers vb;
+    int rc = cublox_b200::detail::detach_voxels(
+        v.g, v.snap_pinned ? v.snap_pinned : v.snap_pageable.data(), &vb);
     if (rc) return rc;
+    s->spare.push_back(vb);
     v.resident = false;
     std::lock_guard<std::mutex> lk(s->mu);
     ++s->stats.evictions;
   }
   int rc;
   if (!m.g) {
+    free_spares(s, need);
     rc = cublox_grid_create(m.half, m.res, m.ctr, m.has_thr, m.thr, m.origin, s->stream, &m.g);
     if (rc) return rc;
     cublox_grid_set_max_range(m.g, m.max_range);
     if (m.has_lo)
       cublox_grid_set_log_odds(m.g, m.lo[0], m.lo[1], m.lo[2], m.lo[3], m.lo[4], m.lo[5]);
-  } else {
+  } else if (need) {
+    free_spares(s, need);
     rc = cublox_b200::detail::acquire_device(m.g, m.snapshot());
     if (rc) return rc;
   }
@@ -692,6 +755,11 @@ int cublox_server_destroy(cublox_server *s) {
     if (m->g) cublox_grid_destroy(m->g);
     cublox_b200::detail::hfree(m->snap_pinned);
   }
+  for (auto &v : s->spare) {
+    cublox_b200::detail::dfree(v.occ);
+    cublox_b200::detail::dfree(v.cnt);
+    cublox_b200::detail::dfree(v.hit);
+  }
   cublox_batch_destroy(s->batch);
   cublox_b200::detail::free_fetch(&s->fscratch);
   s->pinned.release_all();
@@ -730,12 +798,27 @@ int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float re
   }
   m->voxels = vox;
   m->vox_bytes = cublox_b200::detail::voxel_bytes_for(m->half);
+  m->nalloc = cublox_b200::detail::nalloc_for(m->half);
   std::lock_guard<std::mutex> lk(s->mu);
   if (static_cast<int>(s->maps.size()) >= kMaxMaps)
     return fail(CUBLOX_ERR_INVALID, "server_add_map: at most 4096 maps");
   *map_id = static_cast<int>(s->maps.size());
   s->maps.push_back(std::move(m));
   s->n_maps.store(static_cast<int>(s->maps.size()));
+  // Once the maps outgrow the budget, evictions will come: pin every map's
+  // snapshot buffer now, so that no eviction pins memory while serving
+  // (pinning a few hundred MB takes tens of milliseconds).
+  size_t total = scratch_bytes(s);
+  for (const auto &o : s->maps) total += o->vox_bytes;
+  if (total > s->cfg.hbm_budget_bytes)
+    for (auto &o : s->maps)
+      if (!o->snap_pinned && o->snap_pageable.empty() &&
+          cublox_b200::detail::hmalloc(&o->snap_pinned,
+                                       static_cast<size_t>(o->nalloc) * sizeof(float)) !=
+              cudaSuccess) {
+        cudaGetLastError();  // pinned later, or pageable
+        o->snap_pinned = nullptr;
+      }
   return CUBLOX_OK;
 }
 

@@ -124,6 +124,48 @@ def test_tight_budget_evicts_and_restores_bit_for_bit():
     s.close()
 
 
+def test_swaps_between_maps_of_one_size_allocate_nothing():
+    """Three maps of one size under a budget that holds two: once every map
+    has been admitted, each swap hands the evicted map's voxel buffers to
+    the map coming back (its stored log-odds copied out and in on the
+    server stream) — no device or pinned allocation, no free — and every
+    map still equals a lone grid fed the same scans."""
+    w = synth.serving(n_robots=3, seconds=0.05, scan_rate=400.0, fetch_rate=10.0,
+                      dims=((32, 32, 8),), sensors=SENSORS[:2], probs=(0.5, 0.5), poses=3,
+                      max_range=6.0, threshold=0.5, n_boxes=40, fetch_n=16, fetch_radius=0.6,
+                      seed=17)
+    scratch = C.Server.scratch_bytes(4096, **SMALL_FETCH)
+    per_map = 12 * voxels((32, 32, 8))
+    s = C.Server(hbm_budget_bytes=scratch + int(2.5 * per_map), max_tick_points=4096,
+                 **SMALL_FETCH)
+    ids = [s.add_map(w.halves[r], w.resolution, False, w.threshold, max_range=w.max_range,
+                     log_odds=LO) for r in range(3)]
+    before = None
+    for step in range(8):
+        if step == 1:
+            before = C.runtime_counters()  # every map admitted once
+        for r in range(3):  # round robin: every scan needs a swap
+            pts, origin = w.pool[r][step % 2][step % 3]
+            rid = s.submit_scan(ids[r], pts, origin, True)
+            assert s.wait(rid) == C.REQ_DONE
+    after = C.runtime_counters()
+    st = s.stats()
+    assert st["evictions"] >= 7 * 3 - 2, st
+    assert after == before, (before, after)
+    for r in range(3):  # the lone grids run after the counters are read
+        g = C.OccupancyGrid(w.halves[r], w.resolution, False, w.threshold)
+        g.setLogOddsParams(*LO)
+        g.setMaxRaycastRange(w.max_range)
+        for step in range(8):
+            pts, origin = w.pool[r][step % 2][step % 3]
+            g.update(pts, origin)
+            g.recenter(origin)
+        occ, origin = s.export(ids[r], voxels(w.halves[r]))
+        assert origin == tuple(g.getOriginIndex()), r
+        assert np.array_equal(occ.view(np.uint32), g.export().view(np.uint32)), r
+    s.close()
+
+
 def test_map_larger_than_budget_fails_alone():
     w = workload(n_robots=2, seconds=0.05, seed=13)
     s = C.Server(hbm_budget_bytes=C.Server.scratch_bytes(4096, **SMALL_FETCH)
