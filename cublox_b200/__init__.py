@@ -26,6 +26,7 @@ DEPTH_U16_MM, DEPTH_F32_M = 0, 1
 OPT_RAYCAST, OPT_CUBE, OPT_MATCH, OPT_SORT, OPT_SEGMENT, OPT_FOLD, OPT_BLOCK, OPT_CONTIGUOUS = (
     1, 2, 3, 4, 5, 6, 7, 8)
 OPT_LAYOUT = 9
+OPT_FLAT_CUBE = 10
 LAYOUTS = (320, 230, 221, 0)  # 8x4x1, 4x8x1, 4x4x2 bricks; the reference's hash order
 
 

@@ -488,6 +488,9 @@ int cublox_grid_set_option(cublox_grid *g, int key, int value) {
       if (value != 0 && value != 8 && value != 16 && value != 32) break;
       g->opt_cube = value;
       return CUBLOX_OK;
+    case CUBLOX_OPT_FLAT_CUBE:
+      g->opt_flat = value != 0;
+      return CUBLOX_OK;
     case CUBLOX_OPT_MATCH:
       g->opt_match = value != 0;
       return CUBLOX_OK;
@@ -505,6 +508,7 @@ int cublox_grid_get_option(const cublox_grid *g, int key, int *value) {
   switch (key) {
     case CUBLOX_OPT_RAYCAST: *value = g->opt_raycast; return CUBLOX_OK;
     case CUBLOX_OPT_CUBE: *value = g->opt_cube; return CUBLOX_OK;
+    case CUBLOX_OPT_FLAT_CUBE: *value = g->opt_flat; return CUBLOX_OK;
     case CUBLOX_OPT_MATCH: *value = g->opt_match; return CUBLOX_OK;
     case CUBLOX_OPT_SORT: *value = g->opt_sort; return CUBLOX_OK;
     case CUBLOX_OPT_SEGMENT: *value = g->opt_seg; return CUBLOX_OK;
@@ -655,7 +659,7 @@ static int integrate(cublox_grid *g, const float *dx, const float *dy,
       ps.z = g->d_sorted + 2 * static_cast<size_t>(n);
       ps.stride = 1;
     }
-    launch_raycast_split(ps, g->opt_cube, g->opt_seg, sc, g->stream);
+    launch_raycast_split(ps, g->opt_cube, g->opt_flat, g->opt_seg, sc, g->stream);
   } else if (g->opt_raycast == 1) {
     BinnedScratch b{g->d_bins, g->d_hist, g->d_hist + binned_bins(), g->d_sorted};
     launch_raycast_binned(p, b, g->opt_cube, g->opt_match != 0, g->opt_sort != 0, g->stream);

@@ -50,6 +50,7 @@ struct cublox_grid {
   int opt_block = 512;  // split walk CTA size
   int opt_contig = 0;   // split walk: contiguous segment runs per CTA
   int opt_cube = 32;    // shared-memory counter cube side (0, 16, 32)
+  bool opt_flat = false;  // split walk, cube 32: 32 x 32 x 16 (CUBLOX_OPT_FLAT_CUBE)
   int opt_match = 0;    // merge duplicate voxels within a warp
   int opt_sort = 0;     // walk rays in direction-bin order
   void *d_segs = nullptr;  // split walk: segment records

@@ -173,8 +173,10 @@ struct SplitScratch {
 };
 size_t split_seg_bytes();
 size_t split_ray_bytes();
-void launch_raycast_split(const RayParams &p, int cube, int seg_len, const SplitScratch &sc,
-                          cudaStream_t s);
+// cube: side of the shared-memory counter cube (0, 8, 16, 32); flat (cube
+// 32 only): a 32 x 32 x 16 cube, two CTAs per SM.
+void launch_raycast_split(const RayParams &p, int cube, bool flat, int seg_len,
+                          const SplitScratch &sc, cudaStream_t s);
 // cube: side of the shared-memory counter cube (16 or 32); match: merge
 // duplicate voxel keys within a warp; sort: walk rays in direction order.
 void launch_raycast_binned(const RayParams &p, const BinnedScratch &b, int cube,

@@ -314,14 +314,14 @@ __global__ void __launch_bounds__(3 * kPlanRays) seg_plan_kernel(const RayParams
 // outside the window, for at most `budget` iterations.  Returns true if the
 // segment ended in it; false once the walk is in the window and outside the
 // cube (f then holds it).
-template <int S>
+template <int S, int SZ = S>
 __device__ __forceinline__ bool seg_near(const RayParams &p, uint32_t *cube, const int clo[3],
                                          RayWalk &w, int i, int &budget, FarWalk &f,
                                          uint32_t &incs) {
   for (;; ++i, --budget) {
     if (budget <= 0 || i >= w.max_steps || at_end(w)) return true;
     if (in_window(w, p)) {
-      const int c = cube_cell<S>(w.id[0], w.id[1], w.id[2], clo);
+      const int c = cube_cell<S, SZ>(w.id[0], w.id[1], w.id[2], clo);
       if (c < 0) {
         to_far(p, w, i, f);
         return false;
@@ -335,14 +335,14 @@ __device__ __forceinline__ bool seg_near(const RayParams &p, uint32_t *cube, con
   }
 }
 
-template <int S>
+template <int S, int SZ = S>
 __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const int cl0,
                                                        const int cl1, const int cl2,
                                                        const SegRec *segs, const RayRec *rays,
                                                        const int *seg_count, int *work,
                                                        const int contiguous) {
   extern __shared__ uint32_t cube[];
-  constexpr int kCube = S * S * S;
+  constexpr int kCube = S * S * SZ;
   __shared__ int cta_next;
   for (int q = threadIdx.x; q < kCube / 4; q += blockDim.x)
     reinterpret_cast<uint4 *>(cube)[q] = make_uint4(0u, 0u, 0u, 0u);
@@ -397,18 +397,18 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
       // A ray whose state L1 is the end voxel stops there: segments past it
       // have nothing to walk.
       if (!((rr.flags & kFlagEndsAtL1) && i0 > rr.L1))
-        far = !seg_near<S>(p, cube, clo, w, i0, budget, f, incs);
+        far = !seg_near<S, SZ>(p, cube, clo, w, i0, budget, f, incs);
     }
     __syncwarp();
     if (far) walk_far(p, f, budget, incs);
     if (live && sr.k == 0) {
       // Endpoint (kernels.cu:139-151).
       ++nrays;
-      apply_end<S>(p, cube, ray_end_of<S>(p, w, clo), incs, hits);
+      apply_end<S>(p, cube, ray_end_of<S, SZ>(p, w, clo), incs, hits);
     }
   }
   __syncthreads();
-  flush_cube<S>(p, cube, clo);
+  flush_cube<S, SZ>(p, cube, clo);
   if (p.stats) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -435,22 +435,22 @@ int sm_count_split() {
   return n;
 }
 
-template <int S>
+template <int S, int SZ = S>
 void launch_seg_walk(const RayParams &p, const int clo[3], const SplitScratch &sc,
                      cudaStream_t s) {
-  const size_t smem = sizeof(uint32_t) * S * S * S;
+  const size_t smem = sizeof(uint32_t) * S * S * SZ;
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute(seg_walk_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(seg_walk_kernel<S, SZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
   const int block = sc.block == 256 || sc.block == 1024 ? sc.block : 512;
   static int per_sm[3] = {0, 0, 0};
   int &ps = per_sm[block == 256 ? 0 : (block == 512 ? 1 : 2)];
   if (ps == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, seg_walk_kernel<S>, block, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, seg_walk_kernel<S, SZ>, block, smem);
     if (ps < 1) ps = 1;
   }
   const int grid = sm_count_split() * ps;
-  seg_walk_kernel<S><<<grid, block, smem, s>>>(
+  seg_walk_kernel<S, SZ><<<grid, block, smem, s>>>(
       p, clo[0], clo[1], clo[2], reinterpret_cast<const SegRec *>(sc.segs),
       reinterpret_cast<const RayRec *>(sc.rays), sc.counters, sc.counters + 1, sc.contiguous);
 }
@@ -460,18 +460,21 @@ void launch_seg_walk(const RayParams &p, const int clo[3], const SplitScratch &s
 size_t split_seg_bytes() { return sizeof(SegRec); }
 size_t split_ray_bytes() { return sizeof(RayRec); }
 
-void launch_raycast_split(const RayParams &p, int cube, int seg_len, const SplitScratch &sc,
-                          cudaStream_t s) {
+void launch_raycast_split(const RayParams &p, int cube, bool flat, int seg_len,
+                          const SplitScratch &sc, cudaStream_t s) {
   if (p.n <= 0) return;
   cudaMemsetAsync(sc.counters, 0, 2 * sizeof(int), s);
   seg_plan_kernel<<<(p.n + kPlanRays - 1) / kPlanRays, 3 * kPlanRays, 0, s>>>(
       p, seg_len, sc.max_segs, reinterpret_cast<SegRec *>(sc.segs),
       reinterpret_cast<RayRec *>(sc.rays), sc.counters, sc.seg_cap);
   int clo[3];
-  const int hc = cube / 2;
+  flat = flat && cube >= 32;
   for (int a = 0; a < 3; ++a)
-    clo[a] = pos_to_global_dev(p.o[a], p.inv, p.ctr != 0, p.fp) - hc;
-  if (cube >= 32)
+    clo[a] = pos_to_global_dev(p.o[a], p.inv, p.ctr != 0, p.fp) -
+             (a == 2 && flat ? cube / 4 : cube / 2);
+  if (flat)
+    launch_seg_walk<32, 16>(p, clo, sc, s);
+  else if (cube >= 32)
     launch_seg_walk<32>(p, clo, sc, s);
   else if (cube >= 16)
     launch_seg_walk<16>(p, clo, sc, s);

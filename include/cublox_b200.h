@@ -120,6 +120,9 @@ int cublox_grid_get_fp_mode(const cublox_grid *g, unsigned *mode);
 #define CUBLOX_OPT_CONTIGUOUS 8 /* split walk: each CTA walks one run of
                                    consecutive segments (default 0: all
                                    CTAs share one segment queue)            */
+#define CUBLOX_OPT_FLAT_CUBE 10 /* split walk with cube 32: a 32 x 32 x 16
+                                   cube (half the height, two CTAs per SM);
+                                   0 (default) or 1                      */
 #define CUBLOX_OPT_LAYOUT 9  /* voxel layout of the grid's arrays: log2 of
                                 the brick sides as decimal digits x y z,
                                 bricks of 32 voxels (320: 8 x 4 x 1, the

@@ -359,7 +359,8 @@ def test_fold_variants_exact(small, fold):
 VARIANTS = [dict(raycast=0), dict(raycast=1, cube=32, match=1, sort=1),
             dict(raycast=1, cube=16, match=0, sort=1), dict(raycast=1, cube=0, match=1, sort=0),
             dict(raycast=2, cube=32, seg=48), dict(raycast=2, cube=0, seg=4, sort=0),
-            dict(raycast=2, cube=16, seg=7, contig=0), dict(raycast=2, cube=8, seg=16, sort=1)]
+            dict(raycast=2, cube=16, seg=7, contig=0), dict(raycast=2, cube=8, seg=16, sort=1),
+            dict(raycast=2, cube=32, seg=64, flat=1), dict(raycast=2, cube=32, seg=5, flat=1)]
 
 
 def set_variant(g, v):
@@ -373,6 +374,8 @@ def set_variant(g, v):
         g.set_option(C.OPT_SEGMENT, v["seg"])
         g.set_option(C.OPT_SORT, v.get("sort", 1))
         g.set_option(C.OPT_CONTIGUOUS, v.get("contig", 1))
+        g.set_option(C.OPT_FLAT_CUBE, v.get("flat", 0))
+        assert g.get_option(C.OPT_FLAT_CUBE) == v.get("flat", 0)
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=lambda v: "-".join(f"{k}{x}" for k, x in v.items()))
