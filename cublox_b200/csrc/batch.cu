@@ -154,7 +154,7 @@ __device__ __forceinline__ void walk_item(const MapDesc &md, const WalkItem &ite
       }
     }
     __syncwarp();
-    if (far) walk_far<true>(p, f, f.left, incs);
+    if (far) walk_far(p, f, f.left, incs);
     if (live) apply_end<S>(p, cube, re, incs, hits);
   }
   __syncthreads();
@@ -265,7 +265,7 @@ __device__ __forceinline__ void walk_item_refill(const MapDesc &md, const WalkIt
       far_load(fq + t * kFarWords, f, re);
       alive = true;
     }
-    if (walk_far<true>(p, f, kRefillSteps, incs)) {
+    if (walk_far(p, f, kRefillSteps, incs)) {
       apply_end<S>(p, cube, re, incs, hits);
       alive = false;
     }
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(1024) batch_walk_wq_kernel(const MapDesc *maps
       ++rays;
       const RayEnd re = ray_end_of<S>(p, w, clo);
       FarWalk f;
-      if (!walk_near<S>(p, cube, clo, w, f, incs)) walk_far<true>(p, f, f.left, incs);
+      if (!walk_near<S>(p, cube, clo, w, f, incs)) walk_far(p, f, f.left, incs);
       apply_end<S>(p, cube, re, incs, hits);
     }
     __syncthreads();

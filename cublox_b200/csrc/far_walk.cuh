@@ -132,6 +132,7 @@ __device__ __forceinline__ void to_far(const RayParams &p, const RayWalk &w, int
 template <int A>
 __device__ __forceinline__ bool far_step(FarWalk &f, const RayParams &p) {
   f.tM[A] = fadd(f.tM[A], f.tD[A]);
+  --f.e[A];
   int s = f.slot[A] + f.st[A];
   s = s == p.map[A] ? 0 : (s < 0 ? p.map[A] - 1 : s);
   f.slot[A] = s;
@@ -150,44 +151,23 @@ __device__ __forceinline__ bool far_step(FarWalk &f, const RayParams &p) {
 // iteration counts the current voxel, then steps.  Returns true if the ray's
 // loop is over (window left, endpoint reached or step limit spent), false
 // if only the budget stopped it.
-//
-// Per step the loop keeps only what the next step needs: the endpoint
-// counters e and the out counters both drop by one on every step of their
-// axis, so e - out is fixed during the loop and e is restored from out when
-// the loop stops; the steps taken follow from the iterations left.  kMark:
-// flag the lines counted in (the fold visits only flagged lines); the
-// caller knows whether p.dirty is set.
-template <bool kMark>
 __device__ __forceinline__ bool walk_far(const RayParams &p, FarWalk &f, int budget,
                                          uint32_t &incs) {
   const int lim = min(budget, f.left);
   bool reachable = true;
   int to_end = 0;
-  uint32_t eo[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (f.st[a] == 0 ? f.e[a] != 0 : f.e[a] < 0) reachable = false;
     to_end += f.e[a];
-    eo[a] = static_cast<uint32_t>(f.e[a]) - static_cast<uint32_t>(f.out[a]);  // mod 2^32
   }
-  auto restore_e = [&]() {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) f.e[a] = static_cast<int>(eo[a] + static_cast<uint32_t>(f.out[a]));
-  };
   int n = reachable ? min(lim, to_end) : lim;
   int done = 0;
   for (int pass = 0; pass < 2; ++pass) {
-    const int n0 = n;
-    while (n > 0) {
+    for (; n > 0; --n) {
       atomicAdd(p.cnt + f.h, 1u);
-      if (kMark) {
-        const int line = f.h >> kLineShift;
-        if (line != f.line) {
-          f.line = line;
-          p.dirty[line] = 1;
-        }
-      }
-      --n;
+      mark_line(p, f.h, f.line);
+      ++done;
       bool gone;
       if (f.tM[0] < f.tM[1]) {
         gone = f.tM[0] < f.tM[2] ? far_step<0>(f, p) : far_step<2>(f, p);
@@ -195,15 +175,11 @@ __device__ __forceinline__ bool walk_far(const RayParams &p, FarWalk &f, int bud
         gone = f.tM[1] < f.tM[2] ? far_step<1>(f, p) : far_step<2>(f, p);
       }
       if (gone) {
-        done += n0 - n;
         f.left -= done;
         incs += static_cast<uint32_t>(done);
-        restore_e();
         return true;
       }
     }
-    done += n0;
-    restore_e();
     // At a limit, or where the endpoint could be: stop if on it, else (a
     // counter overshot) only the limits and the window remain.
     if (done >= lim || (f.e[0] | f.e[1] | f.e[2]) == 0) break;

@@ -400,12 +400,7 @@ __global__ void __launch_bounds__(1024) seg_walk_kernel(const RayParams p, const
         far = !seg_near<S, SZ>(p, cube, clo, w, i0, budget, f, incs);
     }
     __syncwarp();
-    if (far) {
-      if (p.dirty)
-        walk_far<true>(p, f, budget, incs);
-      else
-        walk_far<false>(p, f, budget, incs);
-    }
+    if (far) walk_far(p, f, budget, incs);
     if (live && sr.k == 0) {
       // Endpoint (kernels.cu:139-151).
       ++nrays;
