@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcublox_b200.so")
 SOURCES = ["csrc/kernels.cu", "csrc/raycast_binned.cu", "csrc/raycast_split.cu", "csrc/capi.cu",
-           "csrc/noalloc.cu", "csrc/batch.cu", "csrc/server.cpp", "csrc/probe.cu", "csrc/swap.cu"]
+           "csrc/noalloc.cu", "csrc/batch.cu", "csrc/server.cpp", "csrc/probe.cu"]
 HEADERS = ["csrc/kernels.cuh", "csrc/exact_fp.cuh", "csrc/ray_walk.cuh", "csrc/fold.cuh", "csrc/far_walk.cuh", "csrc/dda_jump.cuh", "csrc/grid_internal.hpp", "../include/cublox_b200.h"]
 
 NVCC_FLAGS = [

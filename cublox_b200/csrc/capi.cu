@@ -783,8 +783,7 @@ int cublox_b200::detail::release_scratch(cublox_grid *g) {
   return CUBLOX_OK;
 }
 
-int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host,
-                                        const void *packed) {
+int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host) {
   const size_t n = static_cast<size_t>(g->nalloc);
   cudaError_t e = cudaSuccess;
   if (!g->d_occ) e = cublox_b200::detail::dmalloc(&g->d_occ, n * sizeof(float));
@@ -802,9 +801,7 @@ int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host,
   if ((e = cudaMemsetAsync(g->d_cnt, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(g->d_hit, 0, n * sizeof(uint32_t), g->stream)) != cudaSuccess)
     return cuda_fail(e, "acquire_device", __LINE__);
-  if (packed)
-    e = launch_unpack(packed, g->nalloc, g->d_occ, g->stream);
-  else if (occ_host)
+  if (occ_host)
     e = cudaMemcpyAsync(g->d_occ, occ_host, n * sizeof(float), cudaMemcpyHostToDevice, g->stream);
   else
     e = cudaMemsetAsync(g->d_occ, 0, n * sizeof(float), g->stream);
@@ -813,13 +810,9 @@ int cublox_b200::detail::acquire_device(cublox_grid *g, const float *occ_host,
   return CUBLOX_OK;
 }
 
-int cublox_b200::detail::detach_voxels(cublox_grid *g, float *occ_host, VoxelBuffers *out,
-                                       void *packed, int *d_count) {
+int cublox_b200::detail::detach_voxels(cublox_grid *g, float *occ_host, VoxelBuffers *out) {
   if (!g->d_occ) return fail(CUBLOX_ERR_INVALID, "detach_voxels: grid holds no voxel buffers");
-  if (packed) {
-    const cudaError_t e = launch_pack(g->d_occ, g->nalloc, packed, d_count, g->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "detach_voxels (pack)", __LINE__);
-  } else if (occ_host) {
+  if (occ_host) {
     const cudaError_t e = cudaMemcpyAsync(occ_host, g->d_occ,
                                           sizeof(float) * static_cast<size_t>(g->nalloc),
                                           cudaMemcpyDeviceToHost, g->stream);
@@ -834,16 +827,14 @@ int cublox_b200::detail::detach_voxels(cublox_grid *g, float *occ_host, VoxelBuf
   return CUBLOX_OK;
 }
 
-int cublox_b200::detail::attach_voxels(cublox_grid *g, VoxelBuffers *in, const float *occ_host,
-                                       const void *packed) {
+int cublox_b200::detail::attach_voxels(cublox_grid *g, VoxelBuffers *in, const float *occ_host) {
   if (g->d_occ || in->nalloc != g->nalloc || !in->occ)
     return fail(CUBLOX_ERR_INVALID, "attach_voxels: buffers of another size, or grid not empty");
   const size_t n = static_cast<size_t>(g->nalloc);
   const cudaError_t e =
-      packed     ? launch_unpack(packed, g->nalloc, in->occ, g->stream)
-      : occ_host ? cudaMemcpyAsync(in->occ, occ_host, n * sizeof(float), cudaMemcpyHostToDevice,
-                                   g->stream)
-                 : cudaMemsetAsync(in->occ, 0, n * sizeof(float), g->stream);
+      occ_host ? cudaMemcpyAsync(in->occ, occ_host, n * sizeof(float), cudaMemcpyHostToDevice,
+                                 g->stream)
+               : cudaMemsetAsync(in->occ, 0, n * sizeof(float), g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "attach_voxels", __LINE__);
   g->d_occ = in->occ;
   g->d_cnt = in->cnt;

@@ -166,9 +166,9 @@ int release_device(cublox_grid *g, float *occ_host);
 // fetch and query buffers); the voxel buffers stay.  Syncs the grid's
 // stream.
 int release_scratch(cublox_grid *g);
-// Allocate the voxel buffers again, stored log-odds from occ_host or from a
-// packed snapshot (all unknown if both are null), counters zero.
-int acquire_device(cublox_grid *g, const float *occ_host, const void *packed = nullptr);
+// Allocate the voxel buffers again, stored log-odds from occ_host (all
+// unknown if null), counters zero.
+int acquire_device(cublox_grid *g, const float *occ_host);
 // A grid's voxel buffers (stored log-odds, traversal and hit counters)
 // detached from it, to be handed to another grid of the same allocation
 // size without freeing and allocating.  The counters are zero (they are
@@ -182,29 +182,12 @@ struct VoxelBuffers {
 // Voxels the arrays of a grid with these half sizes hold (padding included).
 int64_t nalloc_for(const int half[3]);
 // Detach g's voxel buffers into *out after enqueueing, on g's stream, the
-// copy of its stored log-odds: packed into the pinned snapshot `packed`
-// (d_count: one device int of scratch), else whole to occ_host (pinned for
-// the copy to be asynchronous).  No sync, no free.  g must not be used
-// until attach_voxels.
-int detach_voxels(cublox_grid *g, float *occ_host, VoxelBuffers *out, void *packed = nullptr,
-                  int *d_count = nullptr);
+// copy of its stored log-odds to occ_host (pinned for the copy to be
+// asynchronous).  No sync, no free.  g must not be used until attach_voxels.
+int detach_voxels(cublox_grid *g, float *occ_host, VoxelBuffers *out);
 // Give g the buffers *in (same nalloc) and enqueue, on g's stream, the copy
-// of its stored log-odds from the packed snapshot, else from occ_host (all
-// unknown if both are null).
-int attach_voxels(cublox_grid *g, VoxelBuffers *in, const float *occ_host,
-                  const void *packed = nullptr);
-// Sparse snapshots of stored log-odds (csrc/swap.cu): only the 32-voxel
-// lines holding a non-zero value are copied, by kernels that write and read
-// the pinned snapshot directly.  packed_snapshot_bytes: the snapshot's size
-// for arrays of nalloc voxels.  launch_pack: occ -> snap on stream s (d_count:
-// one device int of scratch; the count lands in the snapshot's header).
-// launch_unpack: zero occ, then snap -> occ.  unpack_on_host: the same on
-// the host (after the stream that packed it has been synchronised).
-size_t packed_snapshot_bytes(int64_t nalloc);
-cudaError_t launch_pack(const float *occ, int64_t nalloc, void *snap, int *d_count,
-                        cudaStream_t s);
-cudaError_t launch_unpack(const void *snap, int64_t nalloc, float *occ, cudaStream_t s);
-void unpack_on_host(const void *snap, int64_t nalloc, float *occ);
+// of its stored log-odds from occ_host (all unknown if null).
+int attach_voxels(cublox_grid *g, VoxelBuffers *in, const float *occ_host);
 // fetch_batch on stream st (ordered after the grid's work by the caller),
 // outputs sized to the samples found, in the scratch `sc` (the grid's own if
 // null).

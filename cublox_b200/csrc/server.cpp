@@ -81,14 +81,14 @@ struct MapState {
   bool has_lo = false;
   cublox_grid *g = nullptr;  // created at first admission
   bool resident = false;
-  // stored log-odds while evicted (the grid's own layout): a pinned packed
-  // snapshot (only the lines holding a non-zero value; csrc/swap.cu)
+  // stored log-odds while evicted (the grid's own layout): a pinned buffer
   // allocated when the maps outgrow the budget (cublox_server_add_map) or at
-  // the map's first eviction, and kept; a whole pageable copy if pinning
-  // failed
-  void *snap_pinned = nullptr;
+  // the map's first eviction, and kept; pageable memory if pinning failed
+  float *snap_pinned = nullptr;
   std::vector<float> snap_pageable;
-  const float *pageable() const { return snap_pageable.empty() ? nullptr : snap_pageable.data(); }
+  const float *snapshot() const {
+    return snap_pinned ? snap_pinned : (snap_pageable.empty() ? nullptr : snap_pageable.data());
+  }
   size_t vox_bytes = 0;  // device bytes of the map's arrays
   int64_t nalloc = 0;    // voxels each array holds (padding included)
   int64_t voxels = 0;
@@ -191,7 +191,6 @@ struct cublox_server {
   // voxel buffers of evicted maps, kept for the next map of the same size
   // (worker thread only)
   std::vector<cublox_b200::detail::VoxelBuffers> spare;
-  int *d_count = nullptr;  // device scratch of the snapshot packer (server stream)
   std::atomic<int> n_maps{0};                    // maps[0, n_maps) are published
   std::deque<Tick> inflight;
   std::deque<FetchJob> fetch_jobs;
@@ -270,8 +269,7 @@ size_t used_bytes(cublox_server *s) {
 int take_spare(cublox_server *s, MapState &m) {
   for (size_t i = 0; i < s->spare.size(); ++i) {
     if (s->spare[i].nalloc != m.nalloc) continue;
-    const int rc =
-        cublox_b200::detail::attach_voxels(m.g, &s->spare[i], m.pageable(), m.snap_pinned);
+    const int rc = cublox_b200::detail::attach_voxels(m.g, &s->spare[i], m.snapshot());
     if (rc) return rc;
     s->spare.erase(s->spare.begin() + static_cast<std::ptrdiff_t>(i));
     return 1;
@@ -361,20 +359,18 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
       return fail(CUBLOX_ERR_NOMEM, "server: no map can be evicted");
     }
     MapState &v = *s->maps[victim];
+    const size_t n = static_cast<size_t>(v.nalloc);
     if (!v.snap_pinned && v.snap_pageable.empty() &&
-        cublox_b200::detail::hmalloc(&v.snap_pinned,
-                                     cublox_b200::detail::packed_snapshot_bytes(v.nalloc)) !=
-            cudaSuccess) {
+        cublox_b200::detail::hmalloc(&v.snap_pinned, n * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       v.snap_pinned = nullptr;
-      v.snap_pageable.resize(static_cast<size_t>(v.nalloc));
+      v.snap_pageable.resize(n);
     }
     // The stored log-odds go to the snapshot on the server stream, ordered
     // before any later use of the buffers; the buffers become a spare set.
     cublox_b200::detail::VoxelBuffers vb;
-    int rc = v.snap_pinned
-                 ? cublox_b200::detail::detach_voxels(v.g, nullptr, &vb, v.snap_pinned, s->d_count)
-                 : cublox_b200::detail::detach_voxels(v.g, v.snap_pageable.data(), &vb);
+    int rc = cublox_b200::detail::detach_voxels(
+        v.g, v.snap_pinned ? v.snap_pinned : v.snap_pageable.data(), &vb);
     if (rc) return rc;
     s->spare.push_back(vb);
     v.resident = false;
@@ -391,7 +387,7 @@ int admit(cublox_server *s, int mi, const std::vector<char> &busy, bool *later) 
       cublox_grid_set_log_odds(m.g, m.lo[0], m.lo[1], m.lo[2], m.lo[3], m.lo[4], m.lo[5]);
   } else if (need) {
     free_spares(s, need);
-    rc = cublox_b200::detail::acquire_device(m.g, m.pageable(), m.snap_pinned);
+    rc = cublox_b200::detail::acquire_device(m.g, m.snapshot());
     if (rc) return rc;
   }
   m.resident = true;
@@ -713,10 +709,6 @@ int cublox_server_create(const cublox_server_config *cfg, cublox_server **out) {
   }
   cublox_batch_set_option(s->batch, CUBLOX_BATCH_OPT_GRAPHS, s->cfg.graphs ? 1 : 0);
   rc = cublox_batch_reserve(s->batch, s->cfg.max_tick_points, 64);
-  if (!rc && cublox_b200::detail::dmalloc(&s->d_count, sizeof(int)) != cudaSuccess) {
-    cudaGetLastError();
-    rc = fail(CUBLOX_ERR_NOMEM, "server_create: device allocation failed");
-  }
   if (!rc) rc = s->pinned.init(s->cfg.pinned_pool_bytes, s->device);
   if (!rc)
     rc = cublox_b200::detail::reserve_fetch(&s->fscratch, s->cfg.max_fetch_centres,
@@ -724,7 +716,6 @@ int cublox_server_create(const cublox_server_config *cfg, cublox_server **out) {
   if (rc) {
     const std::string msg = cublox_last_error();
     cublox_b200::detail::free_fetch(&s->fscratch);
-    cublox_b200::detail::dfree(s->d_count);
     s->pinned.release_all();
     cublox_batch_destroy(s->batch);
     cudaStreamDestroy(s->stream);
@@ -769,7 +760,6 @@ int cublox_server_destroy(cublox_server *s) {
     cublox_b200::detail::dfree(v.cnt);
     cublox_b200::detail::dfree(v.hit);
   }
-  cublox_b200::detail::dfree(s->d_count);
   cublox_batch_destroy(s->batch);
   cublox_b200::detail::free_fetch(&s->fscratch);
   s->pinned.release_all();
@@ -824,7 +814,7 @@ int cublox_server_add_map(cublox_server *s, const int half_map_size[3], float re
     for (auto &o : s->maps)
       if (!o->snap_pinned && o->snap_pageable.empty() &&
           cublox_b200::detail::hmalloc(&o->snap_pinned,
-                                       cublox_b200::detail::packed_snapshot_bytes(o->nalloc)) !=
+                                       static_cast<size_t>(o->nalloc) * sizeof(float)) !=
               cudaSuccess) {
         cudaGetLastError();  // pinned later, or pageable
         o->snap_pinned = nullptr;
@@ -975,16 +965,7 @@ int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int orig
     rc = cublox_grid_export(m.g, occ_host);
     if (rc) return rc;
   } else {
-    // the snapshot is complete once the server stream has run its copy
-    if (cudaStreamSynchronize(s->stream) != cudaSuccess)
-      return fail(CUBLOX_ERR_CUDA, "server_export: stream synchronisation failed");
-    if (m.snap_pinned) {
-      std::vector<float> arr(static_cast<size_t>(m.nalloc));
-      cublox_b200::detail::unpack_on_host(m.snap_pinned, m.nalloc, arr.data());
-      cublox_b200::detail::layout_to_reference(m.g, arr.data(), occ_host);
-    } else {
-      cublox_b200::detail::layout_to_reference(m.g, m.pageable(), occ_host);
-    }
+    cublox_b200::detail::layout_to_reference(m.g, m.snapshot(), occ_host);
   }
   if (origin_index) cublox_grid_origin(m.g, origin_index, nullptr);
   return CUBLOX_OK;
