@@ -965,6 +965,9 @@ int cublox_server_export(cublox_server *s, int map_id, float *occ_host, int orig
     rc = cublox_grid_export(m.g, occ_host);
     if (rc) return rc;
   } else {
+    // the snapshot is complete once the server stream has run its copy
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess)
+      return fail(CUBLOX_ERR_CUDA, "server_export: stream synchronisation failed");
     cublox_b200::detail::layout_to_reference(m.g, m.snapshot(), occ_host);
   }
   if (origin_index) cublox_grid_origin(m.g, origin_index, nullptr);
