@@ -164,6 +164,7 @@ def lib():
             "cublox_server_scratch_bytes": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_uint64)],
                                             ctypes.c_int),
             "cublox_runtime_counters": ([i64, ctypes.c_int], ctypes.c_int),
+            "cublox_test_fail_allocations": ([ctypes.c_int64, ctypes.c_int64], ctypes.c_int),
             "cublox_probe_red_rate": ([ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "cublox_batch_reserve_maps": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int64],
@@ -819,6 +820,13 @@ def red_rate(buffer_bytes: int, total_ops: int = 1 << 30, stream: int = 0) -> fl
 
 
 COUNTER_NAMES = ("device_allocs", "device_frees", "pinned_allocs", "pinned_frees", "graph_builds")
+
+
+def fail_allocations(skip: int, count: int):
+    """Test hook (cublox_test_fail_allocations): after `skip` more device or
+    pinned allocations, the next `count` fail as if memory were exhausted;
+    count 0 turns it off."""
+    _check(lib().cublox_test_fail_allocations(int(skip), int(count)), "test_fail_allocations")
 
 
 def runtime_counters() -> dict:

@@ -815,6 +815,8 @@ int ensure_dev(void **p, size_t bytes) {
   return CUBLOX_OK;
 }
 
+void drop_graph(cublox_batch *b);
+
 int ensure_capacity(cublox_batch *b, int n_maps, int n_witems, int n_fitems) {
   if (n_maps > b->maps_cap || n_witems > b->witems_cap || n_fitems > b->fitems_cap) {
     if (b->staged) cudaEventSynchronize(b->staged);
@@ -829,8 +831,12 @@ int ensure_capacity(cublox_batch *b, int n_maps, int n_witems, int n_fitems) {
         (rc = ensure_dev(reinterpret_cast<void **>(&b->d_fitems), sizeof(FoldItem) * fc)) ||
         (rc = ensure_pinned(reinterpret_cast<void **>(&b->h_maps), sizeof(MapDesc) * mc)) ||
         (rc = ensure_pinned(reinterpret_cast<void **>(&b->h_witems), sizeof(WalkItem) * wc)) ||
-        (rc = ensure_pinned(reinterpret_cast<void **>(&b->h_fitems), sizeof(FoldItem) * fc)))
+        (rc = ensure_pinned(reinterpret_cast<void **>(&b->h_fitems), sizeof(FoldItem) * fc))) {
+      // some buffers are gone: the next update sizes them all again
+      b->maps_cap = b->witems_cap = b->fitems_cap = 0;
+      drop_graph(b);
       return rc;
+    }
     b->maps_cap = mc;
     b->witems_cap = wc;
     b->fitems_cap = fc;
@@ -850,6 +856,7 @@ int reserve_points(cublox_batch *b, size_t floats) {
   if (floats > b->points_cap) {
     floats = std::max(floats, 2 * b->points_cap);
     cudaStreamSynchronize(b->stream);
+    b->points_cap = 0;
     if ((rc = ensure_dev(reinterpret_cast<void **>(&b->d_points), floats * sizeof(float))))
       return rc;
     b->points_cap = floats;
@@ -857,6 +864,7 @@ int reserve_points(cublox_batch *b, size_t floats) {
   if (floats > b->h_points_cap) {
     floats = std::max(floats, 2 * b->h_points_cap);
     cudaStreamSynchronize(b->stream);  // a walk may be reading the old buffer in place
+    b->h_points_cap = 0;
     if ((rc = ensure_pinned(reinterpret_cast<void **>(&b->h_points), floats * sizeof(float))))
       return rc;
     b->h_points_cap = floats;

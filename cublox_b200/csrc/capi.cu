@@ -31,7 +31,21 @@ namespace cublox_b200 {
 namespace detail {
 void count(Counter c) { g_counters[c].fetch_add(1, std::memory_order_relaxed); }
 
+// Test hook (cublox_test_fail_allocations): after g_fail_skip more
+// allocations, the next g_fail_count fail without a CUDA call.
+std::atomic<int64_t> g_fail_skip{0}, g_fail_count{0};
+
+bool injected_failure() {
+  if (g_fail_count.load(std::memory_order_relaxed) <= 0) return false;
+  if (g_fail_skip.fetch_sub(1, std::memory_order_relaxed) > 0) return false;
+  return g_fail_count.fetch_sub(1, std::memory_order_relaxed) > 0;
+}
+
 cudaError_t dev_alloc(void **p, size_t bytes) {
+  if (injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
   count(kDevAllocs);
   return cudaMalloc(p, bytes);
 }
@@ -43,6 +57,10 @@ cudaError_t dev_free(void *p) {
 }
 
 cudaError_t pinned_alloc(void **p, size_t bytes) {
+  if (injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
   count(kPinnedAllocs);
   return cudaMallocHost(p, bytes);
 }
@@ -125,6 +143,14 @@ extern "C" {
 
 const char *cublox_last_error(void) { return g_err.c_str(); }
 const char *cublox_version(void) { return "cublox_b200 0.2 (sm_100a)"; }
+
+int cublox_test_fail_allocations(int64_t skip, int64_t count) {
+  if (skip < 0 || count < 0) return fail(CUBLOX_ERR_INVALID, "test_fail_allocations: negative");
+  cublox_b200::detail::g_fail_count.store(0);
+  cublox_b200::detail::g_fail_skip.store(skip);
+  cublox_b200::detail::g_fail_count.store(count);
+  return CUBLOX_OK;
+}
 
 int cublox_runtime_counters(int64_t *out, int n) {
   if (!out || n < 0) return fail(CUBLOX_ERR_INVALID, "runtime_counters: bad argument");

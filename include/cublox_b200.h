@@ -57,6 +57,13 @@ int cublox_binary_version(int *binary_version);
  * graphs instantiated.  Fills the first n (entries past 5 read 0).  No
  * counterpart in the reference.                                             */
 int cublox_runtime_counters(int64_t *out, int n);
+/* Test hook: once `skip` more device or pinned allocations have been made,
+ * the next `count` fail as if memory were exhausted (no CUDA call is made;
+ * the failing call returns CUBLOX_ERR_NOMEM or its caller's error), so that
+ * tests can drive the out-of-memory paths without exhausting a GPU; count 0
+ * turns it off.  Process-wide.  No counterpart in the reference, whose
+ * CUDA_OK aborts the process on any failed call (OccupancyGrid.cpp:32-49). */
+int cublox_test_fail_allocations(int64_t skip, int64_t count);
 /* Measures the device's throughput of 32-bit atomic adds whose result is
  * unused (the walk's only memory operation) to pseudo-random distinct
  * addresses of a buffer of buffer_bytes (allocated and freed by the call):
