@@ -170,14 +170,15 @@ def cpu_baseline(w, scans, origins, steps, budget_s=12.0):
                       f"{threads} threads, {dt:.1f} s"}
 
 
-def profiled_traffic(n_maps: int):
-    """DRAM bytes of one batched step (walk + fold) per map, from the ncu
-    capture recorded in profiles/traffic.json, scaled to n_maps (each map's
-    walk and fold touch only its own voxels).  Returns (bytes, source)."""
+def profiled_traffic(n_maps: int, key: str = "update_bytes_per_map"):
+    """DRAM bytes of one batched step per map (walk + fold, or the kernel
+    `key` names), from the ncu capture recorded in profiles/traffic.json,
+    scaled to n_maps (each map's walk and fold touch only its own voxels).
+    Returns (bytes, source)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
-        return float(t["update_bytes_per_map"]) * n_maps, t.get("source")
+        return float(t[key]) * n_maps, t.get("source")
     except (OSError, KeyError, ValueError):
         return None, None
 
@@ -1079,6 +1080,14 @@ def main():
     red_l2 = C.red_rate(64 << 20, 1 << 30)      # buffer in L2
     red_hbm = C.red_rate(4 << 30, 1 << 30)      # buffer far beyond L2
     ach = float(np.mean(h["incs"]) / (np.mean(h["walk_ms"]) / 1e3))
+    fold_bytes = profiled_traffic(h["K"], "fold_bytes_per_map")[0]
+    if fold_bytes:
+        fold_gbs = fold_bytes / (float(np.mean(h["fold_ms"])) / 1e3) / 1e9
+        out["roofline"]["fold"] = {
+            "kernel": "batch fold (flagged lines)", "achieved": fold_gbs, "unit": "GB/s",
+            "peak": h["peak"], "frac": fold_gbs / h["peak"], "peak_source": h["peak_kind"],
+            "basis": "the fold's ncu DRAM bytes per map x maps / its live device time: the "
+                     "bytes it must move (256 B read and up to 256 B written per flagged line)"}
     out["roofline"]["l2_atomic"] = {
         "kernel": "batch walk", "achieved": ach, "unit": "atomic adds/s",
         "peak": red_l2, "frac": ach / red_l2, "peak_beyond_l2": red_hbm,
