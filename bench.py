@@ -73,6 +73,7 @@ class Clocks:
         self.index = index
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -83,7 +84,15 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: let its first sample land
+            # before the timed region begins, so that the region's own
+            # samples follow
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.01)
+            with open(self.path) as f:
+                self.skip = sum(1 for _ in f)  # samples taken before the region
         except Exception:
             self.proc = None
         return self
@@ -111,6 +120,8 @@ class Clocks:
                 os.unlink(self.path)
             except Exception:
                 pass
+        if len(rows) > self.skip:
+            rows = rows[self.skip:]  # keep the region's own samples when there are any
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
