@@ -60,8 +60,9 @@ struct FoldItem {
 // [4] a fused launch's fold wait gave up (the rest of the launch then skips
 // its waits and folds), [5] the fused launch's wait limit (sleep rounds)
 constexpr int kCounters = 6;
-constexpr int kFoldItemLines = 1 << 12;  // 32-voxel lines per fold item
-static_assert(kFoldItemLines == kListLines, "a fold item is one CTA's line list");
+constexpr int kFoldItemLines = 1 << 11;  // 32-voxel lines per fold item
+static_assert(kFoldItemLines <= kListLines && kFoldItemLines % 16 == 0,
+              "a fold item fits one CTA's line list");
 // Fused launch: how long a fold item waits for its map's walk items
 // (rounds of a ~256 ns sleep, about 2 s) before it gives up and flags
 // kErrWaitTimeout in the map's error word (CUBLOX_BATCH_OPT_WAIT_LIMIT).

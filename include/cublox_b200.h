@@ -307,7 +307,7 @@ typedef struct cublox_batch cublox_batch;
 #define CUBLOX_BATCH_OPT_NUM_SHAPES 5 /* read only: number of shapes        */
 #define CUBLOX_BATCH_OPT_FOLD 6       /* fold: 0 (default) the 32-voxel
                                          lines the walk flagged, compacted
-                                         into a list per 4096 lines; 1 every
+                                         into a list per 2048 lines; 1 every
                                          line (the reference's full sweep,
                                          for comparison); 2 the flagged
                                          lines, 32 flags at a time per
