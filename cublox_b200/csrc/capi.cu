@@ -772,20 +772,6 @@ size_t cublox_b200::detail::device_bytes(const cublox_grid *g) {
   return b;
 }
 
-int cublox_b200::detail::release_device(cublox_grid *g, float *occ_host) {
-  cudaError_t e = cudaStreamSynchronize(g->stream);
-  if (e == cudaSuccess && occ_host && g->d_occ)
-    e = cudaMemcpy(occ_host, g->d_occ, sizeof(float) * static_cast<size_t>(g->nalloc),
-                   cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_fail(e, "release_device", __LINE__);
-  cublox_b200::detail::dfree(g->d_occ);
-  cublox_b200::detail::dfree(g->d_cnt);
-  cublox_b200::detail::dfree(g->d_hit);
-  g->d_occ = nullptr;
-  g->d_cnt = g->d_hit = nullptr;
-  return release_scratch(g);
-}
-
 int cublox_b200::detail::release_scratch(cublox_grid *g) {
   const cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "release_scratch", __LINE__);

@@ -157,17 +157,13 @@ RayParams ray_params(const cublox_grid *g, const float *x, const float *y, const
 // Device memory a grid holds now: voxel buffers plus the per-call scratch
 // it has grown.
 size_t device_bytes(const cublox_grid *g);
-// Give back every device buffer of a grid but the few bytes of bookkeeping,
-// copying the stored log-odds to occ_host first (if not null).  The grid
-// keeps its host state (window origin, parameters) and must not be used
-// until acquire_device.
-int release_device(cublox_grid *g, float *occ_host);
 // Free the per-call scratch a grid has grown (cloud staging, walk plans,
 // fetch and query buffers); the voxel buffers stay.  Syncs the grid's
 // stream.
 int release_scratch(cublox_grid *g);
-// Allocate the voxel buffers again, stored log-odds from occ_host (all
-// unknown if null), counters zero.
+// Allocate the voxel buffers of a grid whose buffers were detached
+// (detach_voxels), stored log-odds from occ_host (all unknown if null),
+// counters zero.
 int acquire_device(cublox_grid *g, const float *occ_host);
 // A grid's voxel buffers (stored log-odds, traversal and hit counters)
 // detached from it, to be handed to another grid of the same allocation
