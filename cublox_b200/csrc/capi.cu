@@ -1164,9 +1164,8 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
     g->last_cleared = g->voxel_num - keep;
   }
   // Brick layouts: the bricks holding a marked slab, as three lists (x
-  // brick columns, y brick rows, z brick levels).  An x brick column whose
-  // slots are all marked is one contiguous run of the arrays: such columns
-  // are cleared by memsets and left off the list.
+  // brick columns, y brick rows, z brick levels), all cleared by one kernel
+  // (a column whose slots are all marked is written as whole lines).
   const bool bricks = g->lay_code != 0;
   std::vector<int> blist;
   int nb[3] = {0, 0, 0};
@@ -1176,20 +1175,9 @@ int cublox_grid_recenter(cublox_grid *g, const float pos[3], int *action) {
     for (int a = 0; a < 3; ++a) {
       const int B = 1 << g->lay.lb[a];
       for (int b = 0; b < g->nbr[a]; ++b) {
-        int any = 0, all = 1;
-        for (int sl = b * B; sl < std::min((b + 1) * B, g->map[a]); ++sl) {
-          const bool mk = marked(a, sl);
-          any |= mk;
-          all &= mk;
-        }
+        bool any = false;
+        for (int sl = b * B; sl < std::min((b + 1) * B, g->map[a]); ++sl) any |= marked(a, sl);
         if (!any) continue;
-        if (a == 0 && all) {
-          if (!x_runs.empty() && x_runs.back().second == b)
-            ++x_runs.back().second;
-          else
-            x_runs.push_back({b, b + 1});
-          continue;
-        }
         blist.push_back(b);
         ++nb[a];
       }
