@@ -256,19 +256,22 @@ __global__ void __launch_bounds__(256) clear_kernel(const ClearParams p) {
   }
 }
 
-// Union-of-slabs clear for 32-voxel brick layouts.  A warp takes one
-// (x brick, y brick) column of bricks at a time, a lane per voxel of a
-// brick: the columns of the listed x bricks crossed with every y brick,
-// then of every x brick crossed with the listed y bricks (the warp walks the
-// column's z bricks, consecutive 128-byte lines), then of every (x, y) brick
-// for the listed z bricks.  A lane clears its voxel if its x, y or z slot is
-// marked; lanes of padding slots (past the map) do nothing; a brick on two
-// lists is cleared twice, with the same result.  One index division per
-// column, not per brick: the clear runs at memory speed.
+// Union-of-slabs clear for 32-voxel brick layouts.  A warp takes up to
+// kClearZ bricks of one (x brick, y brick) column at a time, a lane per
+// voxel of a brick: the columns of the listed x bricks crossed with every y
+// brick, then of every x brick crossed with the listed y bricks (the warp
+// walks consecutive 128-byte lines of the column), then of every (x, y)
+// brick for the listed z bricks.  A lane clears its voxel if its x, y or z
+// slot is marked; lanes of padding slots (past the map) do nothing; a brick
+// on two lists is cleared twice, with the same result.  Index divisions are
+// per run of lines, not per brick.
+constexpr int kClearZ = 8;
+
 __global__ void __launch_bounds__(256) clear_bricks_kernel(const ClearParams p) {
   const int lane = threadIdx.x & 31;
-  const int u0 = p.nb[0] * p.nbr[1];  // listed x bricks x every y brick
-  const int u1 = p.nbr[0] * p.nb[1];  // every x brick x listed y bricks
+  const int chunks = (p.nbr[2] + kClearZ - 1) / kClearZ;  // runs of z bricks per column
+  const int u0 = p.nb[0] * p.nbr[1] * chunks;  // listed x bricks x every y brick
+  const int u1 = p.nbr[0] * p.nb[1] * chunks;  // every x brick x listed y bricks
   const int u2 = p.nb[2] > 0 ? p.nbr[0] * p.nbr[1] : 0;
   const int units = u0 + u1 + u2;
   const int l12 = p.lay.lb[1] + p.lay.lb[2];
@@ -278,14 +281,17 @@ __global__ void __launch_bounds__(256) clear_bricks_kernel(const ClearParams p) 
   auto marked = [](const uint32_t *m, int s) { return ((m[s >> 5] >> (s & 31)) & 1u) != 0u; };
   for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < units;
        u += (gridDim.x * blockDim.x) >> 5) {
-    int bx, by;
+    int bx, by, z0 = 0;
     if (u < u0) {
-      bx = p.blist[u / p.nbr[1]];
-      by = u % p.nbr[1];
+      const int col = u / chunks;
+      z0 = (u - col * chunks) * kClearZ;
+      bx = p.blist[col / p.nbr[1]];
+      by = col % p.nbr[1];
     } else if (u < u0 + u1) {
-      const int v = u - u0;
-      bx = v / p.nb[1];
-      by = p.blist[p.nb[0] + v % p.nb[1]];
+      const int v = u - u0, col = v / chunks;
+      z0 = (v - col * chunks) * kClearZ;
+      bx = col / p.nb[1];
+      by = p.blist[p.nb[0] + col % p.nb[1]];
     } else {
       const int v = u - u0 - u1;
       bx = v / p.nbr[1];
@@ -296,7 +302,8 @@ __global__ void __launch_bounds__(256) clear_bricks_kernel(const ClearParams p) 
     const bool xy = marked(p.xmask, s0) || marked(p.ymask, s1);
     float *col = p.occ + bx * p.lay.bs[0] + by * p.lay.bs[1] + lane;
     if (u < u0 + u1) {
-      for (int bz = 0; bz < p.nbr[2]; ++bz) {
+      const int z1 = min(z0 + kClearZ, p.nbr[2]);
+      for (int bz = z0; bz < z1; ++bz) {
         const int s2 = (bz << p.lay.lb[2]) + i2;
         if (s2 < p.map[2] && (xy || (p.any_z && marked(p.zmask, s2))))
           col[bz * p.lay.bs[2]] = 0.0f;
@@ -693,11 +700,12 @@ void launch_relayout(const float *src, float *dst, const VoxLayout &lay, const i
 
 void launch_clear(const ClearParams &p, cudaStream_t s) {
   if (p.blist) {
-    const long long units = static_cast<long long>(p.nb[0]) * p.nbr[1] +
-                            static_cast<long long>(p.nbr[0]) * p.nb[1] +
+    const long long chunks = (p.nbr[2] + kClearZ - 1) / kClearZ;
+    const long long units = static_cast<long long>(p.nb[0]) * p.nbr[1] * chunks +
+                            static_cast<long long>(p.nbr[0]) * p.nb[1] * chunks +
                             (p.nb[2] > 0 ? static_cast<long long>(p.nbr[0]) * p.nbr[1] : 0);
     if (units <= 0) return;
-    long long grid = (units + 7) / 8;  // a column of bricks per warp
+    long long grid = (units + 7) / 8;  // a run of a column's bricks per warp
     if (grid > sm_count() * 16) grid = sm_count() * 16;
     clear_bricks_kernel<<<static_cast<int>(grid), 256, 0, s>>>(p);
     return;
